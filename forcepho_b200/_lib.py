@@ -1,0 +1,120 @@
+"""ctypes binding of ``libfpho.so`` (the C ABI declared in include/fpho.h).
+
+The library is built in-tree by :mod:`forcepho_b200.build`.  Importing this
+module loads it; if it is missing it is compiled (nvcc is present wherever the
+package is built), and if that is impossible the import fails loudly: there is
+no CPU fallback for the hot path.
+"""
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import build as _build
+
+FPHO_OK = 0
+FPHO_IO_HOST = 1
+FPHO_WANT_RESIDUAL = 2
+
+_ERRNAMES = {1: "INVALID", 2: "CUDA", 3: "NOMEM", 4: "LIMIT", 5: "STATE", 6: "KERNEL"}
+
+
+class FphoError(RuntimeError):
+    """A C-ABI call returned a non-zero status."""
+
+    def __init__(self, code, func, msg):
+        self.code = code
+        super().__init__(f"{func} -> FPHO_ERR_{_ERRNAMES.get(code, code)}: {msg}")
+
+
+def _load():
+    path = _build.LIB
+    if _build.needs_build():
+        _build.build()
+    if not os.path.exists(path):
+        raise ImportError(f"forcepho_b200: CUDA library {path} is missing and could not be built")
+    return ctypes.CDLL(path)
+
+
+lib = _load()
+
+c_void_p = ctypes.c_void_p
+c_int = ctypes.c_int
+c_uint = ctypes.c_uint
+c_int64_p = ctypes.POINTER(ctypes.c_int64)
+
+_SIGS = {
+    "fpho_last_error": (ctypes.c_char_p, []),
+    "fpho_abi_version": (c_int, []),
+    "fpho_sizeof": (c_int, [c_int]),
+    "fpho_patch_create": (c_int, [c_void_p, c_int, c_int, c_void_p, ctypes.POINTER(c_void_p)]),
+    "fpho_patch_replace_meta": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "fpho_patch_swap_data_residual": (c_int, [c_void_p, c_void_p]),
+    "fpho_patch_retrieve": (c_int, [c_void_p, c_int, c_void_p, c_void_p]),
+    "fpho_patch_device_struct": (c_int, [c_void_p, ctypes.POINTER(c_void_p)]),
+    "fpho_patch_info": (c_int, [c_void_p, c_int64_p]),
+    "fpho_patch_free": (c_int, [c_void_p]),
+    "fpho_patch_set_config": (c_int, [c_void_p, c_int, c_int, c_void_p]),
+    "fpho_variant_info": (c_int, [c_int, ctypes.POINTER(c_int)]),
+    "fpho_patch_count_pairs": (c_int, [c_void_p, c_int, ctypes.POINTER(ctypes.c_longlong)]),
+    "fpho_patch_error_word": (c_int, [c_void_p, ctypes.POINTER(c_int)]),
+    "fpho_evaluate_proposal": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_int,
+                                       c_uint, c_void_p]),
+    "fpho_EvaluateProposal": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                      c_void_p]),
+}
+
+
+def _bind():
+    missing = []
+    for name, (res, args) in _SIGS.items():
+        try:
+            f = getattr(lib, name)
+        except AttributeError:
+            missing.append(name)
+            continue
+        f.restype = res
+        f.argtypes = args
+    if missing:
+        raise ImportError(f"libfpho.so lacks symbols: {missing}")
+
+
+_bind()
+
+
+def last_error():
+    return lib.fpho_last_error().decode(errors="replace")
+
+
+def check(rc, func="fpho"):
+    if rc != FPHO_OK:
+        raise FphoError(rc, func, last_error())
+    return rc
+
+
+def call(name, *args):
+    """Call a C-ABI function and raise FphoError on a non-zero status."""
+    return check(getattr(lib, name)(*args), name)
+
+
+def variants():
+    """List of (threads per CTA, pixels per thread) of the compiled tile kernels."""
+    out = (c_int * 2)()
+    n = lib.fpho_variant_info(0, out)
+    res = []
+    for v in range(n):
+        lib.fpho_variant_info(v, out)
+        res.append((out[0], out[1]))
+    return res
+
+
+def ptr(a):
+    """Address of a numpy array or torch tensor (or an int)."""
+    if a is None:
+        return None
+    if isinstance(a, int):
+        return a
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    return a.data_ptr()

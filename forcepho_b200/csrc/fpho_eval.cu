@@ -1,0 +1,723 @@
+// fpho_eval.cu -- patch handles and single-patch evaluation behind the C ABI
+// of include/fpho.h.
+//
+// Per evaluation, three kernels run on the caller's stream:
+//   build_image_gaussians  one thread per image Gaussian (exposure, source, PSF
+//                          component): record + culling box into the workspace;
+//   tile_kernel<NT,K>      one CTA per pixel tile (fpho_tile.cuh);
+//   reduce_bands           FP64 sum of the tile partials of each band.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdarg>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "fpho_impl.cuh"
+#include "fpho_internal.h"
+#include "fpho_tile.cuh"
+
+using namespace fpho;
+
+// ======================================================================= errors
+namespace fpho {
+static thread_local std::string g_last_error;
+
+int set_error(int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+void clear_error() { g_last_error.clear(); }
+}  // namespace fpho
+
+#define CUDA_TRY(call)                                                                  \
+    do {                                                                                \
+        cudaError_t e_ = (call);                                                        \
+        if (e_ != cudaSuccess)                                                          \
+            return set_error(FPHO_ERR_CUDA, "%s failed: %s (%s:%d)", #call,             \
+                             cudaGetErrorString(e_), __FILE__, __LINE__);               \
+    } while (0)
+
+extern "C" const char *fpho_last_error(void) { return fpho::g_last_error.c_str(); }
+extern "C" int fpho_abi_version(void) { return (1 << 16) | 0; }
+extern "C" int fpho_sizeof(int which) {
+    switch (which) {
+        case 0: return (int)sizeof(fpho_patch_struct);
+        case 1: return (int)sizeof(fpho_source);
+        case 2: return (int)sizeof(fpho_psfgauss);
+        case 3: return (int)sizeof(fpho_response);
+        default: return -1;
+    }
+}
+
+// ======================================================================= kernels
+namespace fpho {
+
+__global__ void build_image_gaussians(PatchView pv, const fpho_source *src, float *gtab,
+                                      float4 *gbox) {
+    const int e = blockIdx.y;
+    const int g0 = pv.gauss_start[e];
+    const int n = pv.gauss_start[e + 1] - g0;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int npsf = pv.exp_npsf[e];
+    const int s = i / npsf, p = i - s * npsf;
+    build_one_gaussian(pv, src, e, s, p, gtab + (size_t)(g0 + i) * GREC, gbox + g0 + i);
+}
+
+// Bounding boxes of every tile: over all pixels and over pixels with ierr != 0.
+__global__ void tile_bboxes(PatchView pv, const TileDesc *tiles, float4 *tbox_all,
+                            float4 *tbox_w) {
+    const TileDesc td = tiles[blockIdx.x];
+    float ax0 = INFINITY, ax1 = -INFINITY, ay0 = INFINITY, ay1 = -INFINITY;
+    float wx0 = INFINITY, wx1 = -INFINITY, wy0 = INFINITY, wy1 = -INFINITY;
+    for (int i = threadIdx.x; i < td.count; i += blockDim.x) {
+        const int pix = td.pix_begin + i;
+        const float x = pv.xpix[pix], y = pv.ypix[pix];
+        ax0 = fminf(ax0, x); ax1 = fmaxf(ax1, x);
+        ay0 = fminf(ay0, y); ay1 = fmaxf(ay1, y);
+        if (pv.ierr[pix] != 0.0f) {
+            wx0 = fminf(wx0, x); wx1 = fmaxf(wx1, x);
+            wy0 = fminf(wy0, y); wy1 = fmaxf(wy1, y);
+        }
+    }
+    __shared__ float red[8][32];
+    float v[8] = {ax0, -ax1, ay0, -ay1, wx0, -wx1, wy0, -wy1};
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+        for (int o = 16; o > 0; o >>= 1) v[k] = fminf(v[k], __shfl_xor_sync(0xffffffffu, v[k], o));
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0)
+        for (int k = 0; k < 8; ++k) red[k][warp] = v[k];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int nw = blockDim.x / 32;
+        for (int k = 0; k < 8; ++k)
+            for (int w = 1; w < nw; ++w) red[k][0] = fminf(red[k][0], red[k][w]);
+        tbox_all[blockIdx.x] = make_float4(red[0][0], -red[1][0], red[2][0], -red[3][0]);
+        tbox_w[blockIdx.x] = make_float4(red[4][0], -red[5][0], red[6][0], -red[7][0]);
+    }
+}
+
+// Sum tile partials per band in double.  grid (n_bands, ceil(out_stride/128)).
+__global__ void reduce_bands(const int *tile_band_start, const double *pchi2, const float *pgrad,
+                             int stride, double *chi2_out, float *dchi2_out, int out_stride) {
+    const int b = blockIdx.x;
+    const int t0 = tile_band_start[b], t1 = tile_band_start[b + 1];
+    const int j = blockIdx.y * blockDim.x + threadIdx.x;
+    if (j < out_stride) {
+        double acc = 0.0;
+        if (j < stride)
+            for (int t = t0; t < t1; ++t) acc += (double)pgrad[(size_t)t * stride + j];
+        dchi2_out[(size_t)b * out_stride + j] = (float)acc;
+    }
+    if (blockIdx.y == 0 && threadIdx.x < 32) {
+        double c = 0.0;
+        for (int t = t0 + threadIdx.x; t < t1; t += 32) c += pchi2[t];
+        for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+        if (threadIdx.x == 0) chi2_out[b] = c;
+    }
+}
+
+template <int NT, int K>
+__global__ void __launch_bounds__(NT) tile_kernel(TileArgs A) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ uint64_t mbar;
+    if (threadIdx.x == 0) {
+        mbar_init(&mbar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    uint32_t phase = 0;
+    tile_body<NT, K>(A, blockIdx.x, smem, &mbar, phase);
+}
+
+// ------------------------------------------------------------ variants
+struct Variant {
+    int nt, k;
+    const void *fn;
+};
+static const Variant kVariants[] = {
+    {128, 4, (const void *)tile_kernel<128, 4>},
+    {128, 2, (const void *)tile_kernel<128, 2>},
+    {256, 2, (const void *)tile_kernel<256, 2>},
+    {64, 4, (const void *)tile_kernel<64, 4>},
+    {256, 4, (const void *)tile_kernel<256, 4>},
+    {128, 8, (const void *)tile_kernel<128, 8>},
+};
+constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
+
+int variant_count() { return kNumVariants; }
+int variant_tile_pixels(int v) { return kVariants[v].nt * kVariants[v].k; }
+int variant_threads(int v) { return kVariants[v].nt; }
+
+static std::mutex g_attr_mu;
+static size_t g_attr_set[64][kNumVariants];  // per device, per variant
+
+int launch_tile_kernel(int variant, const TileArgs &A, int n_tiles, cudaStream_t stream) {
+    if (n_tiles <= 0) return FPHO_OK;
+    const Variant &V = kVariants[variant];
+    const size_t smem = tile_smem_bytes(variant, A.live_cap, A.pgrad_stride);
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    {
+        std::lock_guard<std::mutex> lk(g_attr_mu);
+        if (dev < 64 && g_attr_set[dev][variant] < smem) {
+            CUDA_TRY(cudaFuncSetAttribute(V.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)smem));
+            g_attr_set[dev][variant] = smem;
+        }
+    }
+    void *args[] = {(void *)&A};
+    CUDA_TRY(cudaLaunchKernel(V.fn, dim3(n_tiles), dim3(V.nt), args, smem, stream));
+    return FPHO_OK;
+}
+
+size_t tile_smem_bytes(int variant, int live_cap, int stride) {
+    return (size_t)live_cap * GREC * 4 + (size_t)live_cap * 8 +
+           (size_t)(kVariants[variant].nt / 32) * stride * 4;
+}
+
+}  // namespace fpho
+
+// ======================================================================= handle
+struct fpho_patch {
+    // host copies of the index arrays
+    int n_bands = 0, n_exp = 0, n_sources = 0, n_radii = 0;
+    int64_t npix = 0;
+    std::vector<int16_t> band_start, band_N;
+    std::vector<int> exposure_start, exposure_N, n_psf_per_source, psfgauss_start;
+    std::vector<int> exp_band, exp_npsf, gauss_start;
+    int n_gauss = 0;
+    int64_t n_psfrows = 0;
+    bool has_residual = false;
+    // device pixel + index arrays
+    float *d_data = nullptr, *d_ierr = nullptr, *d_xpix = nullptr, *d_ypix = nullptr,
+          *d_residual = nullptr;
+    int *d_exposure_start = nullptr, *d_exposure_N = nullptr;
+    int16_t *d_band_start = nullptr, *d_band_N = nullptr;
+    // device metadata
+    float *d_rad2 = nullptr, *d_D = nullptr, *d_crpix = nullptr, *d_crval = nullptr,
+          *d_CW = nullptr, *d_G = nullptr;
+    int *d_npsf = nullptr, *d_psfgauss_start = nullptr;
+    fpho_psfgauss *d_psfgauss = nullptr;
+    int *d_exp_band = nullptr, *d_exp_npsf = nullptr, *d_gauss_start = nullptr;
+    fpho_patch_struct *d_struct = nullptr;
+    // tile plan
+    int variant = 0, live_cap = 512, n_tiles = 0;
+    std::vector<int> tile_band_start;
+    fpho::TileDesc *d_tiles = nullptr;
+    float4 *d_tbox_all = nullptr, *d_tbox_w = nullptr;
+    int *d_tile_band_start = nullptr;
+    // workspace
+    float *d_gtab = nullptr;
+    float4 *d_gbox = nullptr;
+    double *d_pchi2 = nullptr;
+    float *d_pgrad = nullptr;
+    fpho_source *d_prop = nullptr;
+    double *d_chi2_out = nullptr;
+    float *d_dchi2_out = nullptr;
+    int d_dchi2_cap = 0;
+    int *d_err = nullptr;
+    long long *d_pairs = nullptr;
+    int count_pairs = 0;
+};
+
+namespace {
+
+template <typename T>
+int dalloc(T **p, size_t n) {
+    *p = nullptr;
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc((void **)p, n * sizeof(T));
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return set_error(FPHO_ERR_NOMEM, "cudaMalloc of %zu bytes failed: %s", n * sizeof(T),
+                         cudaGetErrorString(e));
+    }
+    return FPHO_OK;
+}
+template <typename T>
+void dfree(T *&p) {
+    if (p) cudaFree((void *)p);
+    p = nullptr;
+}
+template <typename T>
+int dupload(T **dst, const T *src, size_t n, cudaStream_t s) {
+    int rc = dalloc(dst, n);
+    if (rc) return rc;
+    if (n) CUDA_TRY(cudaMemcpyAsync(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice, s));
+    return FPHO_OK;
+}
+
+void free_meta(fpho_patch *p) {
+    dfree(p->d_rad2); dfree(p->d_D); dfree(p->d_crpix); dfree(p->d_crval); dfree(p->d_CW);
+    dfree(p->d_G); dfree(p->d_npsf); dfree(p->d_psfgauss_start); dfree(p->d_psfgauss);
+    dfree(p->d_exp_band); dfree(p->d_exp_npsf); dfree(p->d_gauss_start);
+    dfree(p->d_gtab); dfree(p->d_gbox); dfree(p->d_prop);
+}
+void free_plan(fpho_patch *p) {
+    dfree(p->d_tiles); dfree(p->d_tbox_all); dfree(p->d_tbox_w); dfree(p->d_tile_band_start);
+    dfree(p->d_pchi2); dfree(p->d_pgrad);
+}
+
+// Validate the index arrays of a host patch description and fill host copies.
+int read_pixel_index(fpho_patch *p, const fpho_patch_struct *h, int n_bands) {
+    if (!h) return set_error(FPHO_ERR_INVALID, "patch description is NULL");
+    if (n_bands < 1 || n_bands > FPHO_MAXBANDS)
+        return set_error(FPHO_ERR_LIMIT, "n_bands=%d outside [1, %d]", n_bands, FPHO_MAXBANDS);
+    if (!h->data || !h->ierr || !h->xpix || !h->ypix || !h->exposure_start || !h->exposure_N ||
+        !h->band_start || !h->band_N)
+        return set_error(FPHO_ERR_INVALID, "a pixel or index array pointer is NULL");
+    p->n_bands = n_bands;
+    p->band_start.assign(h->band_start, h->band_start + n_bands);
+    p->band_N.assign(h->band_N, h->band_N + n_bands);
+    int n_exp = 0;
+    for (int b = 0; b < n_bands; ++b) {
+        if (p->band_start[b] < 0 || p->band_N[b] < 0)
+            return set_error(FPHO_ERR_INVALID, "band %d: negative band_start/band_N", b);
+        n_exp = std::max(n_exp, (int)p->band_start[b] + (int)p->band_N[b]);
+    }
+    if (n_exp < 1) return set_error(FPHO_ERR_INVALID, "patch has no exposures");
+    p->n_exp = n_exp;
+    p->exposure_start.assign(h->exposure_start, h->exposure_start + n_exp);
+    p->exposure_N.assign(h->exposure_N, h->exposure_N + n_exp);
+    p->exp_band.assign(n_exp, -1);
+    for (int b = 0; b < n_bands; ++b)
+        for (int e = p->band_start[b]; e < p->band_start[b] + p->band_N[b]; ++e) {
+            if (p->exp_band[e] != -1)
+                return set_error(FPHO_ERR_INVALID, "exposure %d belongs to bands %d and %d", e,
+                                 p->exp_band[e], b);
+            p->exp_band[e] = b;
+        }
+    int64_t npix = 0;
+    for (int e = 0; e < n_exp; ++e) {
+        if (p->exposure_start[e] < 0 || p->exposure_N[e] < 0)
+            return set_error(FPHO_ERR_INVALID, "exposure %d: negative exposure_start/N", e);
+        npix = std::max<int64_t>(npix, (int64_t)p->exposure_start[e] + p->exposure_N[e]);
+    }
+    if (npix > (int64_t)INT32_MAX) return set_error(FPHO_ERR_LIMIT, "npix exceeds 2^31-1");
+    p->npix = npix;
+    return FPHO_OK;
+}
+
+// Validate and upload the per-scene metadata; derive the image-Gaussian index.
+int upload_meta(fpho_patch *p, const fpho_patch_struct *h, cudaStream_t s) {
+    if (!h->rad2 || !h->D || !h->crpix || !h->crval || !h->CW || !h->G || !h->n_psf_per_source ||
+        !h->psfgauss || !h->psfgauss_start)
+        return set_error(FPHO_ERR_INVALID, "a metadata array pointer is NULL");
+    const int nsrc = h->n_sources, nrad = h->n_radii;
+    if (nsrc < 1 || nsrc > FPHO_MAX_ACTIVE_SOURCES)
+        return set_error(FPHO_ERR_LIMIT, "n_sources=%d outside [1, %d]", nsrc,
+                         FPHO_MAX_ACTIVE_SOURCES);
+    if (nrad < 1 || nrad > FPHO_MAXRADII)
+        return set_error(FPHO_ERR_LIMIT, "n_radii=%d outside [1, %d]", nrad, FPHO_MAXRADII);
+    const int nb = p->n_bands, ne = p->n_exp;
+    std::vector<int> npsf(h->n_psf_per_source, h->n_psf_per_source + nb);
+    for (int b = 0; b < nb; ++b)
+        if (npsf[b] < 0 || npsf[b] > FPHO_MAX_PSF_PER_SOURCE)
+            return set_error(FPHO_ERR_LIMIT, "band %d: n_psf_per_source=%d outside [0, %d]", b,
+                             npsf[b], FPHO_MAX_PSF_PER_SOURCE);
+    std::vector<int> pstart(h->psfgauss_start, h->psfgauss_start + ne);
+    std::vector<int> exp_npsf(ne, 0), gstart(ne + 1, 0);
+    int64_t nrows = 0, ng = 0;
+    for (int e = 0; e < ne; ++e) {
+        const int b = p->exp_band[e];
+        exp_npsf[e] = (b >= 0) ? npsf[b] : 0;
+        if (exp_npsf[e] > 0) {
+            if (pstart[e] < 0) return set_error(FPHO_ERR_INVALID, "psfgauss_start[%d] < 0", e);
+            nrows = std::max<int64_t>(nrows, (int64_t)pstart[e] + exp_npsf[e]);
+        }
+        gstart[e] = (int)ng;
+        ng += (int64_t)nsrc * exp_npsf[e];
+        if (ng > (int64_t)INT32_MAX / 2)
+            return set_error(FPHO_ERR_LIMIT, "too many image Gaussians");
+    }
+    gstart[ne] = (int)ng;
+    for (int e = 0; e < ne; ++e)
+        for (int q = 0; q < exp_npsf[e]; ++q) {
+            const int k = h->psfgauss[pstart[e] + q].sersic_radius_bin;
+            if (k < 0 || k >= nrad)
+                return set_error(FPHO_ERR_INVALID,
+                                 "psfgauss[%d].sersic_radius_bin=%d outside [0, n_radii=%d)",
+                                 pstart[e] + q, k, nrad);
+        }
+    free_meta(p);
+    p->n_sources = nsrc;
+    p->n_radii = nrad;
+    p->n_psf_per_source = npsf;
+    p->psfgauss_start = pstart;
+    p->exp_npsf = exp_npsf;
+    p->gauss_start = gstart;
+    p->n_gauss = (int)ng;
+    p->n_psfrows = nrows;
+    const size_t es = (size_t)ne * nsrc;
+    int rc;
+    if ((rc = dupload(&p->d_rad2, h->rad2, nrad, s))) return rc;
+    if ((rc = dupload(&p->d_D, h->D, es * 4, s))) return rc;
+    if ((rc = dupload(&p->d_CW, h->CW, es * 4, s))) return rc;
+    if ((rc = dupload(&p->d_crpix, h->crpix, es * 2, s))) return rc;
+    if ((rc = dupload(&p->d_crval, h->crval, es * 2, s))) return rc;
+    if ((rc = dupload(&p->d_G, h->G, (size_t)ne, s))) return rc;
+    if ((rc = dupload(&p->d_npsf, npsf.data(), (size_t)nb, s))) return rc;
+    if ((rc = dupload(&p->d_psfgauss_start, pstart.data(), (size_t)ne, s))) return rc;
+    if ((rc = dupload(&p->d_psfgauss, h->psfgauss, (size_t)nrows, s))) return rc;
+    if ((rc = dupload(&p->d_exp_band, p->exp_band.data(), (size_t)ne, s))) return rc;
+    if ((rc = dupload(&p->d_exp_npsf, exp_npsf.data(), (size_t)ne, s))) return rc;
+    if ((rc = dupload(&p->d_gauss_start, gstart.data(), (size_t)ne + 1, s))) return rc;
+    if ((rc = dalloc(&p->d_gtab, (size_t)ng * GREC))) return rc;
+    if ((rc = dalloc(&p->d_gbox, (size_t)ng))) return rc;
+    if ((rc = dalloc(&p->d_prop, (size_t)nsrc))) return rc;
+    // metadata arrays are read from host memory by the async copies above
+    CUDA_TRY(cudaStreamSynchronize(s));
+    return FPHO_OK;
+}
+
+int build_plan(fpho_patch *p, cudaStream_t s);
+
+int refresh_struct(fpho_patch *p, cudaStream_t s) {
+    fpho_patch_struct hs;
+    memset(&hs, 0, sizeof(hs));
+    hs.data = p->d_data; hs.ierr = p->d_ierr; hs.xpix = p->d_xpix; hs.ypix = p->d_ypix;
+    hs.residual = p->d_residual;
+    hs.exposure_start = p->d_exposure_start; hs.exposure_N = p->d_exposure_N;
+    hs.band_start = p->d_band_start; hs.band_N = p->d_band_N;
+    hs.n_sources = p->n_sources; hs.n_radii = p->n_radii;
+    hs.rad2 = p->d_rad2; hs.D = p->d_D; hs.crpix = p->d_crpix; hs.crval = p->d_crval;
+    hs.CW = p->d_CW; hs.G = p->d_G; hs.n_psf_per_source = p->d_npsf;
+    hs.psfgauss = p->d_psfgauss; hs.psfgauss_start = p->d_psfgauss_start;
+    if (!p->d_struct) {
+        int rc = dalloc(&p->d_struct, 1);
+        if (rc) return rc;
+    }
+    CUDA_TRY(cudaMemcpyAsync(p->d_struct, &hs, sizeof(hs), cudaMemcpyHostToDevice, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    return FPHO_OK;
+}
+
+}  // namespace
+
+namespace fpho {
+
+PatchView make_view(const fpho_patch *p) {
+    PatchView v;
+    v.data = p->d_data; v.ierr = p->d_ierr; v.xpix = p->d_xpix; v.ypix = p->d_ypix;
+    v.residual = p->d_residual;
+    v.rad2 = p->d_rad2; v.D = p->d_D; v.crpix = p->d_crpix; v.crval = p->d_crval;
+    v.CW = p->d_CW; v.G = p->d_G;
+    v.psfgauss = p->d_psfgauss; v.psfgauss_start = p->d_psfgauss_start;
+    v.exp_band = p->d_exp_band; v.exp_npsf = p->d_exp_npsf; v.gauss_start = p->d_gauss_start;
+    v.n_sources = p->n_sources; v.n_exp = p->n_exp; v.n_bands = p->n_bands;
+    v.n_radii = p->n_radii;
+    return v;
+}
+
+}  // namespace fpho
+
+namespace {
+
+int build_plan(fpho_patch *p, cudaStream_t s) {
+    free_plan(p);
+    const int tp = variant_tile_pixels(p->variant);
+    std::vector<TileDesc> tiles;
+    p->tile_band_start.assign(p->n_bands + 1, 0);
+    for (int b = 0; b < p->n_bands; ++b) {
+        p->tile_band_start[b] = (int)tiles.size();
+        for (int e = p->band_start[b]; e < p->band_start[b] + p->band_N[b]; ++e) {
+            const int n = p->exposure_N[e];
+            for (int off = 0; off < n; off += tp)
+                tiles.push_back({e, b, p->exposure_start[e] + off, std::min(tp, n - off)});
+        }
+    }
+    p->tile_band_start[p->n_bands] = (int)tiles.size();
+    p->n_tiles = (int)tiles.size();
+    int rc;
+    if ((rc = dupload(&p->d_tiles, tiles.data(), tiles.size(), s))) return rc;
+    if ((rc = dupload(&p->d_tile_band_start, p->tile_band_start.data(),
+                      p->tile_band_start.size(), s)))
+        return rc;
+    if ((rc = dalloc(&p->d_tbox_all, tiles.size()))) return rc;
+    if ((rc = dalloc(&p->d_tbox_w, tiles.size()))) return rc;
+    if ((rc = dalloc(&p->d_pchi2, tiles.size()))) return rc;
+    if ((rc = dalloc(&p->d_pgrad, tiles.size() * (size_t)7 * p->n_sources))) return rc;
+    if (p->n_tiles > 0) {
+        tile_bboxes<<<p->n_tiles, 128, 0, s>>>(make_view(p), p->d_tiles, p->d_tbox_all,
+                                              p->d_tbox_w);
+        CUDA_TRY(cudaGetLastError());
+    }
+    CUDA_TRY(cudaStreamSynchronize(s));
+    return FPHO_OK;
+}
+
+}  // namespace
+
+// ======================================================================= C ABI
+extern "C" int fpho_patch_create(const fpho_patch_struct *host, int n_bands, int return_residual,
+                                 void *stream, fpho_patch **out) {
+    clear_error();
+    if (!out) return set_error(FPHO_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    cudaStream_t s = (cudaStream_t)stream;
+    fpho_patch *p = new (std::nothrow) fpho_patch();
+    if (!p) return set_error(FPHO_ERR_NOMEM, "host allocation failed");
+    int rc = read_pixel_index(p, host, n_bands);
+    if (!rc) {
+        const size_t np = (size_t)p->npix;
+        if (!rc) rc = dupload(&p->d_data, host->data, np, s);
+        if (!rc) rc = dupload(&p->d_ierr, host->ierr, np, s);
+        if (!rc) rc = dupload(&p->d_xpix, host->xpix, np, s);
+        if (!rc) rc = dupload(&p->d_ypix, host->ypix, np, s);
+        if (!rc) rc = dupload(&p->d_exposure_start, p->exposure_start.data(), (size_t)p->n_exp, s);
+        if (!rc) rc = dupload(&p->d_exposure_N, p->exposure_N.data(), (size_t)p->n_exp, s);
+        if (!rc) rc = dupload(&p->d_band_start, p->band_start.data(), (size_t)p->n_bands, s);
+        if (!rc) rc = dupload(&p->d_band_N, p->band_N.data(), (size_t)p->n_bands, s);
+        if (!rc && return_residual) {
+            rc = dalloc(&p->d_residual, np);
+            if (!rc && cudaMemsetAsync(p->d_residual, 0, np * sizeof(float), s) != cudaSuccess)
+                rc = set_error(FPHO_ERR_CUDA, "cudaMemsetAsync failed");
+            p->has_residual = true;
+        }
+    }
+    if (!rc) rc = upload_meta(p, host, s);
+    if (!rc) rc = dalloc(&p->d_chi2_out, (size_t)p->n_bands);
+    if (!rc) rc = dalloc(&p->d_err, 1);
+    if (!rc) rc = dalloc(&p->d_pairs, 1);
+    if (!rc) rc = build_plan(p, s);
+    if (!rc) rc = refresh_struct(p, s);
+    if (rc) {
+        fpho_patch_free(p);
+        return rc;
+    }
+    *out = p;
+    return FPHO_OK;
+}
+
+extern "C" int fpho_patch_replace_meta(fpho_patch *p, const fpho_patch_struct *host, void *stream) {
+    clear_error();
+    if (!p || !host) return set_error(FPHO_ERR_INVALID, "NULL argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    const int old_nsrc = p->n_sources;
+    int rc = upload_meta(p, host, s);
+    if (rc) return rc;
+    if (p->n_sources != old_nsrc) {
+        dfree(p->d_pgrad);
+        if ((rc = dalloc(&p->d_pgrad, (size_t)std::max(p->n_tiles, 1) * 7 * p->n_sources)))
+            return rc;
+    }
+    return refresh_struct(p, s);
+}
+
+extern "C" int fpho_patch_swap_data_residual(fpho_patch *p, void *stream) {
+    clear_error();
+    if (!p) return set_error(FPHO_ERR_INVALID, "NULL patch");
+    if (!p->has_residual)
+        return set_error(FPHO_ERR_STATE, "patch was created without a residual array");
+    std::swap(p->d_data, p->d_residual);
+    return refresh_struct(p, (cudaStream_t)stream);
+}
+
+extern "C" int fpho_patch_retrieve(fpho_patch *p, int which, float *host_out, void *stream) {
+    clear_error();
+    if (!p || !host_out) return set_error(FPHO_ERR_INVALID, "NULL argument");
+    const float *src = nullptr;
+    switch (which) {
+        case 0: src = p->d_data; break;
+        case 1: src = p->d_residual; break;
+        case 2: src = p->d_ierr; break;
+        case 3: src = p->d_xpix; break;
+        case 4: src = p->d_ypix; break;
+        default: return set_error(FPHO_ERR_INVALID, "which=%d not in 0..4", which);
+    }
+    if (!src) return set_error(FPHO_ERR_STATE, "array %d is not allocated", which);
+    cudaStream_t s = (cudaStream_t)stream;
+    CUDA_TRY(cudaMemcpyAsync(host_out, src, (size_t)p->npix * sizeof(float),
+                             cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    return FPHO_OK;
+}
+
+extern "C" int fpho_patch_device_struct(fpho_patch *p, const void **dev_struct) {
+    clear_error();
+    if (!p || !dev_struct) return set_error(FPHO_ERR_INVALID, "NULL argument");
+    *dev_struct = p->d_struct;
+    return FPHO_OK;
+}
+
+extern "C" int fpho_patch_info(const fpho_patch *p, int64_t out[7]) {
+    clear_error();
+    if (!p || !out) return set_error(FPHO_ERR_INVALID, "NULL argument");
+    out[0] = p->n_bands; out[1] = p->n_exp; out[2] = p->npix; out[3] = p->n_sources;
+    out[4] = p->n_radii; out[5] = p->n_tiles; out[6] = p->n_gauss;
+    return FPHO_OK;
+}
+
+extern "C" int fpho_patch_free(fpho_patch *p) {
+    clear_error();
+    if (!p) return FPHO_OK;
+    free_meta(p);
+    free_plan(p);
+    dfree(p->d_data); dfree(p->d_ierr); dfree(p->d_xpix); dfree(p->d_ypix); dfree(p->d_residual);
+    dfree(p->d_exposure_start); dfree(p->d_exposure_N); dfree(p->d_band_start);
+    dfree(p->d_band_N); dfree(p->d_struct); dfree(p->d_chi2_out); dfree(p->d_dchi2_out);
+    dfree(p->d_err); dfree(p->d_pairs);
+    delete p;
+    return FPHO_OK;
+}
+
+// ------------------------------------------------------------ tuning hooks
+extern "C" int fpho_patch_set_config(fpho_patch *p, int variant, int live_cap, void *stream) {
+    clear_error();
+    if (!p) return set_error(FPHO_ERR_INVALID, "NULL patch");
+    if (variant < 0 || variant >= variant_count())
+        return set_error(FPHO_ERR_INVALID, "variant %d not in [0, %d)", variant, variant_count());
+    const int nt = variant_threads(variant);
+    if (live_cap < nt || live_cap > 4096)
+        return set_error(FPHO_ERR_INVALID, "live_cap %d outside [%d, 4096]", live_cap, nt);
+    if (tile_smem_bytes(variant, live_cap, 7 * p->n_sources) > 227 * 1024)
+        return set_error(FPHO_ERR_LIMIT, "shared memory for live_cap %d exceeds 227 KB",
+                         live_cap);
+    const bool replan = variant_tile_pixels(variant) != variant_tile_pixels(p->variant);
+    p->variant = variant;
+    p->live_cap = live_cap;
+    if (replan) return build_plan(p, (cudaStream_t)stream);
+    return FPHO_OK;
+}
+
+extern "C" int fpho_variant_info(int variant, int out[2]) {
+    clear_error();
+    if (variant < 0 || variant >= variant_count() || !out)
+        return set_error(FPHO_ERR_INVALID, "bad variant");
+    out[0] = variant_threads(variant);
+    out[1] = variant_tile_pixels(variant) / variant_threads(variant);
+    return variant_count();
+}
+
+extern "C" int fpho_patch_count_pairs(fpho_patch *p, int enable, long long *last_count) {
+    clear_error();
+    if (!p) return set_error(FPHO_ERR_INVALID, "NULL patch");
+    p->count_pairs = enable;
+    if (last_count) {
+        long long v = 0;
+        CUDA_TRY(cudaMemcpy(&v, p->d_pairs, sizeof(v), cudaMemcpyDeviceToHost));
+        *last_count = v;
+    }
+    return FPHO_OK;
+}
+
+namespace fpho {
+
+// Enqueue one evaluation with device-resident proposal and outputs.
+int enqueue_evaluate(fpho_patch *p, const fpho_source *d_prop, double *d_chi2, float *d_dchi2,
+                     int out_stride, bool want_residual, cudaStream_t s) {
+    if (want_residual && !p->d_residual)
+        return set_error(FPHO_ERR_STATE,
+                         "residual requested but the patch was created without one");
+    CUDA_TRY(cudaMemsetAsync(p->d_err, 0, sizeof(int), s));
+    if (p->count_pairs) CUDA_TRY(cudaMemsetAsync(p->d_pairs, 0, sizeof(long long), s));
+    const PatchView pv = make_view(p);
+    int max_g = 0;
+    for (int e = 0; e < p->n_exp; ++e)
+        max_g = std::max(max_g, p->gauss_start[e + 1] - p->gauss_start[e]);
+    if (max_g > 0) {
+        dim3 grid((max_g + 127) / 128, p->n_exp);
+        build_image_gaussians<<<grid, 128, 0, s>>>(pv, d_prop, p->d_gtab, p->d_gbox);
+        CUDA_TRY(cudaGetLastError());
+    }
+    TileArgs A;
+    A.pv = pv;
+    A.tiles = p->d_tiles;
+    A.tbox_all = p->d_tbox_all;
+    A.tbox_w = p->d_tbox_w;
+    A.gtab = p->d_gtab;
+    A.gbox = p->d_gbox;
+    A.pchi2 = p->d_pchi2;
+    A.pgrad = p->d_pgrad;
+    A.pgrad_stride = 7 * p->n_sources;
+    A.want_residual = want_residual ? 1 : 0;
+    A.live_cap = p->live_cap;
+    A.err = p->d_err;
+    A.pairs = p->count_pairs ? p->d_pairs : nullptr;
+    int rc = launch_tile_kernel(p->variant, A, p->n_tiles, s);
+    if (rc) return rc;
+    dim3 rg(p->n_bands, (out_stride + 127) / 128);
+    reduce_bands<<<rg, 128, 0, s>>>(p->d_tile_band_start, p->d_pchi2, p->d_pgrad,
+                                    7 * p->n_sources, d_chi2, d_dchi2, out_stride);
+    CUDA_TRY(cudaGetLastError());
+    return FPHO_OK;
+}
+
+}  // namespace fpho
+
+extern "C" int fpho_evaluate_proposal(fpho_patch *p, const fpho_source *proposal, int n_sources,
+                                      double *chi2, float *dchi2, int dchi2_stride,
+                                      unsigned flags, void *stream) {
+    clear_error();
+    if (!p || !proposal || !chi2 || !dchi2) return set_error(FPHO_ERR_INVALID, "NULL argument");
+    if (n_sources != p->n_sources)
+        return set_error(FPHO_ERR_INVALID, "n_sources=%d but the patch has %d", n_sources,
+                         p->n_sources);
+    if (dchi2_stride < 7 * n_sources)
+        return set_error(FPHO_ERR_INVALID, "dchi2_stride=%d < 7*n_sources=%d", dchi2_stride,
+                         7 * n_sources);
+    cudaStream_t s = (cudaStream_t)stream;
+    const bool host_io = (flags & FPHO_IO_HOST) != 0;
+    const bool want_res = (flags & FPHO_WANT_RESIDUAL) != 0;
+    if (!host_io) return enqueue_evaluate(p, proposal, chi2, dchi2, dchi2_stride, want_res, s);
+
+    const size_t gbytes = (size_t)p->n_bands * dchi2_stride;
+    if (p->d_dchi2_cap < (int)gbytes) {
+        dfree(p->d_dchi2_out);
+        int rc = dalloc(&p->d_dchi2_out, gbytes);
+        if (rc) return rc;
+        p->d_dchi2_cap = (int)gbytes;
+    }
+    CUDA_TRY(cudaMemcpyAsync(p->d_prop, proposal, sizeof(fpho_source) * n_sources,
+                             cudaMemcpyHostToDevice, s));
+    int rc = enqueue_evaluate(p, p->d_prop, p->d_chi2_out, p->d_dchi2_out, dchi2_stride,
+                              want_res, s);
+    if (rc) return rc;
+    int err = 0;
+    CUDA_TRY(cudaMemcpyAsync(chi2, p->d_chi2_out, sizeof(double) * p->n_bands,
+                             cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaMemcpyAsync(dchi2, p->d_dchi2_out, sizeof(float) * gbytes,
+                             cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaMemcpyAsync(&err, p->d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    if (err) return set_error(FPHO_ERR_KERNEL, "tile kernel reported error word 0x%x", err);
+    return FPHO_OK;
+}
+
+extern "C" int fpho_EvaluateProposal(fpho_patch *p, const void *dev_patch_struct,
+                                     const void *dev_proposal, void *pchi2, void *pdchi2_dp,
+                                     void *stream) {
+    clear_error();
+    if (!p || !dev_proposal || !pchi2 || !pdchi2_dp)
+        return set_error(FPHO_ERR_INVALID, "NULL argument");
+    if (dev_patch_struct != (const void *)p->d_struct)
+        return set_error(FPHO_ERR_INVALID,
+                         "dev_patch_struct is not the device struct of this patch handle");
+    if (p->n_sources > FPHO_MAXSOURCES)
+        return set_error(FPHO_ERR_LIMIT,
+                         "the Response layout holds %d sources; use fpho_evaluate_proposal",
+                         FPHO_MAXSOURCES);
+    return enqueue_evaluate(p, (const fpho_source *)dev_proposal, (double *)pchi2,
+                            (float *)pdchi2_dp, FPHO_MAXSOURCES * FPHO_NPARAMS,
+                            p->d_residual != nullptr, (cudaStream_t)stream);
+}
+
+extern "C" int fpho_patch_error_word(fpho_patch *p, int *out) {
+    clear_error();
+    if (!p || !out) return set_error(FPHO_ERR_INVALID, "NULL argument");
+    CUDA_TRY(cudaMemcpy(out, p->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    return FPHO_OK;
+}

@@ -1,0 +1,215 @@
+// fpho_impl.cuh -- internals shared by the forcepho_b200 CUDA translation units.
+//
+// Device-side layout (all per evaluation, owned by a patch handle):
+//   gtab  float[n_gauss][32]  one 128-byte record per image Gaussian
+//                             (exposure-major, then source, then PSF component),
+//                             written by build_image_gaussians and staged into
+//                             shared memory per tile by bulk copies;
+//   gbox  float4[n_gauss]     axis-aligned box enclosing the Gaussian's
+//                             exp-argument <= 36 ellipse (plus a safety margin),
+//                             used to cull Gaussians per pixel tile.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fpho.h"
+
+namespace fpho {
+
+// ---------------------------------------------------------------- records
+constexpr int GREC = 32;  // floats per image-Gaussian record
+enum RecField : int {
+    R_NXC = 0, R_NYC = 1, R_FXX = 2, R_FXY = 3,      // -xcen, -ycen, F11, F21
+    R_FYY = 4, R_HA = 5, R_HB = 6, R_C0 = 7,          // F22, -amp/24, -amp*c0, c0
+    R_SRC = 8, R_AMP = 9, R_SXX = 10, R_SYY = 11,     // source (int bits), amp, Sigma11, Sigma22
+    // Jacobian of (A, x, y, fxx, fyy, fxy) w.r.t. (flux, ra, dec, q, pa, n, rh);
+    // rows acting on x, y and F are pre-multiplied by amp (see tile kernel).
+    R_JA_FLUX = 12, R_JA_Q = 13, R_JA_PA = 14, R_JA_N = 15,
+    R_JA_RH = 16, R_JX_RA = 17, R_JY_RA = 18, R_JX_DEC = 19,
+    R_JY_DEC = 20, R_JFXX_Q = 21, R_JFXY_Q = 22, R_JFYY_Q = 23,
+    R_JFXX_PA = 24, R_JFXY_PA = 25, R_JFYY_PA = 26,
+    // 27..31 unused
+};
+// c0 = 1 - (fxx + fyy)/24, so that H = 1 + (|v|^2 - fxx - fyy)/24 = |v|^2/24 + c0.
+
+// Culling margin on the half-widths of the exp-argument <= 36 ellipse.  The
+// per-pixel exp-argument is computed in float from F; its error relative to the
+// exact quadratic form is a few ulp times the condition number of F (< 1e-4
+// here), so a 1e-3 relative plus 1e-3 pixel widening keeps the box conservative.
+constexpr float CULL_REL = 1.0e-3f;
+constexpr float CULL_ABS = 1.0e-3f;
+
+// ---------------------------------------------------------------- views
+// Device pointers of one patch, passed to kernels by value.
+struct PatchView {
+    const float *data, *ierr, *xpix, *ypix;
+    float *residual;
+    const float *rad2, *D, *crpix, *crval, *CW, *G;
+    const fpho_psfgauss *psfgauss;
+    const int *psfgauss_start;
+    const int *exp_band;     // [n_exp] band of each exposure (-1: none)
+    const int *exp_npsf;     // [n_exp] PSF components per source in that band
+    const int *gauss_start;  // [n_exp + 1] first image Gaussian of each exposure
+    int n_sources, n_exp, n_bands, n_radii;
+};
+
+// One pixel tile: a contiguous run of at most TILE pixels of one exposure.
+struct TileDesc {
+    int exposure;
+    int band;
+    int pix_begin;  // index into the patch pixel arrays
+    int count;      // valid pixels (<= tile size)
+};
+
+// ---------------------------------------------------------------- 2x2 algebra
+// Row-major 2x2 matrix (a b / c d), the operations of forcepho/src/matrix22.cc.
+struct M22 {
+    float a, b, c, d;
+};
+__host__ __device__ __forceinline__ M22 mmul(M22 A, M22 B) {
+    return {A.a * B.a + A.b * B.c, A.a * B.b + A.b * B.d, A.c * B.a + A.d * B.c,
+            A.c * B.b + A.d * B.d};
+}
+__host__ __device__ __forceinline__ M22 mscal(float s, M22 A) {
+    return {s * A.a, s * A.b, s * A.c, s * A.d};
+}
+
+// Build image Gaussian (exposure e, source s, PSF component p): sky Gaussian of
+// radius bin k convolved with PSF Gaussian p, with its Jacobian.
+// Follows GetGaussianAndJacobian (forcepho/src/common_kernel.cc:175-240) and
+// ConvolveOneSource (forcepho/src/compute_gaussians_kernel.cc:45-114),
+// including the PSF row index psfgauss[psfgauss_start[e] + p] used for every
+// source.  Writes one record and one culling box.
+__device__ __forceinline__ void build_one_gaussian(const PatchView &pv, const fpho_source *src,
+                                                   int e, int s, int p, float *rec, float4 *box) {
+    const int band = pv.exp_band[e];
+    const fpho_source &gal = src[s];
+    const fpho_psfgauss pg = pv.psfgauss[pv.psfgauss_start[e] + p];
+    const int k = pg.sersic_radius_bin;
+    const int dcw = 4 * (pv.n_sources * e + s);
+    const int cr = 2 * (pv.n_sources * e + s);
+
+    const float G = pv.G[e];
+    const float q = gal.q;
+    float sn, cs;
+    sincosf(gal.pa, &sn, &cs);
+    const M22 D = {pv.D[dcw], pv.D[dcw + 1], pv.D[dcw + 2], pv.D[dcw + 3]};
+    const M22 R = {cs, -sn, sn, cs};
+    const M22 S = {1.0f / q, 0.0f, 0.0f, q};
+    const M22 dS = {-1.0f / (q * q), 0.0f, 0.0f, 1.0f};
+    const M22 dR = {-sn, -cs, cs, -sn};
+    const M22 DR = mmul(D, R);
+    const M22 T = mmul(DR, S);
+    const M22 dTq = mmul(DR, dS);
+    const M22 dTpa = mmul(mmul(D, dR), S);
+    const M22 CW = {pv.CW[dcw], pv.CW[dcw + 1], pv.CW[dcw + 2], pv.CW[dcw + 3]};
+    const float s0 = gal.ra - pv.crval[cr];
+    const float s1 = gal.dec - pv.crval[cr + 1];
+    const float xs = CW.a * s0 + CW.b * s1 + pv.crpix[cr];
+    const float ys = CW.c * s0 + CW.d * s1 + pv.crpix[cr + 1];
+
+    const float r2 = pv.rad2[k];
+    const float samp = gal.mixture_amplitudes[k];
+    const float flux = gal.fluxes[band];
+
+    // Sigma = r2 T T^t + C_psf ; F = Sigma^-1
+    const float t12 = T.a * T.c + T.b * T.d;
+    const M22 Sig = {r2 * (T.a * T.a + T.b * T.b) + pg.Cxx, r2 * t12 + pg.Cxy,
+                     r2 * t12 + pg.Cxy, r2 * (T.c * T.c + T.d * T.d) + pg.Cyy};
+    const float idet = 1.0f / (Sig.a * Sig.d - Sig.b * Sig.c);
+    const M22 F = {Sig.d * idet, -Sig.b * idet, -Sig.c * idet, Sig.a * idet};
+    const float detF = F.a * F.d - F.b * F.c;
+    const float tmp = G * pg.amp * sqrtf(detF) * (1.0f / (2.0f * 3.14159265358979323846f));
+    const float amp = tmp * flux * samp;
+
+    // dSigma/dq = r2 (T dT^t + dT T^t), dF = -F dSigma F, dA = amp/2 tr(Sigma dF)
+    float jF[2][3], jA[2];
+    {
+        const M22 dTs[2] = {dTq, dTpa};
+#pragma unroll
+        for (int w = 0; w < 2; ++w) {
+            const M22 B = dTs[w];
+            const float o = T.a * B.c + T.b * B.d + T.c * B.a + T.d * B.b;
+            const M22 dSig = mscal(r2, M22{2.0f * (T.a * B.a + T.b * B.b), o, o,
+                                           2.0f * (T.c * B.c + T.d * B.d)});
+            const M22 dF = mscal(-1.0f, mmul(mmul(F, dSig), F));
+            const M22 M = mmul(Sig, dF);
+            jA[w] = 0.5f * amp * (M.a + M.d);
+            jF[w][0] = dF.a;  // fxx
+            jF[w][1] = dF.c;  // fxy
+            jF[w][2] = dF.d;  // fyy
+        }
+    }
+
+    const float xc = xs + pg.xcen;
+    const float yc = ys + pg.ycen;
+    const float c0 = 1.0f - (F.a + F.d) * (1.0f / 24.0f);
+
+    float4 *r4 = reinterpret_cast<float4 *>(rec);
+    r4[0] = make_float4(-xc, -yc, F.a, F.c);
+    r4[1] = make_float4(F.d, -amp * (1.0f / 24.0f), -amp * c0, c0);
+    r4[2] = make_float4(__int_as_float(s), amp, Sig.a, Sig.d);
+    r4[3] = make_float4(tmp * samp, jA[0], jA[1], tmp * flux * gal.damplitude_dnsersic[k]);
+    r4[4] = make_float4(tmp * flux * gal.damplitude_drh[k], amp * CW.a, amp * CW.c, amp * CW.b);
+    r4[5] = make_float4(amp * CW.d, amp * jF[0][0], amp * jF[0][1], amp * jF[0][2]);
+    r4[6] = make_float4(amp * jF[1][0], amp * jF[1][1], amp * jF[1][2], 0.0f);
+    r4[7] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+
+    // exp-argument <= 36 ellipse: half-widths 6 sqrt(Sigma11), 6 sqrt(Sigma22)
+    const float wx = 6.0f * sqrtf(fmaxf(Sig.a, 0.0f)) * (1.0f + CULL_REL) + CULL_ABS;
+    const float wy = 6.0f * sqrtf(fmaxf(Sig.d, 0.0f)) * (1.0f + CULL_REL) + CULL_ABS;
+    *box = make_float4(xc - wx, xc + wx, yc - wy, yc + wy);
+}
+
+// ---------------------------------------------------------------- packed f32x2
+// Two pixels per register pair: sm_100 executes add/mul/fma on .f32x2 operands
+// as one instruction.  Values are carried as 64-bit integers holding {lo, hi}.
+typedef unsigned long long v2;
+
+__device__ __forceinline__ v2 pk(float lo, float hi) {
+    v2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ v2 pk1(float x) { return pk(x, x); }
+__device__ __forceinline__ float lo(v2 v) {
+    float a, b;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+    return a;
+}
+__device__ __forceinline__ float hi(v2 v) {
+    float a, b;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+    return b;
+}
+__device__ __forceinline__ void unpk(v2 v, float &a, float &b) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+}
+__device__ __forceinline__ v2 add2(v2 a, v2 b) {
+    v2 d;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ v2 mul2(v2 a, v2 b) {
+    v2 d;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(d) : "l"(a), "l"(b));
+    return d;
+}
+__device__ __forceinline__ v2 fma2(v2 a, v2 b, v2 c) {
+    v2 d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+
+// 2^x on the SFU (MUFU.EX2), flush-to-zero: inputs below -126 give 0.
+__device__ __forceinline__ float ex2f(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// -0.5 * log2(e): exp(-Q/2) = 2^(Q * KEXP)
+constexpr float KEXP = -0.72134752044448170368f;
+
+}  // namespace fpho

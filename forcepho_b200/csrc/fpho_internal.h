@@ -1,0 +1,29 @@
+// fpho_internal.h -- host-side helpers shared by the forcepho_b200 translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+
+#include "fpho.h"
+
+struct fpho_patch;
+
+namespace fpho {
+
+struct PatchView;
+struct TileArgs;
+
+// Record a failure message for fpho_last_error() and return `code`.
+int set_error(int code, const char *fmt, ...);
+void clear_error();
+
+// Tile-kernel variants (threads per CTA x pixels per thread).
+int variant_count();
+int variant_tile_pixels(int v);
+int variant_threads(int v);
+size_t tile_smem_bytes(int variant, int live_cap, int stride);
+int launch_tile_kernel(int variant, const TileArgs &A, int n_tiles, cudaStream_t stream);
+
+PatchView make_view(const fpho_patch *p);
+
+}  // namespace fpho

@@ -1,0 +1,449 @@
+// fpho_tile.cuh -- the pixel-tile kernel body shared by the single-patch and
+// the batched evaluation.
+//
+// One CTA evaluates one tile of up to NT*K pixels of one exposure:
+//   1. cull: keep the exposure's image Gaussians whose exp-argument <= 36 box
+//      overlaps the tile's pixel bounding box (provably equivalent to the
+//      reference's per-pixel `exparg > 36` skip, which is still applied to
+//      every Gaussian that can cross the threshold inside the tile);
+//   2. stage the kept 128-byte records into shared memory with cp.async.bulk
+//      (one bulk copy per record, completion on an mbarrier);
+//   3. residual pass: r = data - sum_g amp G H over kept Gaussians, in the
+//      reference's Gaussian order (ComputeResidualImage, common_kernel.cc:57-83);
+//   4. chi2 per pixel in double, exactly as compute_gaussians_kernel.cc:286-293;
+//   5. gradient pass: for each kept Gaussian, each thread accumulates the
+//      derivatives of its pixels' model w.r.t. the Gaussian's image-space
+//      parameters (A, x, y, fxx, fyy, fxy), then applies the Gaussian's
+//      Jacobian once (ComputeGaussianDerivative, common_kernel.cc:95-143, with
+//      the per-pixel Jacobian product moved out of the pixel loop);
+//   6. per-source sums are reduced across the warp and the CTA in a fixed
+//      order and written as this tile's partial; chi2 partials stay double.
+// Pixel pairs are processed as packed .f32x2 operands (two pixels per
+// instruction).
+#pragma once
+
+#include "fpho_impl.cuh"
+
+namespace fpho {
+
+struct TileArgs {
+    PatchView pv;
+    const TileDesc *tiles;
+    const float4 *tbox_all;   // per tile bounding box of all pixels (x0, x1, y0, y1)
+    const float4 *tbox_w;     // per tile bounding box of pixels with ierr != 0
+    const float *gtab;        // image-Gaussian records
+    const float4 *gbox;       // culling boxes
+    double *pchi2;            // [n_tiles] chi2 partial per tile
+    float *pgrad;             // [n_tiles][pgrad_stride] gradient partial per tile
+    int pgrad_stride;         // 7 * n_sources
+    int want_residual;
+    int live_cap;             // records that fit in the shared-memory stage (>= NT)
+    int *err;                 // error word (bit 0: bulk-copy wait gave up)
+    long long *pairs;         // optional: evaluated (pixel, Gaussian) pairs, or nullptr
+};
+
+// ------------------------------------------------------------ mbarrier + bulk copy
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+__device__ __forceinline__ void bulk_g2s(void *dst_smem, const void *src_gmem, uint32_t bytes,
+                                         uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+            smem_u32(dst_smem)),
+        "l"(src_gmem), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+__device__ __forceinline__ void fence_proxy_async_smem() {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// Bounded wait on an mbarrier phase.  Gives up after `limit` polls, records
+// bit 0 in the error word and returns false; never spins forever.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, int *err) {
+    const int limit = 1 << 22;
+    for (int i = 0; i < limit; ++i)
+        if (mbar_try_wait(bar, parity)) return true;
+    atomicOr(err, 1);
+    return false;
+}
+
+// ------------------------------------------------------------ warp helpers
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Reduce 7 per-lane values across the warp; afterwards lane k (k < 7) holds
+// the warp total of value k.  Uses 4+2+1+1+1 shuffles instead of 7*5.
+__device__ __forceinline__ float warp_reduce7(float v[8], int lane) {
+    // round 1: lanes < 16 keep 0..3, lanes >= 16 keep 4..7
+    {
+        const bool up = lane & 16;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const float send = up ? v[i] : v[i + 4];
+            const float keep = up ? v[i + 4] : v[i];
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 16);
+        }
+    }
+    {
+        const bool up = lane & 8;
+#pragma unroll
+        for (int i = 0; i < 2; ++i) {
+            const float send = up ? v[i] : v[i + 2];
+            const float keep = up ? v[i + 2] : v[i];
+            v[i] = keep + __shfl_xor_sync(0xffffffffu, send, 8);
+        }
+    }
+    {
+        const bool up = lane & 4;
+        const float send = up ? v[0] : v[1];
+        const float keep = up ? v[1] : v[0];
+        v[0] = keep + __shfl_xor_sync(0xffffffffu, send, 4);
+    }
+    v[0] += __shfl_xor_sync(0xffffffffu, v[0], 2);
+    v[0] += __shfl_xor_sync(0xffffffffu, v[0], 1);
+    // value index held by this lane group: bits (16 -> 4, 8 -> 2, 4 -> 1)
+    return v[0];
+}
+__device__ __forceinline__ int reduce7_index(int lane) {
+    return ((lane >> 4) & 1) * 4 + ((lane >> 3) & 1) * 2 + ((lane >> 2) & 1);
+}
+
+// ------------------------------------------------------------ shared layout
+template <int NT>
+struct TileSmem {
+    static constexpr int NW = NT / 32;
+    // dynamic shared memory: [recs live_cap*128 B][live_idx live_cap*4][live_flag live_cap*4]
+    //                        [wacc NW*stride*4]
+    static __host__ __device__ size_t bytes(int live_cap, int stride) {
+        return (size_t)live_cap * GREC * 4 + (size_t)live_cap * 8 + (size_t)NW * stride * 4;
+    }
+};
+
+// ------------------------------------------------------------ the tile body
+template <int NT, int K>
+__device__ __forceinline__ void tile_body(const TileArgs &A, int tile, unsigned char *smem,
+                                          uint64_t *mbar, uint32_t &phase) {
+    static_assert(K % 2 == 0, "pixels per thread must be even (packed pairs)");
+    constexpr int NW = NT / 32;
+    constexpr int KP = K / 2;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int cap = A.live_cap;
+    const int stride = A.pgrad_stride;
+
+    float *recs = reinterpret_cast<float *>(smem);
+    int *live_idx = reinterpret_cast<int *>(smem + (size_t)cap * GREC * 4);
+    int *live_flag = live_idx + cap;
+    float *wacc = reinterpret_cast<float *>(live_flag + cap);
+
+    __shared__ int s_cnt[NW];
+    __shared__ double s_chi2[NW];
+    __shared__ int s_any_weight;
+
+    const TileDesc td = A.tiles[tile];
+    const float4 bb = A.want_residual ? A.tbox_all[tile] : A.tbox_w[tile];
+    const int g0 = A.pv.gauss_start[td.exposure];
+    const int g1 = A.pv.gauss_start[td.exposure + 1];
+
+    for (int j = tid; j < NW * stride; j += NT) wacc[j] = 0.0f;
+
+    // ---- load this thread's pixels (packed pairs: pixel j and j+1 of the thread)
+    const float xmid = 0.5f * (bb.x + bb.y), ymid = 0.5f * (bb.z + bb.w);
+    v2 X[KP], Y[KP], R[KP], R2[KP];
+    float D[K], IE[K];
+    int any_w = 0;
+#pragma unroll
+    for (int j = 0; j < KP; ++j) {
+        float xs[2], ys[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int li = tid + (2 * j + h) * NT;
+            const bool ok = li < td.count;
+            const int pix = td.pix_begin + (ok ? li : 0);
+            xs[h] = ok ? A.pv.xpix[pix] : xmid;
+            ys[h] = ok ? A.pv.ypix[pix] : ymid;
+            D[2 * j + h] = ok ? A.pv.data[pix] : 0.0f;
+            IE[2 * j + h] = ok ? A.pv.ierr[pix] : 0.0f;
+            any_w |= (IE[2 * j + h] != 0.0f);
+        }
+        X[j] = pk(xs[0], xs[1]);
+        Y[j] = pk(ys[0], ys[1]);
+        R[j] = pk(D[2 * j], D[2 * j + 1]);
+    }
+    if (tid == 0) s_any_weight = 0;
+    __syncthreads();
+    if (any_w) s_any_weight = 1;
+    __syncthreads();
+    const bool tile_has_weight = s_any_weight != 0;
+
+    const v2 KEXP2 = pk1(KEXP);
+    long long npairs = 0;
+
+    // ---- chunked scan + stage.  Returns the number of staged records; `cursor`
+    // advances through [g0, g1).
+    auto scan_and_stage = [&](int &cursor) -> int {
+        int n = 0;
+        while (cursor < g1 && n + NT <= cap) {
+            const int idx = cursor + tid;
+            bool live = false;
+            if (idx < g1) {
+                const float4 gb = A.gbox[idx];
+                live = !(gb.y < bb.x || gb.x > bb.y || gb.w < bb.z || gb.z > bb.w);
+            }
+            const unsigned ball = __ballot_sync(0xffffffffu, live);
+            if (lane == 0) s_cnt[warp] = __popc(ball);
+            __syncthreads();
+            int off = 0, tot = 0;
+#pragma unroll
+            for (int w = 0; w < NW; ++w) {
+                off += (w < warp) ? s_cnt[w] : 0;
+                tot += s_cnt[w];
+            }
+            if (live) live_idx[n + off + __popc(ball & ((1u << lane) - 1u))] = idx;
+            n += tot;
+            cursor += NT;
+            __syncthreads();
+        }
+        // stage records with bulk copies issued by warp 0
+        fence_proxy_async_smem();
+        if (warp == 0) {
+            if (lane == 0) mbar_arrive_expect_tx(mbar, (uint32_t)n * GREC * 4);
+            __syncwarp();
+            for (int i = lane; i < n; i += 32)
+                bulk_g2s(recs + (size_t)i * GREC, A.gtab + (size_t)live_idx[i] * GREC, GREC * 4,
+                         mbar);
+        }
+        mbar_wait_bounded(mbar, phase, A.err);
+        phase ^= 1u;
+        // per (tile, Gaussian): can the exp-argument cross 36 inside the tile?
+        for (int i = tid; i < n; i += NT) {
+            const float *r = recs + (size_t)i * GREC;
+            const float nxc = r[R_NXC], nyc = r[R_NYC];
+            const float fxx = r[R_FXX], fxy = r[R_FXY], fyy = r[R_FYY];
+            float qmax = 0.0f;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const float dx = ((c & 1) ? bb.y : bb.x) + nxc;
+                const float dy = ((c & 2) ? bb.w : bb.z) + nyc;
+                const float q = dx * (fxx * dx + fxy * dy) + dy * (fyy * dy + fxy * dx);
+                qmax = fmaxf(qmax, q);
+            }
+            live_flag[i] = (qmax * (1.0f + CULL_REL) + CULL_ABS >= FPHO_MAX_EXP_ARG) ? 1 : 0;
+        }
+        __syncthreads();
+        return n;
+    };
+
+    // ------------------------------------------------------------ pass 1
+    // npairs counts the records staged over all pass-1 chunks; if that equals
+    // the last chunk's size, the whole kept set is still resident for pass 2.
+    int cursor = g0;
+    int n_last = 0;
+    {
+        bool first = true;
+        while (cursor < g1 || first) {
+            if (!first) __syncthreads();  // previous chunk fully consumed
+            first = false;
+            const int n = scan_and_stage(cursor);
+            n_last = n;
+            npairs += (long long)n;
+            for (int i = 0; i < n; ++i) {
+                const float4 *r4 = reinterpret_cast<const float4 *>(recs + (size_t)i * GREC);
+                const float4 a = r4[0], b = r4[1];
+                const v2 NXC = pk1(a.x), NYC = pk1(a.y), FXX = pk1(a.z), FXY = pk1(a.w);
+                const v2 FYY = pk1(b.x), HA = pk1(b.y), HB = pk1(b.z);
+                const bool cut = live_flag[i] != 0;
+#pragma unroll
+                for (int j = 0; j < KP; ++j) {
+                    const v2 DX = add2(X[j], NXC), DY = add2(Y[j], NYC);
+                    const v2 VX = fma2(FXY, DY, mul2(FXX, DX));
+                    const v2 VY = fma2(FXY, DX, mul2(FYY, DY));
+                    const v2 Q = fma2(DY, VY, mul2(DX, VX));
+                    const v2 E = mul2(Q, KEXP2);
+                    float e0, e1, q0, q1;
+                    unpk(E, e0, e1);
+                    float g0v = ex2f(e0), g1v = ex2f(e1);
+                    if (cut) {
+                        unpk(Q, q0, q1);
+                        g0v = (q0 > FPHO_MAX_EXP_ARG) ? 0.0f : g0v;
+                        g1v = (q1 > FPHO_MAX_EXP_ARG) ? 0.0f : g1v;
+                    }
+                    const v2 S = fma2(VY, VY, mul2(VX, VX));
+                    const v2 NAH = fma2(S, HA, HB);  // -amp * H
+                    R[j] = fma2(NAH, pk(g0v, g1v), R[j]);
+                }
+            }
+        }
+    }
+
+    // ---- residual store, chi2 (double) and the per-pixel adjoint -2 r ie^2
+    double chi2 = 0.0;
+#pragma unroll
+    for (int j = 0; j < KP; ++j) {
+        float r[2];
+        unpk(R[j], r[0], r[1]);
+        float r2v[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int k = 2 * j + h;
+            const int li = tid + k * NT;
+            if (A.want_residual && li < td.count) A.pv.residual[td.pix_begin + li] = r[h];
+            const float ie = IE[k];
+            const float rie = r[h] * ie;
+            const float die = D[k] * ie;
+            double c = ((double)rie - (double)die);
+            c *= ((double)rie + (double)die);
+            chi2 += (ie != 0.0f) ? c : 0.0;
+            r2v[h] = (ie != 0.0f) ? -2.0f * (rie * ie) : 0.0f;
+        }
+        R2[j] = pk(r2v[0], r2v[1]);
+    }
+    chi2 = warp_sum_d(chi2);
+    if (lane == 0) s_chi2[warp] = chi2;
+
+    // ------------------------------------------------------------ pass 2
+    if (tile_has_weight) {
+        const v2 C24 = pk1(1.0f / 24.0f);
+        // re-use the staged chunk if the kept set fit in one, otherwise rescan
+        int cursor2 = g0;
+        bool first = true;
+        const bool reuse = (npairs == (long long)n_last);
+        while (first || cursor2 < g1) {
+            int n;
+            if (first && reuse) {
+                n = n_last;
+                cursor2 = g1;
+            } else {
+                __syncthreads();
+                n = scan_and_stage(cursor2);
+            }
+            first = false;
+            v2 P[7];
+#pragma unroll
+            for (int k = 0; k < 7; ++k) P[k] = 0ull;
+            for (int i = 0; i < n; ++i) {
+                const float4 *r4 = reinterpret_cast<const float4 *>(recs + (size_t)i * GREC);
+                const float4 a = r4[0], b = r4[1];
+                const v2 NXC = pk1(a.x), NYC = pk1(a.y), FXX = pk1(a.z), FXY = pk1(a.w);
+                const v2 FYY = pk1(b.x), C0 = pk1(b.w);
+                const bool cut = live_flag[i] != 0;
+                v2 aA = 0ull, aHVx = 0ull, aHVy = 0ull, aVx = 0ull, aVy = 0ull;
+                v2 aHXX = 0ull, aHXY = 0ull, aHYY = 0ull, aW = 0ull;
+                v2 aT1 = 0ull, aT2 = 0ull, aT3 = 0ull;
+#pragma unroll
+                for (int j = 0; j < KP; ++j) {
+                    const v2 DX = add2(X[j], NXC), DY = add2(Y[j], NYC);
+                    const v2 VX = fma2(FXY, DY, mul2(FXX, DX));
+                    const v2 VY = fma2(FXY, DX, mul2(FYY, DY));
+                    const v2 T1 = mul2(DX, VX);
+                    const v2 Q = fma2(DY, VY, T1);
+                    const v2 E = mul2(Q, KEXP2);
+                    float e0, e1, q0, q1;
+                    unpk(E, e0, e1);
+                    float g0v = ex2f(e0), g1v = ex2f(e1);
+                    if (cut) {
+                        unpk(Q, q0, q1);
+                        g0v = (q0 > FPHO_MAX_EXP_ARG) ? 0.0f : g0v;
+                        g1v = (q1 > FPHO_MAX_EXP_ARG) ? 0.0f : g1v;
+                    }
+                    const v2 S = fma2(VY, VY, mul2(VX, VX));
+                    const v2 H = fma2(S, C24, C0);
+                    const v2 W = mul2(R2[j], pk(g0v, g1v));
+                    const v2 WH = mul2(W, H);
+                    aA = add2(aA, WH);
+                    aHVx = fma2(WH, VX, aHVx);
+                    aHVy = fma2(WH, VY, aHVy);
+                    aVx = fma2(W, VX, aVx);
+                    aVy = fma2(W, VY, aVy);
+                    const v2 HDX = mul2(WH, DX);
+                    aHXX = fma2(HDX, DX, aHXX);
+                    aHXY = fma2(HDX, DY, aHXY);
+                    aHYY = fma2(mul2(WH, DY), DY, aHYY);
+                    aW = add2(aW, W);
+                    aT1 = fma2(W, T1, aT1);
+                    aT2 = fma2(W, mul2(DY, VY), aT2);
+                    aT3 = fma2(W, fma2(DX, VY, mul2(DY, VX)), aT3);
+                }
+                // image-space gradient of this Gaussian over the thread's pixels
+                // (amp factors are folded into the Jacobian rows)
+                const v2 C12 = pk1(1.0f / 12.0f), CM12 = pk1(-1.0f / 12.0f);
+                const v2 CMH = pk1(-0.5f), CM24 = pk1(-1.0f / 24.0f), CM1 = pk1(-1.0f);
+                const v2 gA = aA;
+                const v2 gx = fma2(CM12, fma2(FXY, aVy, mul2(FXX, aVx)), aHVx);
+                const v2 gy = fma2(CM12, fma2(FXY, aVx, mul2(FYY, aVy)), aHVy);
+                const v2 wq = mul2(aW, CM24);
+                const v2 gfxx = fma2(C12, aT1, fma2(CMH, aHXX, wq));
+                const v2 gfyy = fma2(C12, aT2, fma2(CMH, aHYY, wq));
+                const v2 gfxy = fma2(C12, aT3, mul2(CM1, aHXY));
+                const float4 j3 = r4[3], j4 = r4[4], j5 = r4[5], j6 = r4[6];
+                P[0] = fma2(pk1(j3.x), gA, P[0]);
+                P[1] = fma2(pk1(j4.z), gy, fma2(pk1(j4.y), gx, P[1]));
+                P[2] = fma2(pk1(j5.x), gy, fma2(pk1(j4.w), gx, P[2]));
+                P[3] = fma2(pk1(j5.w), gfyy,
+                            fma2(pk1(j5.z), gfxy, fma2(pk1(j5.y), gfxx, fma2(pk1(j3.y), gA, P[3]))));
+                P[4] = fma2(pk1(j6.z), gfyy,
+                            fma2(pk1(j6.y), gfxy, fma2(pk1(j6.x), gfxx, fma2(pk1(j3.z), gA, P[4]))));
+                P[5] = fma2(pk1(j3.w), gA, P[5]);
+                P[6] = fma2(pk1(j4.x), gA, P[6]);
+                // flush at a source boundary or at the end of the chunk
+                const int src = __float_as_int(r4[2].x);
+                const int nsrc_next =
+                    (i + 1 < n) ? __float_as_int(recs[(size_t)(i + 1) * GREC + R_SRC]) : -1;
+                if (nsrc_next != src) {
+                    float v[8];
+#pragma unroll
+                    for (int k = 0; k < 7; ++k) {
+                        float l, h;
+                        unpk(P[k], l, h);
+                        v[k] = l + h;
+                        P[k] = 0ull;
+                    }
+                    v[7] = 0.0f;
+                    const float tot = warp_reduce7(v, lane);
+                    const int k = reduce7_index(lane);
+                    if ((lane & 3) == 0 && k < 7) wacc[warp * stride + src * 7 + k] += tot;
+                }
+            }
+        }
+    }
+    __syncthreads();
+
+    // ---- tile partials (fixed-order sums)
+    if (tid == 0) {
+        double c = 0.0;
+#pragma unroll
+        for (int w = 0; w < NW; ++w) c += s_chi2[w];
+        A.pchi2[tile] = c;
+    }
+    for (int j = tid; j < stride; j += NT) {
+        float v = 0.0f;
+#pragma unroll
+        for (int w = 0; w < NW; ++w) v += wacc[w * stride + j];
+        A.pgrad[(size_t)tile * stride + j] = v;
+    }
+    if (A.pairs && tid == 0) atomicAdd(reinterpret_cast<unsigned long long *>(A.pairs),
+                                       (unsigned long long)(npairs * (long long)td.count));
+}
+
+}  // namespace fpho

@@ -1,0 +1,134 @@
+"""Device communication of patch data.
+
+:class:`GPUPatchMixin` mirrors forcepho/patches/device_patch.py:260-393
+(``send_to_device``, ``replace_device_meta_ptrs``,
+``send_patchstruct_to_device``, ``swap_on_device``, ``retrieve_array``,
+``free``, ``get_proposer`` and the ``device_patch`` attribute), backed by a
+``fpho_patch`` handle of the C ABI instead of pycuda allocations.
+:class:`DevicePatchMixin` adds the reference's fixed-source subtraction and
+rendering helpers that are built on the same evaluation
+(device_patch.py:113-254).
+"""
+
+import ctypes
+
+import numpy as np
+
+from .. import _lib
+from ..proposal import GPUProposer
+
+__all__ = ["DevicePatch", "DevicePatchMixin", "GPUPatchMixin"]
+
+_ARRAY_CODE = {"data": 0, "residual": 1, "ierr": 2, "xpix": 3, "ypix": 4}
+
+
+class DevicePatch:
+    """Owner of one ``fpho_patch`` handle (device copy of a patch + workspace)."""
+
+    def __init__(self, patch, return_residual=False, stream=None):
+        st = patch.host_struct()
+        self._keep = st  # host arrays stay referenced by `patch`
+        h = ctypes.c_void_p()
+        _lib.call("fpho_patch_create", st.ctypes.data, int(patch.n_bands),
+                  int(bool(return_residual)), stream, ctypes.byref(h))
+        self.handle = h.value
+        self.return_residual = bool(return_residual)
+
+    def info(self):
+        out = (ctypes.c_int64 * 7)()
+        _lib.call("fpho_patch_info", self.handle, out)
+        keys = ["n_bands", "n_exp", "npix", "n_sources", "n_radii", "n_tiles", "n_gauss"]
+        return dict(zip(keys, list(out)))
+
+    @property
+    def device_struct(self):
+        """Device address of the patch struct (device pointers inside)."""
+        p = ctypes.c_void_p()
+        _lib.call("fpho_patch_device_struct", self.handle, ctypes.byref(p))
+        return p.value
+
+    def set_config(self, variant, live_cap, stream=None):
+        _lib.call("fpho_patch_set_config", self.handle, int(variant), int(live_cap), stream)
+
+    def free(self):
+        if getattr(self, "handle", None):
+            _lib.lib.fpho_patch_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class DevicePatchMixin:
+    """Methods shared by device mixins (forcepho/patches/device_patch.py:23-257)."""
+
+    def get_proposer(self):
+        raise NotImplementedError
+
+    def send_to_device(self):
+        raise NotImplementedError
+
+    def render(self, proposal):
+        """Model images (one flat array per exposure) of a proposal, as the
+        reference's ``render`` (device_patch.py:240-254) but taking the
+        packed proposal directly."""
+        orig = self.return_residual
+        if not orig or getattr(self, "device_patch", None) is None or \
+                not self.device_patch.return_residual:
+            self.return_residual = True
+            self.free()
+            self.send_to_device()
+        proposer = self.get_proposer()
+        chi2, derivs, residuals = proposer.evaluate_proposal(proposal, patch=self, unpack=True)
+        data = self.split_pix("data")
+        self.return_residual = orig
+        return [d - r for d, r in zip(data, residuals)]
+
+
+class GPUPatchMixin(DevicePatchMixin):
+    """Mix-in for communicating patch data with the GPU through the C ABI."""
+
+    def get_proposer(self):
+        return GPUProposer()
+
+    def send_to_device(self):
+        """Copy every patch array to the device; returns ``self.device_patch``."""
+        self.device_patch = DevicePatch(self, return_residual=self.return_residual)
+        self._dirty_data = False
+        return self.device_patch
+
+    def replace_device_meta_ptrs(self):
+        """Replace the device metadata with the currently packed host metadata."""
+        st = self.host_struct()
+        _lib.call("fpho_patch_replace_meta", self.device_patch.handle, st.ctypes.data, None)
+
+    def send_patchstruct_to_device(self):
+        """The device patch struct is refreshed by every C-ABI call that
+        changes a pointer; this returns the handle for compatibility."""
+        return self.device_patch
+
+    def swap_on_device(self):
+        """Install the packed metadata and make the device residual the data
+        (device_patch.py:346-367)."""
+        if not self.device_patch.return_residual:
+            raise AssertionError("Must instantiate the Patch with `return_residual=True`")
+        self.replace_device_meta_ptrs()
+        _lib.call("fpho_patch_swap_data_residual", self.device_patch.handle, None)
+        self._dirty_data = True
+        return self.device_patch
+
+    def retrieve_array(self, arrname="residual"):
+        """Copy a pixel array (data, residual, ierr, xpix, ypix) to the host."""
+        out = np.empty(self.npix, dtype=np.float32)
+        _lib.call("fpho_patch_retrieve", self.device_patch.handle, _ARRAY_CODE[arrname],
+                  out.ctypes.data, None)
+        return out
+
+    def free(self):
+        dp = getattr(self, "device_patch", None)
+        if dp is not None:
+            dp.free()
+        self.device_patch = None

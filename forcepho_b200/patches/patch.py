@@ -1,0 +1,169 @@
+"""Host-side patch data model.
+
+:class:`PatchBase` mirrors the reference's ``PatchBase``
+(forcepho/patches/patch.py:20-197): the numpy arrays a patch is packed into and
+the ``patch_struct_dtype`` of pointers and counts, which is byte-compatible
+with the ``Patch`` struct of the device ABI (forcepho/src/patch.cc:23-99,
+``fpho_patch_struct`` in include/fpho.h).
+"""
+
+import numpy as np
+
+__all__ = ["PatchBase", "PSF_COLS", "PSF_DTYPE"]
+
+# PSF Gaussian columns, as forcepho/patches/storage.py:35-36
+PSF_COLS = ["amp", "xcen", "ycen", "Cxx", "Cyy", "Cxy"]
+PSF_DTYPE = np.dtype([(c, np.float32) for c in PSF_COLS] + [("sersic_bin", np.int32)])
+
+
+class PatchBase:
+    """Arrays of one patch packed for the device.
+
+    Parameters
+    ----------
+    return_residual : bool
+        Whether evaluations also write the residual image (data - model).
+    pix_dtype, meta_dtype : numpy dtype
+        Must be float32 (the device ABI is single precision).
+    """
+
+    ptr_dtype = np.uintp
+    pdt = np.dtype([('data', ptr_dtype),
+                    ('ierr', ptr_dtype),
+                    ('xpix', ptr_dtype),
+                    ('ypix', ptr_dtype),
+                    ('residual', ptr_dtype),
+                    ('exposure_start', ptr_dtype),
+                    ('exposure_N', ptr_dtype),
+                    ('band_start', ptr_dtype),
+                    ('band_N', ptr_dtype),
+                    ('n_sources', np.int32),
+                    ('n_radii', np.int32),
+                    ('rad2', ptr_dtype),
+                    ('D', ptr_dtype),
+                    ('crpix', ptr_dtype),
+                    ('crval', ptr_dtype),
+                    ('CW', ptr_dtype),
+                    ('G', ptr_dtype),
+                    ('n_psf_per_source', ptr_dtype),
+                    ('psfgauss', ptr_dtype),
+                    ('psfgauss_start', ptr_dtype)],
+                   align=True)
+    patch_struct_dtype = pdt
+    meta_names = ["n_sources", "n_radii", "rad2",
+                  "D", "crpix", "crval", "CW", "G",
+                  "n_psf_per_source", "psfgauss", "psfgauss_start"]
+
+    # dtype of every array field, used to coerce before taking pointers
+    array_dtypes = dict(data=np.float32, ierr=np.float32, xpix=np.float32, ypix=np.float32,
+                        residual=np.float32, exposure_start=np.int32, exposure_N=np.int32,
+                        band_start=np.int16, band_N=np.int16, rad2=np.float32, D=np.float32,
+                        crpix=np.float32, crval=np.float32, CW=np.float32, G=np.float32,
+                        n_psf_per_source=np.int32, psfgauss=PSF_DTYPE, psfgauss_start=np.int32)
+
+    def __init__(self, return_residual=False, pix_dtype=np.float32, meta_dtype=np.float32):
+        if np.dtype(pix_dtype) != np.float32 or np.dtype(meta_dtype) != np.float32:
+            raise ValueError("the device ABI is float32: pix_dtype and meta_dtype must be float32")
+        self.pix_dtype = np.float32
+        self.meta_dtype = np.float32
+        self.return_residual = return_residual
+        self._dirty_data = True
+
+    @property
+    def npix(self):
+        try:
+            return self.xpix.shape[0]
+        except AttributeError:
+            return 0
+
+    @property
+    def n_bands(self):
+        return len(self.band_start)
+
+    @property
+    def n_exp(self):
+        return len(self.exposure_start)
+
+    @property
+    def size(self):
+        s = 0
+        for arrname in self.patch_struct_dtype.names:
+            a = getattr(self, arrname, None)
+            if isinstance(a, np.ndarray):
+                s += a.nbytes
+        return s
+
+    @property
+    def band_N_pix(self):
+        """Pixels (with padding) of each band."""
+        out = np.zeros(self.n_bands, dtype=np.int64)
+        for b in range(self.n_bands):
+            e0, n = int(self.band_start[b]), int(self.band_N[b])
+            out[b] = int(np.sum(self.exposure_N[e0:e0 + n]))
+        return out
+
+    def clear(self):
+        for arrname in self.patch_struct_dtype.names:
+            try:
+                delattr(self, arrname)
+            except AttributeError:
+                pass
+
+    def free(self):
+        pass
+
+    def build_patch(self, npix=1, n_sources=1, n_radii=1, n_bands=1, n_exp=1):
+        """Allocate every array with the proper shape and dtype (as the
+        reference's ``build_patch``, forcepho/patches/patch.py:121-197)."""
+        self.xpix = np.zeros(npix, dtype=np.float32)
+        self.ypix = np.zeros(npix, dtype=np.float32)
+        self.data = np.zeros(npix, dtype=np.float32)
+        self.ierr = np.zeros(npix, dtype=np.float32)
+        self.band_start = np.zeros(n_bands, dtype=np.int16)
+        self.band_N = np.zeros(n_bands, dtype=np.int16)
+        self.exposure_start = np.zeros(n_exp, dtype=np.int32)
+        self.exposure_N = np.zeros(n_exp, dtype=np.int32)
+        self.n_sources = n_sources
+        self.n_radii = n_radii
+        self.rad2 = np.zeros(n_radii, dtype=np.float32)
+        self.D = np.zeros((n_exp, n_sources, 2, 2), dtype=np.float32)
+        self.CW = np.zeros((n_exp, n_sources, 2, 2), dtype=np.float32)
+        self.crpix = np.zeros((n_exp, n_sources, 2), dtype=np.float32)
+        self.crval = np.zeros((n_exp, n_sources, 2), dtype=np.float32)
+        self.G = np.zeros(n_exp, dtype=np.float32)
+        self.n_psf_per_source = np.zeros(n_bands, dtype=np.int32)
+        self.psfgauss = np.zeros(0, dtype=PSF_DTYPE)
+        self.psfgauss_start = np.zeros(n_exp, dtype=np.int32)
+
+    def coerce_arrays(self):
+        """Make every array C-contiguous with the ABI dtype (in place)."""
+        for name, dt in self.array_dtypes.items():
+            a = getattr(self, name, None)
+            if a is None:
+                continue
+            setattr(self, name, np.ascontiguousarray(a, dtype=dt))
+
+    def host_struct(self, residual=None):
+        """A ``patch_struct_dtype`` record holding HOST pointers to this
+        patch's arrays (the form :func:`fpho_patch_create` reads)."""
+        self.coerce_arrays()
+        st = np.zeros(1, dtype=self.patch_struct_dtype)
+        for name in self.patch_struct_dtype.names:
+            if self.patch_struct_dtype[name] == self.ptr_dtype:
+                if name == "residual":
+                    st[name] = 0 if residual is None else residual.ctypes.data
+                else:
+                    st[name] = getattr(self, name).ctypes.data
+            else:
+                st[name] = getattr(self, name)
+        return st
+
+    def split_pix(self, attr):
+        """Split a pixel array into one array per exposure."""
+        arr = getattr(self, attr)
+        return np.split(arr, np.cumsum(self.exposure_N[:-1]))
+
+    def split_band(self, attr):
+        """Split a pixel array into one array per band."""
+        arr = getattr(self, attr)
+        return np.split(arr, np.cumsum(self.band_N_pix[:-1]))

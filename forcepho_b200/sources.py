@@ -1,0 +1,130 @@
+"""Sersic mixture amplitudes and the packing of source parameters into
+proposals.
+
+:class:`SersicTable` holds the amplitude table of forcepho's Sersic Gaussian
+mixtures and evaluates it exactly like ``Galaxy.amplitudes``,
+``Galaxy.damplitude_dsersic`` and ``Galaxy.damplitude_drh``
+(forcepho/sources.py:623-694): one scipy ``RectBivariateSpline`` (bicubic,
+``s=spline_smoothing``) per mixture radius over the (sersic, rh) grid, with the
+reference's branches for ``sersic`` below the grid and ``rh < 0``.  The spline
+knots and coefficients are exported for the on-device evaluation
+(:mod:`forcepho_b200.device_proposal`).
+
+:func:`proposal_from_params` packs a parameter array in the reference's Scene
+order ``[flux_1..flux_B, ra, dec, q, pa, sersic, rhalf]`` per source
+(forcepho/sources.py:46-97, 526-621) into ``source_struct_dtype``.
+"""
+
+import os
+
+import numpy as np
+from scipy.interpolate import RectBivariateSpline
+
+from .kernel_limits import MAXRADII
+from .proposal import source_struct_dtype
+
+__all__ = ["SersicTable", "default_table", "proposal_from_params", "SHAPE_COLS"]
+
+SHAPE_COLS = ["ra", "dec", "q", "pa", "sersic", "rhalf"]
+_DEFAULT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data",
+                        "sersic_splinedata_large.npz")
+
+
+class SersicTable:
+    """Sersic amplitude splines over a regular (sersic, rh) grid.
+
+    Parameters
+    ----------
+    ngrid, rgrid : 1-d arrays, the grid of Sersic index and half-light radius
+    amplitudes : array (len(ngrid), len(rgrid), n_radii)
+    radii : array (n_radii,), mixture radii in arcsec
+    spline_smoothing : passed to RectBivariateSpline as ``s`` (None -> 0)
+    """
+
+    def __init__(self, ngrid, rgrid, amplitudes, radii, spline_smoothing=None):
+        self.ngrid = np.asarray(ngrid, dtype=np.float64)
+        self.rgrid = np.asarray(rgrid, dtype=np.float64)
+        self.amps = np.asarray(amplitudes, dtype=np.float64)
+        self.radii = np.asarray(radii, dtype=np.float64)
+        if self.amps.shape != (len(self.ngrid), len(self.rgrid), len(self.radii)):
+            raise ValueError("amplitudes must have shape (n_n, n_r, n_radii)")
+        if len(self.radii) > MAXRADII:
+            raise ValueError(f"at most {MAXRADII} mixture radii")
+        s = 0 if spline_smoothing is None else spline_smoothing
+        self.splines = [RectBivariateSpline(self.ngrid, self.rgrid, self.amps[:, :, i], s=s)
+                        for i in range(len(self.radii))]
+        self.sersic_range = (self.ngrid.min(), self.ngrid.max())
+        self.rh_range = (self.rgrid.min(), self.rgrid.max())
+
+    @property
+    def n_radii(self):
+        return len(self.radii)
+
+    @property
+    def rad2(self):
+        return (self.radii ** 2).astype(np.float32)
+
+    def amplitudes(self, sersic, rhalf):
+        if sersic < self.sersic_range[0]:
+            amp = np.zeros(self.n_radii)
+            amp[np.argmin(np.abs(rhalf - self.radii))] = 1.0
+        elif rhalf < 0:
+            amp = np.zeros(self.n_radii)
+            amp[0] = 1.0
+        else:
+            amp = np.array([float(sp(sersic, rhalf)[0, 0]) for sp in self.splines])
+        return amp
+
+    def damplitude_dsersic(self, sersic, rhalf):
+        if sersic < self.sersic_range[0] or rhalf < 0:
+            return np.zeros(self.n_radii)
+        return np.array([float(sp(sersic, rhalf, dx=1)[0, 0]) for sp in self.splines])
+
+    def damplitude_drh(self, sersic, rhalf):
+        if sersic < self.sersic_range[0] or rhalf < 0:
+            return np.zeros(self.n_radii)
+        return np.array([float(sp(sersic, rhalf, dy=1)[0, 0]) for sp in self.splines])
+
+    def knots_and_coeffs(self):
+        """(tx, ty, coeffs[n_radii, len(tx)-4, len(ty)-4]) of the bicubic
+        splines; all radii share the knot vectors."""
+        tx, ty = self.splines[0].get_knots()
+        for sp in self.splines[1:]:
+            a, b = sp.get_knots()
+            if not (np.array_equal(a, tx) and np.array_equal(b, ty)):
+                raise ValueError("splines do not share knots")
+        nc = (len(tx) - 4, len(ty) - 4)
+        c = np.stack([sp.get_coeffs().reshape(nc) for sp in self.splines])
+        return tx, ty, c
+
+
+_default_table = None
+
+
+def default_table():
+    """The table extracted from forcepho's ``sersic_splinedata_large.h5``
+    (sersic 0.8..6.2, rh 0..1 arcsec, 9 radii)."""
+    global _default_table
+    if _default_table is None:
+        d = np.load(_DEFAULT)
+        _default_table = SersicTable(d["ngrid"], d["rgrid"], d["amplitudes"], d["radii"])
+    return _default_table
+
+
+def proposal_from_params(params, n_bands, table=None):
+    """Pack parameters of shape (n_sources, n_bands + 6), in Scene order, into
+    a ``source_struct_dtype`` array (as ``Galaxy.proposal``,
+    forcepho/sources.py:607-621)."""
+    table = table or default_table()
+    params = np.asarray(params, dtype=np.float64).reshape(-1, n_bands + 6)
+    out = np.zeros(len(params), dtype=source_struct_dtype)
+    nr = table.n_radii
+    for i, p in enumerate(params):
+        out["fluxes"][i, :n_bands] = p[:n_bands]
+        ra, dec, q, pa, n, rh = p[n_bands:]
+        out["ra"][i], out["dec"][i], out["q"][i], out["pa"][i] = ra, dec, q, pa
+        out["nsersic"][i], out["rh"][i] = n, rh
+        out["mixture_amplitudes"][i, :nr] = table.amplitudes(n, rh)
+        out["damplitude_drh"][i, :nr] = table.damplitude_drh(n, rh)
+        out["damplitude_dnsersic"][i, :nr] = table.damplitude_dsersic(n, rh)
+    return out

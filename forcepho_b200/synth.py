@@ -1,0 +1,342 @@
+"""Seeded synthetic patches in the reference's packed layout.
+
+No public dataset is involved in forcepho's hot path; its inputs are packed
+patches (pixel data, inverse errors and pixel coordinates per exposure,
+per-exposure astrometry, photometric conversion and PSF mixtures) and source
+proposals.  This module draws them from ``numpy.random.default_rng(seed)``
+with the distributions of the five workloads the benchmarks and tests use:
+
+  config 0  1 band x 1 exposure of 64x64 px, 1 source, 3-Gaussian PSF
+  config 1  8 bands x 4 exposures of 128x128 px, 20 sources, 5-Gaussian PSFs,
+            per-exposure rotation (+-1 deg), scale (+-2%), flux calibration
+            U[0.8, 1.2], 2% of pixels masked (ierr = 0)
+  config 2  the config-1 patch (driven through the differentiable form)
+  config 3  256 patches: sources U{1..30}, bands U{1..8}, exposures per band
+            U{1..8}, exposure side U[32, 200] px
+  config 4  60 sources (half with sersic in [3.5, 6], rh up to 1 arcsec,
+            fluxes LogNormal(0, 3)), 15 bands x 6 exposures of 256x256 px,
+            6-Gaussian PSFs
+
+Pixel scale 0.03 arcsec/px.  D (pixels per arcsec) and CW (pixels per degree,
+CW = D diag(3600 cos dec0, 3600)) follow forcepho/slow/stamp.py:250-254.
+Pixels are packed per exposure in 8x8 superpixels ordered along a Morton
+curve, each exposure padded to whole superpixels with pixels at x = y = -1 and
+ierr = 0 (the reference's padding convention, forcepho/patches/pixel_patch.py
+:472-483).  The PSF mixture of an exposure is repeated for every Sersic radius
+bin (sersic_bin = 0..n_radii-1) and every source.  Data are the truth model
+plus Gaussian noise of sigma = 0.05 x the exposure's peak, ierr = 1/sigma.
+Proposals are evaluated at the truth perturbed by 1% in every parameter.
+"""
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from .patches.patch import PSF_DTYPE, PatchBase
+from .patches.device_patch import GPUPatchMixin
+from .sources import default_table, proposal_from_params
+
+__all__ = ["PatchSpec", "SyntheticPatch", "make_config", "make_patch", "config_spec",
+           "render_model_numpy", "PIXEL_SCALE", "DEC0"]
+
+PIXEL_SCALE = 0.03      # arcsec per pixel
+DEC0 = -27.78           # declination of the patch centre (degrees)
+
+
+@dataclass
+class PatchSpec:
+    n_sources: int
+    exposures_per_band: list          # exposures of each band
+    shapes: list                      # (nx, ny) per exposure
+    n_psf: int = 3                    # PSF Gaussians per exposure
+    psf_sigma: tuple = (0.5, 3.0)     # PSF component sigma range (px)
+    rot_deg: float = 0.0              # per-exposure rotation amplitude
+    scale_frac: float = 0.0           # per-exposure pixel-scale amplitude
+    g_range: tuple = (1.0, 1.0)       # photometric conversion range
+    mask_frac: float = 0.0            # fraction of pixels with ierr = 0
+    flux_sigma: float = 1.0           # LogNormal sigma of fluxes
+    position: str = "uniform"         # "centre" (+-0.3") or "uniform" over the patch
+    sersic: tuple = (1.0, 5.0)
+    rh: tuple = (0.05, 0.3)
+    bright_fraction: float = 0.0      # fraction drawn from sersic/rh "bright" ranges
+    bright_sersic: tuple = (3.5, 6.0)
+    bright_rh: tuple = (0.05, 1.0)
+    perturb: float = 0.01
+    extra: dict = field(default_factory=dict)
+
+    @property
+    def n_bands(self):
+        return len(self.exposures_per_band)
+
+
+def config_spec(k, rng=None):
+    """PatchSpec of config k (0, 1, 2 or 4; config 3 draws one spec per patch
+    from ``rng``, see :func:`make_config`)."""
+    if k == 0:
+        return PatchSpec(n_sources=1, exposures_per_band=[1], shapes=[(64, 64)], n_psf=3,
+                         psf_sigma=(0.5, 3.0), flux_sigma=1.0, position="centre")
+    if k in (1, 2):
+        return PatchSpec(n_sources=20, exposures_per_band=[4] * 8, shapes=[(128, 128)] * 32,
+                         n_psf=5, psf_sigma=(0.5, 4.0), rot_deg=1.0, scale_frac=0.02,
+                         g_range=(0.8, 1.2), mask_frac=0.02, flux_sigma=1.5)
+    if k == 3:
+        rng = rng or np.random.default_rng(0)
+        nb = int(rng.integers(1, 9))
+        epb = [int(rng.integers(1, 9)) for _ in range(nb)]
+        shapes = []
+        for _ in range(sum(epb)):
+            side = int(np.round(rng.uniform(32, 200)))
+            shapes.append((side, side))
+        return PatchSpec(n_sources=int(rng.integers(1, 31)), exposures_per_band=epb,
+                         shapes=shapes, n_psf=5, psf_sigma=(0.5, 4.0), rot_deg=1.0,
+                         scale_frac=0.02, g_range=(0.8, 1.2), mask_frac=0.02, flux_sigma=1.5)
+    if k == 4:
+        return PatchSpec(n_sources=60, exposures_per_band=[6] * 15, shapes=[(256, 256)] * 90,
+                         n_psf=6, psf_sigma=(0.5, 4.0), rot_deg=1.0, scale_frac=0.02,
+                         g_range=(0.8, 1.2), mask_frac=0.02, flux_sigma=3.0,
+                         bright_fraction=0.5, bright_sersic=(3.5, 6.0), bright_rh=(0.05, 1.0))
+    raise ValueError(f"unknown config {k}")
+
+
+class SyntheticPatch(PatchBase, GPUPatchMixin):
+    """A packed synthetic patch with its truth and perturbed parameters.
+
+    Attributes beyond the PatchBase arrays: ``spec``, ``table`` (SersicTable),
+    ``truth`` and ``params`` (n_sources x (n_bands + 6) in Scene order),
+    ``original_shapes`` and ``original_sizes`` per exposure."""
+
+    def __init__(self, return_residual=False):
+        PatchBase.__init__(self, return_residual=return_residual)
+        self.device_patch = None
+
+    @property
+    def n_sources_(self):
+        return self.n_sources
+
+    def proposal(self, params=None):
+        p = self.params if params is None else params
+        return proposal_from_params(p, self.n_bands, self.table)
+
+    def truth_proposal(self):
+        return proposal_from_params(self.truth, self.n_bands, self.table)
+
+    @property
+    def pairs_per_eval(self):
+        """Nominal (pixel, image Gaussian) pairs of one evaluation: every
+        pixel (padding included) times the Gaussians of its exposure."""
+        npsf_e = np.repeat(self.n_psf_per_source, self.band_N.astype(np.int64))
+        return int(np.sum(self.exposure_N.astype(np.int64) * npsf_e * self.n_sources))
+
+
+def _morton_order(nsx, nsy):
+    sx, sy = np.meshgrid(np.arange(nsx), np.arange(nsy), indexing="ij")
+    sx, sy = sx.ravel(), sy.ravel()
+
+    def spread(v):
+        v = v.astype(np.uint64)
+        out = np.zeros_like(v)
+        for b in range(16):
+            out |= ((v >> np.uint64(b)) & np.uint64(1)) << np.uint64(2 * b)
+        return out
+
+    code = spread(sx) | (spread(sy) << np.uint64(1))
+    o = np.argsort(code, kind="stable")
+    return sx[o], sy[o]
+
+
+def _pack_exposure_pixels(nx, ny):
+    """x, y, valid arrays of one exposure in Morton-ordered 8x8 superpixels."""
+    nsx, nsy = (nx + 7) // 8, (ny + 7) // 8
+    sx, sy = _morton_order(nsx, nsy)
+    iy, ix = np.meshgrid(np.arange(8), np.arange(8), indexing="ij")
+    x = (sx[:, None] * 8 + ix.ravel()[None, :]).ravel()
+    y = (sy[:, None] * 8 + iy.ravel()[None, :]).ravel()
+    valid = (x < nx) & (y < ny)
+    return x, y, valid
+
+
+def _rot(t):
+    c, s = np.cos(t), np.sin(t)
+    return np.array([[c, -s], [s, c]])
+
+
+def render_model_numpy(patch, params, nsigma=7.0):
+    """FP64 model image (flat, patch pixel order) of Scene-ordered params,
+    with the second-order pixel-integration correction and no cutoff other
+    than truncating each Gaussian at ``nsigma`` (used only to synthesise data)."""
+    table = patch.table
+    nb = patch.n_bands
+    params = np.asarray(params, dtype=np.float64).reshape(-1, nb + 6)
+    model = np.zeros(patch.npix, dtype=np.float64)
+    rad2 = table.radii ** 2
+    for b in range(nb):
+        for e in range(int(patch.band_start[b]), int(patch.band_start[b] + patch.band_N[b])):
+            p0, n = int(patch.exposure_start[e]), int(patch.exposure_N[e])
+            xs = patch.xpix[p0:p0 + n].astype(np.float64)
+            ys = patch.ypix[p0:p0 + n].astype(np.float64)
+            npsf = int(patch.n_psf_per_source[b])
+            psf = patch.psfgauss[int(patch.psfgauss_start[e]):int(patch.psfgauss_start[e]) + npsf]
+            for s, p in enumerate(params):
+                flux, (ra, dec, q, pa, nser, rh) = p[b], p[nb:]
+                amps = table.amplitudes(nser, rh)
+                D = patch.D[e, s].astype(np.float64)
+                CW = patch.CW[e, s].astype(np.float64)
+                T = D @ _rot(pa) @ np.diag([1.0 / q, q])
+                cen = CW @ (np.array([ra, dec]) - patch.crval[e, s]) + patch.crpix[e, s]
+                for row in psf:
+                    k = int(row["sersic_bin"])
+                    Sig = rad2[k] * T @ T.T + np.array([[row["Cxx"], row["Cxy"]],
+                                                        [row["Cxy"], row["Cyy"]]])
+                    F = np.linalg.inv(Sig)
+                    A = patch.G[e] * row["amp"] * np.sqrt(np.linalg.det(F)) / (2 * np.pi) \
+                        * flux * amps[k]
+                    xc, yc = cen[0] + row["xcen"], cen[1] + row["ycen"]
+                    wx, wy = nsigma * np.sqrt(Sig[0, 0]), nsigma * np.sqrt(Sig[1, 1])
+                    m = (np.abs(xs - xc) < wx) & (np.abs(ys - yc) < wy)
+                    if not m.any():
+                        continue
+                    dx, dy = xs[m] - xc, ys[m] - yc
+                    vx = F[0, 0] * dx + F[0, 1] * dy
+                    vy = F[1, 1] * dy + F[0, 1] * dx
+                    H = 1 + (vx * vx + vy * vy - F[0, 0] - F[1, 1]) / 24.0
+                    model[p0:p0 + n][m] += A * np.exp(-0.5 * (dx * vx + dy * vy)) * H
+    return model
+
+
+def make_patch(spec, seed=0, table=None, render=None, return_residual=False):
+    """Draw a SyntheticPatch from ``spec``.
+
+    ``render(patch, params) -> flat model`` synthesises the truth image
+    (default :func:`render_model_numpy`); the data are that model plus noise.
+    """
+    rng = np.random.default_rng(seed)
+    table = table or default_table()
+    nb, ns = spec.n_bands, spec.n_sources
+    n_exp = sum(spec.exposures_per_band)
+    assert len(spec.shapes) == n_exp
+    P = SyntheticPatch(return_residual=return_residual)
+    P.spec, P.table = spec, table
+
+    # --- per-exposure astrometry (linear WCS about the patch centre)
+    cosd = np.cos(np.deg2rad(DEC0))
+    Dexp, CWexp, crpix0 = [], [], []
+    for e in range(n_exp):
+        phi = np.deg2rad(rng.uniform(-spec.rot_deg, spec.rot_deg)) if spec.rot_deg else 0.0
+        scl = 1.0 + (rng.uniform(-spec.scale_frac, spec.scale_frac) if spec.scale_frac else 0.0)
+        D = _rot(phi) / (PIXEL_SCALE * scl)
+        Dexp.append(D)
+        CWexp.append(D @ np.diag([3600.0 * cosd, 3600.0]))
+        nx, ny = spec.shapes[e]
+        crpix0.append(np.array([(nx - 1) / 2.0, (ny - 1) / 2.0]))
+    G = rng.uniform(*spec.g_range, size=n_exp) if spec.g_range[0] != spec.g_range[1] \
+        else np.full(n_exp, spec.g_range[0])
+
+    # --- sources (Scene order: fluxes, ra, dec, q, pa, sersic, rhalf)
+    nx0, ny0 = spec.shapes[0]
+    truth = np.zeros((ns, nb + 6))
+    for s in range(ns):
+        bright = rng.uniform() < spec.bright_fraction
+        nser = rng.uniform(*(spec.bright_sersic if bright else spec.sersic))
+        rh = rng.uniform(*(spec.bright_rh if bright else spec.rh))
+        q = rng.uniform(0.4, 1.0)
+        pa = rng.uniform(-np.pi / 2, np.pi / 2)
+        if spec.position == "centre":
+            off = rng.uniform(-0.3, 0.3, size=2)  # arcsec
+        else:
+            half = 0.45 * np.array([nx0, ny0]) * PIXEL_SCALE
+            off = rng.uniform(-half, half)
+        ra = off[0] / 3600.0 / cosd
+        dec = off[1] / 3600.0
+        fluxes = rng.lognormal(0.0, spec.flux_sigma, size=nb)
+        truth[s] = np.concatenate([fluxes, [ra, dec, q, pa, nser, rh]])
+    P.truth = truth
+    P.params = truth * (1.0 + spec.perturb)
+
+    # --- pixels
+    xs, ys, valid, exp_start, exp_n = [], [], [], [], []
+    i = 0
+    for e in range(n_exp):
+        x, y, v = _pack_exposure_pixels(*spec.shapes[e])
+        x = np.where(v, x, -1).astype(np.float32)
+        y = np.where(v, y, -1).astype(np.float32)
+        xs.append(x); ys.append(y); valid.append(v)
+        exp_start.append(i); exp_n.append(len(x))
+        i += len(x)
+    npix = i
+    P.build_patch(npix=npix, n_sources=ns, n_radii=table.n_radii, n_bands=nb, n_exp=n_exp)
+    P.xpix[:] = np.concatenate(xs)
+    P.ypix[:] = np.concatenate(ys)
+    P.exposure_start[:] = exp_start
+    P.exposure_N[:] = exp_n
+    P.band_N[:] = spec.exposures_per_band
+    P.band_start[:] = np.concatenate([[0], np.cumsum(spec.exposures_per_band)[:-1]])
+    P.original_shapes = [tuple(s) for s in spec.shapes]
+    P.original_sizes = [int(a * b) for a, b in spec.shapes]
+    validall = np.concatenate(valid)
+
+    # --- metadata: per (exposure, source) astrometry packed at the truth position
+    P.rad2[:] = table.rad2
+    for e in range(n_exp):
+        for s in range(ns):
+            sky = truth[s, nb:nb + 2]
+            P.D[e, s] = Dexp[e]
+            P.CW[e, s] = CWexp[e]
+            P.crval[e, s] = sky
+            P.crpix[e, s] = crpix0[e] + CWexp[e] @ sky
+    P.G[:] = G
+
+    # --- PSF: one mixture per exposure, repeated per radius bin and source
+    nr = table.n_radii
+    npsf = nr * spec.n_psf
+    P.n_psf_per_source[:] = npsf
+    rows = []
+    P.psfgauss_start[:] = np.arange(n_exp) * ns * npsf
+    for e in range(n_exp):
+        sig = rng.uniform(*spec.psf_sigma, size=spec.n_psf)
+        amp = rng.dirichlet(np.ones(spec.n_psf))
+        ell = rng.uniform(-0.1, 0.1, size=spec.n_psf)
+        cxy = rng.uniform(-0.05, 0.05, size=spec.n_psf) * sig ** 2
+        off = rng.normal(0.0, 0.05, size=(spec.n_psf, 2))
+        mix = np.zeros(spec.n_psf, dtype=PSF_DTYPE)
+        mix["amp"], mix["xcen"], mix["ycen"] = amp, off[:, 0], off[:, 1]
+        mix["Cxx"], mix["Cyy"], mix["Cxy"] = sig ** 2 * (1 + ell), sig ** 2 * (1 - ell), cxy
+        per_source = np.concatenate([mix.copy() for _ in range(nr)])
+        per_source["sersic_bin"] = np.repeat(np.arange(nr), spec.n_psf)
+        rows.append(np.tile(per_source, ns))
+    P.psfgauss = np.concatenate(rows).astype(PSF_DTYPE)
+
+    # --- data: truth + noise; ierr = 1/sigma per exposure; masked pixels
+    model = (render or render_model_numpy)(P, truth)
+    data = np.zeros(npix, dtype=np.float64)
+    ierr = np.zeros(npix, dtype=np.float64)
+    for e in range(n_exp):
+        sl = slice(exp_start[e], exp_start[e] + exp_n[e])
+        m = model[sl]
+        v = validall[sl]
+        peak = max(np.max(m[v]) if v.any() else 0.0, 1e-12)
+        sigma = 0.05 * peak
+        d = m + rng.normal(0.0, sigma, size=m.shape)
+        ie = np.full(m.shape, 1.0 / sigma)
+        if spec.mask_frac:
+            ie[rng.uniform(size=m.shape) < spec.mask_frac] = 0.0
+        d[~v] = 0.0
+        ie[~v] = 0.0
+        data[sl], ierr[sl] = d, ie
+    P.data[:] = data.astype(np.float32)
+    P.ierr[:] = ierr.astype(np.float32)
+    P.coerce_arrays()
+    P._dirty_data = True
+    return P
+
+
+def make_config(k, seed=0, render=None, return_residual=False, n_patches=256):
+    """Patch (or, for config 3, list of ``n_patches`` patches) of config k."""
+    if k == 3:
+        rng = np.random.default_rng(seed)
+        out = []
+        for i in range(n_patches):
+            spec = config_spec(3, rng)
+            out.append(make_patch(spec, seed=int(rng.integers(2 ** 31)), render=render,
+                                  return_residual=return_residual))
+        return out
+    return make_patch(config_spec(k), seed=seed, render=render, return_residual=return_residual)

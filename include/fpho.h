@@ -1,0 +1,209 @@
+/*
+ * fpho.h -- C ABI of forcepho_b200, a B200 (sm_100a) implementation of
+ * forcepho's proposal-evaluation hot path: given a packed patch and a proposal
+ * of Sersic source parameters, compute chi2 and dchi2/dtheta per band.
+ *
+ * Conventions
+ *   - Every entry point returns an int status (FPHO_OK == 0).  Nothing aborts;
+ *     the message of the last failure on the calling thread is returned by
+ *     fpho_last_error().
+ *   - `stream` is a cudaStream_t passed as void* (NULL = legacy default stream).
+ *     Calls are stream-ordered; a handle may be used by one host thread at a
+ *     time.
+ *   - Device memory is owned either by the caller (pointers passed in) or by
+ *     a handle, freed by the matching *_free call.
+ *   - No torch, numpy or CUDA types appear in the signatures.
+ *
+ * Struct layouts below are the reference's device ABI and are byte-compatible
+ * with it, so patches packed by the reference's python packer
+ * (forcepho/patches/patch.py:43-74) can be handed over unchanged.
+ */
+#ifndef FPHO_H
+#define FPHO_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define FPHO_API __attribute__((visibility("default")))
+#else
+#define FPHO_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Compile-time limits of the reference ABI (forcepho/src/kernel_limits.h:5-26). */
+#define FPHO_MAXBANDS 30     /* Source.fluxes length */
+#define FPHO_MAXSOURCES 30   /* Response stride of the reference (sources per band) */
+#define FPHO_NPARAMS 7       /* flux, ra, dec, q, pa, sersic, rh */
+#define FPHO_MAXRADII 10     /* Source mixture arrays length */
+#define FPHO_MAX_EXP_ARG 36.0f
+
+/* Limits of this implementation (lifted from the reference's 30 sources and
+ * 48 KB of shared memory per band). */
+#define FPHO_MAX_ACTIVE_SOURCES 1024
+#define FPHO_MAX_PSF_PER_SOURCE 1024
+
+enum fpho_status {
+    FPHO_OK = 0,
+    FPHO_ERR_INVALID = 1,   /* bad argument or inconsistent patch description */
+    FPHO_ERR_CUDA = 2,      /* a CUDA runtime call failed */
+    FPHO_ERR_NOMEM = 3,     /* host or device allocation failed */
+    FPHO_ERR_LIMIT = 4,     /* a size exceeds a limit of this implementation */
+    FPHO_ERR_STATE = 5,     /* call not valid in the handle's current state */
+    FPHO_ERR_KERNEL = 6     /* a kernel reported an error word (bounded wait ran out, bad index) */
+};
+
+/* evaluate flags */
+#define FPHO_IO_HOST 1u          /* proposal and outputs are host pointers; the call synchronizes */
+#define FPHO_WANT_RESIDUAL 2u    /* write data - model to the patch's residual array */
+
+/* One PSF Gaussian already matched to a Sersic radius bin:
+ * forcepho/src/patch.cc:101-118 (28 bytes). */
+typedef struct fpho_psfgauss {
+    float amp;
+    float xcen, ycen;
+    float Cxx, Cyy, Cxy;
+    int32_t sersic_radius_bin;
+} fpho_psfgauss;
+
+/* The patch description: forcepho/src/patch.cc:23-99 (152 bytes on LP64).
+ * Pointers are host pointers when given to fpho_patch_create and device
+ * pointers in the copy returned by fpho_patch_device_struct. */
+typedef struct fpho_patch_struct {
+    float *data, *ierr, *xpix, *ypix, *residual;
+    int32_t *exposure_start;   /* [n_exp] first pixel of each exposure */
+    int32_t *exposure_N;       /* [n_exp] pixels (with padding) of each exposure */
+    int16_t *band_start;       /* [n_bands] first exposure of each band */
+    int16_t *band_N;           /* [n_bands] exposures of each band */
+    int32_t n_sources;
+    int32_t n_radii;
+    float *rad2;               /* [n_radii] squared Sersic radii, arcsec^2 */
+    float *D;                  /* [n_exp][n_sources][2][2] pixels per arcsec */
+    float *crpix;              /* [n_exp][n_sources][2] */
+    float *crval;              /* [n_exp][n_sources][2] */
+    float *CW;                 /* [n_exp][n_sources][2][2] d(pixel)/d(ra, dec) */
+    float *G;                  /* [n_exp] flux to counts */
+    int32_t *n_psf_per_source; /* [n_bands] */
+    fpho_psfgauss *psfgauss;   /* [sum_e n_sources * n_psf_per_source[band(e)]] */
+    int32_t *psfgauss_start;   /* [n_exp] */
+} fpho_patch_struct;
+
+/* One source of a proposal: forcepho/src/proposal.cu:13-28 (264 bytes). */
+typedef struct fpho_source {
+    float ra, dec;
+    float q, pa;
+    float nsersic, rh;
+    float fluxes[FPHO_MAXBANDS];
+    float mixture_amplitudes[FPHO_MAXRADII];
+    float damplitude_drh[FPHO_MAXRADII];
+    float damplitude_dnsersic[FPHO_MAXRADII];
+} fpho_source;
+
+/* Per-band gradient block of the reference: forcepho/src/proposal.cu:33-39. */
+typedef struct fpho_response {
+    float dchi2_dparam[FPHO_MAXSOURCES * FPHO_NPARAMS];
+} fpho_response;
+
+typedef struct fpho_patch fpho_patch;   /* opaque: device copy of one patch + workspace */
+typedef struct fpho_batch fpho_batch;   /* opaque: many patches evaluated by one launch */
+
+/* ---- library ---------------------------------------------------------- */
+
+/* Message of the last failure on this thread ("" if none). */
+FPHO_API const char *fpho_last_error(void);
+/* ABI version: (major << 16) | minor. */
+FPHO_API int fpho_abi_version(void);
+/* sizeof checks for bindings: 0 patch_struct, 1 source, 2 psfgauss, 3 response. */
+FPHO_API int fpho_sizeof(int which);
+
+/* ---- patches ---------------------------------------------------------- */
+
+/* Copy every array referenced by the host-side patch description to the
+ * device and prepare the tile plan.  Replaces GPUPatchMixin.send_to_device
+ * (forcepho/patches/device_patch.py:268-300).  n_bands is the number of
+ * bands (the reference passes it as the grid size).  If `return_residual` is
+ * non-zero a device residual array is allocated (host->residual is ignored).
+ * Sizes are derived from the index arrays; they are validated on the host. */
+FPHO_API int fpho_patch_create(const fpho_patch_struct *host, int n_bands, int return_residual,
+                      void *stream, fpho_patch **out);
+
+/* Replace the per-scene metadata (n_sources, rad2, D, crpix, crval, CW, G,
+ * n_psf_per_source, psfgauss, psfgauss_start) with new host arrays, keeping
+ * the pixel arrays.  Replaces GPUPatchMixin.replace_device_meta_ptrs
+ * (device_patch.py:302-311). */
+FPHO_API int fpho_patch_replace_meta(fpho_patch *p, const fpho_patch_struct *host, void *stream);
+
+/* Swap the device data and residual arrays, so that the residual of the last
+ * evaluation becomes the data.  Replaces the pointer swap of
+ * GPUPatchMixin.swap_on_device (device_patch.py:346-367); call
+ * fpho_patch_replace_meta before it to install the next scene's metadata. */
+FPHO_API int fpho_patch_swap_data_residual(fpho_patch *p, void *stream);
+
+/* Copy one pixel array to host memory (npix floats).  which: 0 data,
+ * 1 residual, 2 ierr, 3 xpix, 4 ypix.  Replaces GPUPatchMixin.retrieve_array
+ * (device_patch.py:369-375).  Synchronizes `stream`. */
+FPHO_API int fpho_patch_retrieve(fpho_patch *p, int which, float *host_out, void *stream);
+
+/* Device pointer to a fpho_patch_struct (device pointers inside) describing
+ * the patch, as GPUPatchMixin.device_patch (device_patch.py:313-344). */
+FPHO_API int fpho_patch_device_struct(fpho_patch *p, const void **dev_struct);
+
+/* Sizes: out[0] n_bands, out[1] n_exp, out[2] npix, out[3] n_sources,
+ * out[4] n_radii, out[5] n_tiles, out[6] total image Gaussians. */
+FPHO_API int fpho_patch_info(const fpho_patch *p, int64_t out[7]);
+
+FPHO_API int fpho_patch_free(fpho_patch *p);
+
+/* ---- evaluation ------------------------------------------------------- */
+
+/* Evaluate a proposal on a patch: chi2 per band and dchi2/dtheta per band
+ * and source.  Replaces the launch EvaluateProposal<<<n_bands, 1024, 48000>>>
+ * (forcepho/src/compute_gaussians_kernel.cu:212-312) made by
+ * GPUProposer.evaluate_proposal (forcepho/proposal.py:96-152).
+ *   proposal  fpho_source[n_sources]
+ *   chi2      double[n_bands]: sum over the band's pixels of
+ *             (r*ie - d*ie)(r*ie + d*ie), r = data - model
+ *   dchi2     float[n_bands][dchi2_stride]: dchi2[b][7*s + k] for source s and
+ *             parameter k in (flux, ra, dec, q, pa, sersic, rh);
+ *             dchi2_stride >= 7*n_sources (210 gives the reference's
+ *             fpho_response layout; entries past 7*n_sources are zeroed).
+ *   flags     FPHO_IO_HOST, FPHO_WANT_RESIDUAL
+ * n_sources must equal the patch's n_sources. */
+FPHO_API int fpho_evaluate_proposal(fpho_patch *p, const fpho_source *proposal, int n_sources,
+                           double *chi2, float *dchi2, int dchi2_stride,
+                           unsigned flags, void *stream);
+
+/* The reference kernel's exact argument list: a device fpho_patch_struct*
+ * (as returned by fpho_patch_device_struct for this handle), a device
+ * Source[n_sources], a device double[n_bands] and a device
+ * fpho_response[n_bands].  Same computation as fpho_evaluate_proposal. */
+FPHO_API int fpho_EvaluateProposal(fpho_patch *p, const void *dev_patch_struct, const void *dev_proposal,
+                          void *pchi2, void *pdchi2_dp, void *stream);
+
+/* Read (and keep) the error word of the last evaluation: bit 0 set when a
+ * bounded wait on a bulk copy gave up.  Synchronizes the device. */
+FPHO_API int fpho_patch_error_word(fpho_patch *p, int *out);
+
+/* ---- tuning (no counterpart in the reference) --------------------------- */
+
+/* Number of compiled tile-kernel variants; out[0] threads per CTA and out[1]
+ * pixels per thread of `variant`. */
+FPHO_API int fpho_variant_info(int variant, int out[2]);
+
+/* Select the tile-kernel variant and the shared-memory stage size (image
+ * Gaussians per chunk) used by this patch; re-plans the tiles if the tile
+ * size changes. */
+FPHO_API int fpho_patch_set_config(fpho_patch *p, int variant, int live_cap, void *stream);
+
+/* Enable counting of evaluated (pixel, image Gaussian) pairs, i.e. pairs that
+ * survive the per-tile culling; *last_count receives the count of the last
+ * evaluation (synchronizes).  last_count may be NULL. */
+FPHO_API int fpho_patch_count_pairs(fpho_patch *p, int enable, long long *last_count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FPHO_H */
