@@ -1,0 +1,367 @@
+#!/usr/bin/env python
+"""Benchmark of the proposal-evaluation hot path on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: the realistic plain patch (20 Sersic sources, 8 bands x 4
+exposures of 128x128 px, 5-Gaussian PSFs, 9 mixture radii: 524,288 pixels x
+900 image Gaussians per exposure = 4.72e8 pixel-Gaussian pairs per
+evaluation), synthetic and seeded (forcepho_b200.synth, config 1).  A step is
+one chi2 + gradient evaluation of one proposal on that patch.  With N GPUs
+(torchrun) every rank evaluates its own copy of the patch (independent
+patches: weak scaling, no collective on the data path).
+
+Printed JSON (rank 0):
+  value      evaluations/s over all ranks, inputs resident in HBM, CUDA-event
+             timed per step with an L2 flush between steps (max over ranks);
+  e2e        the same through GPUProposer.evaluate_proposal with the proposal
+             in pinned host memory and results copied back every step;
+  roofline   the pixel-tile kernel: algorithmic FP32 flops (105 per evaluated
+             pixel-Gaussian pair) / its CUDA-event time, against the FP32 FMA
+             throughput measured live by a probe kernel on the same GPU;
+  cpu_baseline  the reference's own CPU kernel (built from its sources into
+             oracle/_ref) on all host cores, one evaluation of the same patch.
+The reference arm (--impl reference) times that CPU kernel over K steps.
+"""
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "chi2+grad evals/s & pix·gauss/s: batched vs plain, 1 B200, rel err ≤1e-6"
+FLOPS_PER_PAIR = 105          # 18 (model) + 87 (gradient) FP32 flops, FMA = 2
+WORKLOAD = "config1: 20 src, 8 bands x 4 exp x 128x128 px, 5-gauss PSF, 9 radii"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default 1000 on the GPU, 20 for the CPU reference)")
+    ap.add_argument("--warmup", type=int, default=None,
+                    help="untimed warm-up steps (default 20 on the GPU, 3 for the reference)")
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--variant", type=int, default=None)
+    ap.add_argument("--live-cap", type=int, default=None)
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """Samples SM clock and throttle reasons with nvidia-smi from a thread,
+    one query at a time, for as long as the context is open (plus one sample
+    on entry and one on exit)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        import threading
+        self.idx = gpu_index
+        self.lines = []
+        self._stop = threading.Event()
+        self._thread = threading.Thread(target=self._run, daemon=True)
+
+    def _query(self):
+        try:
+            out = subprocess.run(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
+                                  "--format=csv,noheader,nounits"], capture_output=True,
+                                 text=True, timeout=10).stdout
+            self.lines.extend(ln for ln in out.splitlines() if ln.strip())
+        except (OSError, subprocess.SubprocessError):
+            pass
+
+    def _run(self):
+        while not self._stop.is_set():
+            self._query()
+            self._stop.wait(0.05)
+
+    def __enter__(self):
+        self._thread.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._thread.join(timeout=15)
+        self._query()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in getattr(self, "lines", []):
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ CPU reference
+def cpu_reference_time(P, prop, reps, cores):
+    """Seconds per full evaluation (all bands) of the reference CPU kernel,
+    bands spread over `cores` spawn worker processes."""
+    from oracle import oracle as O
+    if not O.ref_available(P.n_sources):
+        O.build()
+    pool = O.ref_pool(P.n_sources, cores)
+    try:
+        O.ref_evaluate(P, prop, pool=pool)  # warm-up (loads the module everywhere)
+        times = []
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            O.ref_evaluate(P, prop, pool=pool)
+            times.append(time.perf_counter() - t0)
+    finally:
+        pool.close()
+        pool.join()
+    return times
+
+
+def make_workload(seed, device_render):
+    from forcepho_b200 import synth
+    render = synth.render_model_gpu if device_render else None
+    return synth.make_config(1, seed=seed, render=render)
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    P = make_workload(args.seed, device_render=False)
+    prop = P.proposal()
+    cores = len(os.sched_getaffinity(0))
+    times = cpu_reference_time(P, prop, args.warmup + args.steps, min(cores, P.n_bands))
+    t = times[args.warmup:]
+    sec = float(np.mean(t))
+    value = 1.0 / sec
+    line = {
+        "metric": METRIC, "value": value, "unit": "evals/s", "impl": "reference",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "pairs_per_eval": P.pairs_per_eval},
+        "pix_gauss_per_s": P.pairs_per_eval * value,
+        "cpu_baseline": {"value": value, "unit": "evals/s", "cores": min(cores, P.n_bands),
+                         "kind": "reference",
+                         "sample": "one full evaluation (8 bands, one band per process) per step"},
+        "e2e": {"value": value, "unit": "evals/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ------------------------------------------------------------------ GPU arm
+def probe_fp32(torch, lib):
+    """Measured FP32 FMA (TFLOP/s) and MUFU.EX2 (Gop/s) throughput."""
+    dev = torch.cuda.current_device()
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    out = torch.zeros(sms * 16, device="cuda")
+    s = torch.cuda.current_stream()
+    res = {}
+    for which, iters, per in ((0, 4096, 32), (1, 1024, 8)):
+        blocks, threads = sms * 8, 256
+        for rep in range(3):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            lib.call("fpho_probe_launch", which, blocks, threads, iters, out.data_ptr(),
+                     s.cuda_stream)
+            e1.record(s)
+            torch.cuda.synchronize()
+            rate = blocks * threads * iters * per / (e0.elapsed_time(e1) * 1e-3)
+            res[which] = max(res.get(which, 0.0), rate)
+    return res[0] / 1e12, res[1] / 1e9
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    from forcepho_b200 import _lib
+    from forcepho_b200.proposal import GPUProposer
+    from forcepho_b200.autotune import choose_config
+
+    P = make_workload(args.seed, device_render=True)
+    prop = P.proposal()
+    P.return_residual = False
+    P.send_to_device()
+    dp = P.device_patch
+    cfg = choose_config(P, variant=args.variant, live_cap=args.live_cap)
+    dp.set_config(cfg["variant"], cfg["live_cap"])
+    stream = torch.cuda.current_stream()
+    sp = stream.cuda_stream
+
+    dprop = torch.from_numpy(prop.view(np.uint8).copy()).cuda()
+    nb, ns = P.n_bands, P.n_sources
+    chi2 = torch.zeros(nb, dtype=torch.float64, device="cuda")
+    dchi2 = torch.zeros(nb * ns * 7, dtype=torch.float32, device="cuda")
+
+    def step():
+        _lib.call("fpho_evaluate_proposal", dp.handle, dprop.data_ptr(), ns, chi2.data_ptr(),
+                  dchi2.data_ptr(), 7 * ns, 0, sp)
+
+    # evaluated pairs (after per-tile culling), counted once
+    _lib.call("fpho_patch_count_pairs", dp.handle, 1, None)
+    step()
+    torch.cuda.synchronize()
+    import ctypes
+    cnt = ctypes.c_longlong()
+    _lib.call("fpho_patch_count_pairs", dp.handle, 0, ctypes.byref(cnt))
+    evaluated_pairs = int(cnt.value)
+
+    # L2 (126 MB) is flushed between timed steps by writing 256 MB; the flush
+    # sits between the step's events, outside the timed intervals.
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        for e0, e1 in evs:
+            flush.zero_()
+            e0.record(stream)
+            step()
+            e1.record(stream)
+        torch.cuda.synchronize()
+    step_ms = [e0.elapsed_time(e1) for e0, e1 in evs]
+    if world > 1:
+        dist.barrier()
+
+    # the dominant kernel alone: events recorded by the library around it
+    _lib.call("fpho_patch_time_tiles", dp.handle, 1)
+    tms = ctypes.c_float()
+    tile_ms = []
+    for _ in range(min(args.steps, 50)):
+        flush.zero_()
+        step()
+        _lib.call("fpho_patch_last_tile_ms", dp.handle, ctypes.byref(tms))
+        tile_ms.append(tms.value)
+    _lib.call("fpho_patch_time_tiles", dp.handle, 0)
+
+    total_ms = float(np.sum(step_ms))
+    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = world * args.steps / (total_ms * 1e-3)
+
+    # end-to-end through the public API: pinned host proposal -> results on host
+    hprop = torch.from_numpy(prop.view(np.uint8).copy()).pin_memory()
+    hchi2 = torch.zeros(nb, dtype=torch.float64).pin_memory()
+    hdchi2 = torch.zeros(nb * ns * 7, dtype=torch.float32).pin_memory()
+
+    def e2e_step():
+        _lib.call("fpho_evaluate_proposal", dp.handle, hprop.data_ptr(), ns, hchi2.data_ptr(),
+                  hdchi2.data_ptr(), 7 * ns, _lib.FPHO_IO_HOST, sp)
+
+    for _ in range(args.warmup):
+        e2e_step()
+    if world > 1:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    e2e_s = time.perf_counter() - t0
+    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world * args.steps / float(te.item())
+
+    fp32_tflops, ex2_gops = probe_fp32(torch, _lib)
+    tile_s = float(np.mean(tile_ms)) * 1e-3
+    achieved = evaluated_pairs * FLOPS_PER_PAIR / tile_s / 1e12
+    sfu = evaluated_pairs * 2 / tile_s / 1e9
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cores = len(os.sched_getaffinity(0))
+        use = min(cores, nb)
+        times = cpu_reference_time(P, prop, 3, use)
+        cpu = {"value": 1.0 / float(np.mean(times)), "unit": "evals/s", "cores": use,
+               "kind": "reference",
+               "sample": "3 full evaluations of the same patch (8 bands, one band per "
+                         f"process on {use} of {cores} host cores)"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "evals/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD, "pairs_per_eval": P.pairs_per_eval,
+                       "evaluated_pairs": evaluated_pairs, "l2": "flushed between steps",
+                       "tile_variant": list(_lib.variants()[cfg["variant"]]),
+                       "live_cap": cfg["live_cap"], "parallelism": f"patch-parallel x{world}"},
+            "pix_gauss_per_s": P.pairs_per_eval * value,
+            "evaluated_pix_gauss_per_s": evaluated_pairs * value,
+            "e2e": {"value": e2e_value, "unit": "evals/s",
+                    "h2d_bytes_per_step": int(prop.nbytes),
+                    "d2h_bytes_per_step": int(nb * 8 + nb * ns * 7 * 4 + 4)},
+            "gpu_launches": 3 * args.steps,
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_tflops,
+                         "unit": "TFLOP/s", "frac": achieved / fp32_tflops,
+                         "traffic": None,
+                         "peak_source": "measured live: packed FP32 FMA probe kernel",
+                         "kernel": "tile_kernel", "kernel_ms": tile_s * 1e3,
+                         "sfu_gops": sfu, "sfu_peak_gops": ex2_gops, "sfu_frac": sfu / ex2_gops},
+            "clocks": clk.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    P.free()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    ref = args.impl == "reference"
+    if args.steps is None:
+        args.steps = 20 if ref else 1000
+    if args.warmup is None:
+        args.warmup = 3 if ref else 20
+    args.warmup = max(args.warmup, 3)
+    if ref:
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -63,6 +63,11 @@ _SIGS = {
                                        c_uint, c_void_p]),
     "fpho_EvaluateProposal": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                       c_void_p]),
+    "fpho_patch_time_tiles": (c_int, [c_void_p, c_int]),
+    "fpho_patch_image_gaussians": (c_int, [c_void_p, c_int, c_void_p, c_int,
+                                           ctypes.POINTER(c_int)]),
+    "fpho_patch_last_tile_ms": (c_int, [c_void_p, ctypes.POINTER(ctypes.c_float)]),
+    "fpho_probe_launch": (c_int, [c_int, c_int, c_int, c_int, c_void_p, c_void_p]),
 }
 
 

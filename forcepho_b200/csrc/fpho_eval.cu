@@ -231,7 +231,11 @@ struct fpho_patch {
     int *d_err = nullptr;
     long long *d_pairs = nullptr;
     int count_pairs = 0;
+    // optional events recorded around the tile kernel (timing of the dominant kernel)
+    cudaEvent_t ev_tile0 = nullptr, ev_tile1 = nullptr;
 };
+
+static void destroy_patch(fpho_patch *p);
 
 namespace {
 
@@ -289,6 +293,8 @@ int read_pixel_index(fpho_patch *p, const fpho_patch_struct *h, int n_bands) {
         n_exp = std::max(n_exp, (int)p->band_start[b] + (int)p->band_N[b]);
     }
     if (n_exp < 1) return set_error(FPHO_ERR_INVALID, "patch has no exposures");
+    if (n_exp > 65535)  // exposures index gridDim.y of the image-Gaussian kernel
+        return set_error(FPHO_ERR_LIMIT, "n_exp=%d exceeds 65535", n_exp);
     p->n_exp = n_exp;
     p->exposure_start.assign(h->exposure_start, h->exposure_start + n_exp);
     p->exposure_N.assign(h->exposure_N, h->exposure_N + n_exp);
@@ -312,7 +318,8 @@ int read_pixel_index(fpho_patch *p, const fpho_patch_struct *h, int n_bands) {
 }
 
 // Validate and upload the per-scene metadata; derive the image-Gaussian index.
-int upload_meta(fpho_patch *p, const fpho_patch_struct *h, cudaStream_t s) {
+int upload_meta(fpho_patch *p, const fpho_patch_struct *h, cudaStream_t s,
+                bool validate_only = false) {
     if (!h->rad2 || !h->D || !h->crpix || !h->crval || !h->CW || !h->G || !h->n_psf_per_source ||
         !h->psfgauss || !h->psfgauss_start)
         return set_error(FPHO_ERR_INVALID, "a metadata array pointer is NULL");
@@ -352,6 +359,7 @@ int upload_meta(fpho_patch *p, const fpho_patch_struct *h, cudaStream_t s) {
                                  "psfgauss[%d].sersic_radius_bin=%d outside [0, n_radii=%d)",
                                  pstart[e] + q, k, nrad);
         }
+    if (validate_only) return FPHO_OK;
     free_meta(p);
     p->n_sources = nsrc;
     p->n_radii = nrad;
@@ -471,6 +479,8 @@ extern "C" int fpho_patch_create(const fpho_patch_struct *host, int n_bands, int
     fpho_patch *p = new (std::nothrow) fpho_patch();
     if (!p) return set_error(FPHO_ERR_NOMEM, "host allocation failed");
     int rc = read_pixel_index(p, host, n_bands);
+    // every host-side check happens before the first CUDA call
+    if (!rc) rc = upload_meta(p, host, s, /*validate_only=*/true);
     if (!rc) {
         const size_t np = (size_t)p->npix;
         if (!rc) rc = dupload(&p->d_data, host->data, np, s);
@@ -495,7 +505,7 @@ extern "C" int fpho_patch_create(const fpho_patch_struct *host, int n_bands, int
     if (!rc) rc = build_plan(p, s);
     if (!rc) rc = refresh_struct(p, s);
     if (rc) {
-        fpho_patch_free(p);
+        destroy_patch(p);
         return rc;
     }
     *out = p;
@@ -561,16 +571,21 @@ extern "C" int fpho_patch_info(const fpho_patch *p, int64_t out[7]) {
     return FPHO_OK;
 }
 
-extern "C" int fpho_patch_free(fpho_patch *p) {
-    clear_error();
-    if (!p) return FPHO_OK;
+static void destroy_patch(fpho_patch *p) {
     free_meta(p);
     free_plan(p);
     dfree(p->d_data); dfree(p->d_ierr); dfree(p->d_xpix); dfree(p->d_ypix); dfree(p->d_residual);
     dfree(p->d_exposure_start); dfree(p->d_exposure_N); dfree(p->d_band_start);
     dfree(p->d_band_N); dfree(p->d_struct); dfree(p->d_chi2_out); dfree(p->d_dchi2_out);
     dfree(p->d_err); dfree(p->d_pairs);
+    if (p->ev_tile0) cudaEventDestroy(p->ev_tile0);
+    if (p->ev_tile1) cudaEventDestroy(p->ev_tile1);
     delete p;
+}
+
+extern "C" int fpho_patch_free(fpho_patch *p) {
+    clear_error();
+    if (p) destroy_patch(p);
     return FPHO_OK;
 }
 
@@ -647,8 +662,10 @@ int enqueue_evaluate(fpho_patch *p, const fpho_source *d_prop, double *d_chi2, f
     A.live_cap = p->live_cap;
     A.err = p->d_err;
     A.pairs = p->count_pairs ? p->d_pairs : nullptr;
+    if (p->ev_tile0) CUDA_TRY(cudaEventRecord(p->ev_tile0, s));
     int rc = launch_tile_kernel(p->variant, A, p->n_tiles, s);
     if (rc) return rc;
+    if (p->ev_tile1) CUDA_TRY(cudaEventRecord(p->ev_tile1, s));
     dim3 rg(p->n_bands, (out_stride + 127) / 128);
     reduce_bands<<<rg, 128, 0, s>>>(p->d_tile_band_start, p->d_pchi2, p->d_pgrad,
                                     7 * p->n_sources, d_chi2, d_dchi2, out_stride);
@@ -713,6 +730,44 @@ extern "C" int fpho_EvaluateProposal(fpho_patch *p, const void *dev_patch_struct
     return enqueue_evaluate(p, (const fpho_source *)dev_proposal, (double *)pchi2,
                             (float *)pdchi2_dp, FPHO_MAXSOURCES * FPHO_NPARAMS,
                             p->d_residual != nullptr, (cudaStream_t)stream);
+}
+
+extern "C" int fpho_patch_image_gaussians(fpho_patch *p, int exposure, float *host_out,
+                                          int max_records, int *n_out) {
+    clear_error();
+    if (!p || !host_out || !n_out) return set_error(FPHO_ERR_INVALID, "NULL argument");
+    if (exposure < 0 || exposure >= p->n_exp)
+        return set_error(FPHO_ERR_INVALID, "exposure %d not in [0, %d)", exposure, p->n_exp);
+    const int g0 = p->gauss_start[exposure], n = p->gauss_start[exposure + 1] - g0;
+    if (n > max_records) return set_error(FPHO_ERR_LIMIT, "exposure has %d records", n);
+    CUDA_TRY(cudaDeviceSynchronize());
+    CUDA_TRY(cudaMemcpy(host_out, p->d_gtab + (size_t)g0 * GREC, (size_t)n * GREC * sizeof(float),
+                        cudaMemcpyDeviceToHost));
+    *n_out = n;
+    return FPHO_OK;
+}
+
+extern "C" int fpho_patch_time_tiles(fpho_patch *p, int enable) {
+    clear_error();
+    if (!p) return set_error(FPHO_ERR_INVALID, "NULL patch");
+    if (enable && !p->ev_tile0) {
+        CUDA_TRY(cudaEventCreate(&p->ev_tile0));
+        CUDA_TRY(cudaEventCreate(&p->ev_tile1));
+    } else if (!enable && p->ev_tile0) {
+        cudaEventDestroy(p->ev_tile0);
+        cudaEventDestroy(p->ev_tile1);
+        p->ev_tile0 = p->ev_tile1 = nullptr;
+    }
+    return FPHO_OK;
+}
+
+extern "C" int fpho_patch_last_tile_ms(fpho_patch *p, float *ms) {
+    clear_error();
+    if (!p || !ms) return set_error(FPHO_ERR_INVALID, "NULL argument");
+    if (!p->ev_tile0) return set_error(FPHO_ERR_STATE, "tile timing is not enabled");
+    CUDA_TRY(cudaEventSynchronize(p->ev_tile1));
+    CUDA_TRY(cudaEventElapsedTime(ms, p->ev_tile0, p->ev_tile1));
+    return FPHO_OK;
 }
 
 extern "C" int fpho_patch_error_word(fpho_patch *p, int *out) {

@@ -63,24 +63,52 @@ struct TileDesc {
 };
 
 // ---------------------------------------------------------------- 2x2 algebra
-// Row-major 2x2 matrix (a b / c d), the operations of forcepho/src/matrix22.cc.
+// Row-major 2x2 matrix (a b / c d) and the operations of
+// forcepho/src/matrix22.cc, written with round-to-nearest intrinsics so that no
+// multiply-add is contracted: the image-Gaussian parameters then equal, bit for
+// bit, the ones the reference CPU kernel builds (compiled without FMA).
 struct M22 {
     float a, b, c, d;
 };
-__host__ __device__ __forceinline__ M22 mmul(M22 A, M22 B) {
-    return {A.a * B.a + A.b * B.c, A.a * B.b + A.b * B.d, A.c * B.a + A.d * B.c,
-            A.c * B.b + A.d * B.d};
+__device__ __forceinline__ float fm(float x, float y) { return __fmul_rn(x, y); }
+__device__ __forceinline__ float fa(float x, float y) { return __fadd_rn(x, y); }
+__device__ __forceinline__ float fs(float x, float y) { return __fsub_rn(x, y); }
+// x*y + z*w without contraction
+__device__ __forceinline__ float dot2(float x, float y, float z, float w) {
+    return fa(fm(x, y), fm(z, w));
 }
-__host__ __device__ __forceinline__ M22 mscal(float s, M22 A) {
-    return {s * A.a, s * A.b, s * A.c, s * A.d};
+__device__ __forceinline__ M22 mmul(M22 A, M22 B) {       // matrix22.cc:136-139
+    return {dot2(A.a, B.a, A.b, B.c), dot2(A.a, B.b, A.b, B.d), dot2(A.c, B.a, A.d, B.c),
+            dot2(A.c, B.b, A.d, B.d)};
+}
+__device__ __forceinline__ M22 mscal(float s, M22 A) {    // matrix22.cc:120-125
+    return {fm(s, A.a), fm(s, A.b), fm(s, A.c), fm(s, A.d)};
+}
+__device__ __forceinline__ M22 symabt(M22 A, M22 B) {     // matrix22.cc:164-167
+    const float t = fa(fa(fa(fm(A.a, B.c), fm(A.b, B.d)), fm(A.c, B.a)), fm(A.d, B.b));
+    return {fm(2.0f, dot2(A.a, B.a, A.b, B.b)), t, t, fm(2.0f, dot2(A.c, B.c, A.d, B.d))};
+}
+__device__ __forceinline__ M22 aba(M22 A, M22 B) {        // matrix22.cc:144-150
+    M22 r;
+    r.a = fa(fa(fa(fm(fm(A.a, A.a), B.a), fm(fm(A.a, A.c), B.b)), fm(fm(A.a, A.b), B.c)),
+             fm(fm(A.b, A.c), B.d));
+    r.b = fa(fa(fa(fm(fm(A.a, A.b), B.a), fm(fm(A.a, A.d), B.b)), fm(fm(A.b, A.b), B.c)),
+             fm(fm(A.b, A.d), B.d));
+    r.c = fa(fa(fa(fm(fm(A.a, A.c), B.a), fm(fm(A.c, A.c), B.b)), fm(fm(A.a, A.d), B.c)),
+             fm(fm(A.c, A.d), B.d));
+    r.d = fa(fa(fa(fm(fm(A.b, A.c), B.a), fm(fm(A.c, A.d), B.b)), fm(fm(A.b, A.d), B.c)),
+             fm(fm(A.d, A.d), B.d));
+    return r;
 }
 
 // Build image Gaussian (exposure e, source s, PSF component p): sky Gaussian of
 // radius bin k convolved with PSF Gaussian p, with its Jacobian.
 // Follows GetGaussianAndJacobian (forcepho/src/common_kernel.cc:175-240) and
-// ConvolveOneSource (forcepho/src/compute_gaussians_kernel.cc:45-114),
-// including the PSF row index psfgauss[psfgauss_start[e] + p] used for every
-// source.  Writes one record and one culling box.
+// ConvolveOneSource (forcepho/src/compute_gaussians_kernel.cc:45-114) in the
+// same operation order, including the PSF row index
+// psfgauss[psfgauss_start[e] + p] used for every source.  cos/sin of the
+// position angle are evaluated in double and rounded once.  Writes one record
+// and one culling box.
 __device__ __forceinline__ void build_one_gaussian(const PatchView &pv, const fpho_source *src,
                                                    int e, int s, int p, float *rec, float4 *box) {
     const int band = pv.exp_band[e];
@@ -92,66 +120,67 @@ __device__ __forceinline__ void build_one_gaussian(const PatchView &pv, const fp
 
     const float G = pv.G[e];
     const float q = gal.q;
-    float sn, cs;
-    sincosf(gal.pa, &sn, &cs);
+    double sd, cd;
+    sincos((double)gal.pa, &sd, &cd);
+    const float sn = (float)sd, cs = (float)cd;
     const M22 D = {pv.D[dcw], pv.D[dcw + 1], pv.D[dcw + 2], pv.D[dcw + 3]};
     const M22 R = {cs, -sn, sn, cs};
-    const M22 S = {1.0f / q, 0.0f, 0.0f, q};
-    const M22 dS = {-1.0f / (q * q), 0.0f, 0.0f, 1.0f};
+    const M22 S = {__fdiv_rn(1.0f, q), 0.0f, 0.0f, q};
+    const M22 dS = {__fdiv_rn(-1.0f, fm(q, q)), 0.0f, 0.0f, 1.0f};
     const M22 dR = {-sn, -cs, cs, -sn};
     const M22 DR = mmul(D, R);
     const M22 T = mmul(DR, S);
     const M22 dTq = mmul(DR, dS);
     const M22 dTpa = mmul(mmul(D, dR), S);
     const M22 CW = {pv.CW[dcw], pv.CW[dcw + 1], pv.CW[dcw + 2], pv.CW[dcw + 3]};
-    const float s0 = gal.ra - pv.crval[cr];
-    const float s1 = gal.dec - pv.crval[cr + 1];
-    const float xs = CW.a * s0 + CW.b * s1 + pv.crpix[cr];
-    const float ys = CW.c * s0 + CW.d * s1 + pv.crpix[cr + 1];
+    const float s0 = fs(gal.ra, pv.crval[cr]);
+    const float s1 = fs(gal.dec, pv.crval[cr + 1]);
+    const float xs = fa(dot2(CW.a, s0, CW.b, s1), pv.crpix[cr]);
+    const float ys = fa(dot2(CW.c, s0, CW.d, s1), pv.crpix[cr + 1]);
 
     const float r2 = pv.rad2[k];
     const float samp = gal.mixture_amplitudes[k];
     const float flux = gal.fluxes[band];
 
     // Sigma = r2 T T^t + C_psf ; F = Sigma^-1
-    const float t12 = T.a * T.c + T.b * T.d;
-    const M22 Sig = {r2 * (T.a * T.a + T.b * T.b) + pg.Cxx, r2 * t12 + pg.Cxy,
-                     r2 * t12 + pg.Cxy, r2 * (T.c * T.c + T.d * T.d) + pg.Cyy};
-    const float idet = 1.0f / (Sig.a * Sig.d - Sig.b * Sig.c);
-    const M22 F = {Sig.d * idet, -Sig.b * idet, -Sig.c * idet, Sig.a * idet};
-    const float detF = F.a * F.d - F.b * F.c;
-    const float tmp = G * pg.amp * sqrtf(detF) * (1.0f / (2.0f * 3.14159265358979323846f));
-    const float amp = tmp * flux * samp;
+    const float t12 = dot2(T.a, T.c, T.b, T.d);
+    const M22 TTt = {dot2(T.a, T.a, T.b, T.b), t12, t12, dot2(T.c, T.c, T.d, T.d)};
+    const M22 sc = mscal(r2, TTt);
+    const M22 Sig = {fa(sc.a, pg.Cxx), fa(sc.b, pg.Cxy), fa(sc.c, pg.Cxy), fa(sc.d, pg.Cyy)};
+    const float idet = __fdiv_rn(1.0f, fs(fm(Sig.a, Sig.d), fm(Sig.b, Sig.c)));
+    const M22 F = {fm(Sig.d, idet), fm(-Sig.b, idet), fm(-Sig.c, idet), fm(Sig.a, idet)};
+    const float detF = fs(fm(F.a, F.d), fm(F.b, F.c));
+    const float tmp = fm(fm(fm(G, pg.amp), __fsqrt_rn(detF)),
+                         (1.0f / (2.0f * 3.14159265358979323846f)));
+    const float amp = fm(fm(tmp, flux), samp);
 
-    // dSigma/dq = r2 (T dT^t + dT T^t), dF = -F dSigma F, dA = amp/2 tr(Sigma dF)
+    // dSigma/dq = r2 symABt(T, dT); dF = -F dSigma F; dA = amp/2 tr(Sigma dF)
     float jF[2][3], jA[2];
     {
         const M22 dTs[2] = {dTq, dTpa};
 #pragma unroll
         for (int w = 0; w < 2; ++w) {
-            const M22 B = dTs[w];
-            const float o = T.a * B.c + T.b * B.d + T.c * B.a + T.d * B.b;
-            const M22 dSig = mscal(r2, M22{2.0f * (T.a * B.a + T.b * B.b), o, o,
-                                           2.0f * (T.c * B.c + T.d * B.d)});
-            const M22 dF = mscal(-1.0f, mmul(mmul(F, dSig), F));
+            const M22 dSig = mscal(r2, symabt(T, dTs[w]));
+            const M22 dF = mscal(-1.0f, aba(F, dSig));
             const M22 M = mmul(Sig, dF);
-            jA[w] = 0.5f * amp * (M.a + M.d);
+            jA[w] = fm(fm(0.5f, amp), fa(M.a, M.d));
             jF[w][0] = dF.a;  // fxx
             jF[w][1] = dF.c;  // fxy
             jF[w][2] = dF.d;  // fyy
         }
     }
 
-    const float xc = xs + pg.xcen;
-    const float yc = ys + pg.ycen;
+    const float xc = fa(xs, pg.xcen);
+    const float yc = fa(ys, pg.ycen);
     const float c0 = 1.0f - (F.a + F.d) * (1.0f / 24.0f);
+    const float tf = fm(tmp, flux);
 
     float4 *r4 = reinterpret_cast<float4 *>(rec);
     r4[0] = make_float4(-xc, -yc, F.a, F.c);
     r4[1] = make_float4(F.d, -amp * (1.0f / 24.0f), -amp * c0, c0);
     r4[2] = make_float4(__int_as_float(s), amp, Sig.a, Sig.d);
-    r4[3] = make_float4(tmp * samp, jA[0], jA[1], tmp * flux * gal.damplitude_dnsersic[k]);
-    r4[4] = make_float4(tmp * flux * gal.damplitude_drh[k], amp * CW.a, amp * CW.c, amp * CW.b);
+    r4[3] = make_float4(fm(tmp, samp), jA[0], jA[1], fm(tf, gal.damplitude_dnsersic[k]));
+    r4[4] = make_float4(fm(tf, gal.damplitude_drh[k]), amp * CW.a, amp * CW.c, amp * CW.b);
     r4[5] = make_float4(amp * CW.d, amp * jF[0][0], amp * jF[0][1], amp * jF[0][2]);
     r4[6] = make_float4(amp * jF[1][0], amp * jF[1][1], amp * jF[1][2], 0.0f);
     r4[7] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);

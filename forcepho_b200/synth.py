@@ -203,6 +203,26 @@ def render_model_numpy(patch, params, nsigma=7.0):
     return model
 
 
+def render_model_gpu(patch, params):
+    """Model image of Scene-ordered params evaluated by the CUDA path itself
+    (residual output with zero data: model = -residual)."""
+    from .proposal import GPUProposer
+    data, ierr = patch.data, patch.ierr
+    patch.data = np.zeros_like(patch.xpix)
+    patch.ierr = np.ones_like(patch.xpix)
+    orig = patch.return_residual
+    patch.return_residual = True
+    try:
+        patch.send_to_device()
+        prop = proposal_from_params(params, patch.n_bands, patch.table)
+        _, _, res = GPUProposer().evaluate_proposal(prop, patch=patch, unpack=False)
+    finally:
+        patch.free()
+        patch.data, patch.ierr = data, ierr
+        patch.return_residual = orig
+    return -res.astype(np.float64)
+
+
 def make_patch(spec, seed=0, table=None, render=None, return_residual=False):
     """Draw a SyntheticPatch from ``spec``.
 

@@ -203,6 +203,26 @@ FPHO_API int fpho_patch_set_config(fpho_patch *p, int variant, int live_cap, voi
  * evaluation (synchronizes).  last_count may be NULL. */
 FPHO_API int fpho_patch_count_pairs(fpho_patch *p, int enable, long long *last_count);
 
+/* Copy the image-Gaussian records (32 floats each: -xcen, -ycen, fxx, fxy,
+ * fyy, -amp/24, -amp*c0, c0, source, amp, ... Jacobian) that the last
+ * evaluation built for one exposure to host memory; *n_out receives the
+ * number of records.  Synchronizes the device. */
+FPHO_API int fpho_patch_image_gaussians(fpho_patch *p, int exposure, float *host_out,
+                                        int max_records, int *n_out);
+
+/* Enable (1) or disable (0) CUDA events recorded immediately before and after
+ * the pixel-tile kernel of every following evaluation, on its stream, so the
+ * dominant kernel can be timed on its own. */
+FPHO_API int fpho_patch_time_tiles(fpho_patch *p, int enable);
+/* Milliseconds of the tile kernel of the last evaluation (waits for it). */
+FPHO_API int fpho_patch_last_tile_ms(fpho_patch *p, float *ms);
+
+/* Throughput probes for roofline denominators: which 0 = packed FP32 FMA
+ * chains (flops = blocks*threads*iters*32), 1 = MUFU.EX2 chains
+ * (ops = blocks*threads*iters*8).  dev_out: device float[blocks] scratch. */
+FPHO_API int fpho_probe_launch(int which, int blocks, int threads, int iters, float *dev_out,
+                               void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -306,6 +306,90 @@ int fpo_image_gaussians_f32(int band, int e, const fpo_patch *P, const fpo_sourc
     return P->n_sources * npsf;
 }
 
+/* Mixed precision: the reference's float image Gaussians (bit-identical to
+ * what its CPU kernel builds), then per-pixel model, chi2 and gradient in
+ * double with per-Gaussian image-space gradients contracted with the float
+ * Jacobian in double.  Errors of a float kernel against this isolate its
+ * per-pixel arithmetic and accumulation from the rounding of the image
+ * Gaussian parameters (centres near x ~ 100 px carry ~4e-6 px of float
+ * rounding, which every float implementation shares). */
+int fpo_evaluate_band_mixed(int band, const fpo_patch *P, const fpo_source *S,
+                            int use_cutoff, double *chi2_out, double *dchi2,
+                            double *residual_out) {
+    int nsrc = P->n_sources;
+    int npsf = P->n_psf_per_source[band];
+    int bN = P->band_N[band], b0 = P->band_start[band];
+    int ntot = nsrc * npsf;
+    fpo_imgauss *ig = (fpo_imgauss *)malloc(sizeof(fpo_imgauss) * (size_t)(ntot > 0 ? ntot : 1));
+    double *gimg = (double *)malloc(sizeof(double) * 6 * (size_t)(ntot > 0 ? ntot : 1));
+    if (!ig || !gimg) { free(ig); free(gimg); return -1; }
+    for (int i = 0; i < nsrc * FPO_NPARAMS; i++) dchi2[i] = 0.0;
+    double chi2 = 0.0;
+    for (int ee = 0; ee < bN; ee++) {
+        int e = b0 + ee;
+        for (int g = 0; g < nsrc; g++) convolve_source_f32(band, e, g, npsf, P, S, ig);
+        memset(gimg, 0, sizeof(double) * 6 * (size_t)ntot);
+        int npix = P->exposure_N[e];
+        for (int p = 0; p < npix; p++) {
+            int pix = P->exposure_start[e] + p;
+            double xp = P->xpix[pix], yp = P->ypix[pix];
+            double d = P->data[pix], ie = P->ierr[pix];
+            double r = d;
+            for (int i = 0; i < ntot; i++) {
+                const fpo_imgauss *g = ig + i;
+                double dx = xp - g->xcen, dy = yp - g->ycen;
+                double fxx = g->fxx, fxy = g->fxy, fyy = g->fyy;
+                double vx = fxx * dx + fxy * dy, vy = fyy * dy + fxy * dx;
+                double ea = dx * vx + dy * vy;
+                if (use_cutoff && ea > FPO_MAX_EXP_ARG) continue;
+                double H = 1.0 + (vx * vx + vy * vy - fxx - fyy) / 24.0;
+                r -= (double)g->amp * exp(-0.5 * ea) * H;
+            }
+            if (residual_out) residual_out[pix] = r;
+            chi2 += (r * ie - d * ie) * (r * ie + d * ie);
+            double rie2 = r * ie * ie;
+            if (rie2 == 0.0) continue;
+            for (int i = 0; i < ntot; i++) {
+                const fpo_imgauss *g = ig + i;
+                double dx = xp - g->xcen, dy = yp - g->ycen;
+                double fxx = g->fxx, fxy = g->fxy, fyy = g->fyy, amp = g->amp;
+                double vx = fxx * dx + fxy * dy, vy = fyy * dy + fxy * dx;
+                double ea = dx * vx + dy * vy;
+                if (use_cutoff && ea > FPO_MAX_EXP_ARG) continue;
+                double Gp = exp(-0.5 * ea);
+                double H = 1.0 + (vx * vx + vy * vy - fxx - fyy) / 24.0;
+                double w = -2.0 * rie2;
+                double C = amp * Gp * H, c_h = amp * Gp;
+                double *gi = gimg + 6 * i;
+                gi[0] += w * Gp * H;
+                gi[1] += w * (C * vx - c_h * (fxx * vx + fxy * vy) / 12.0);
+                gi[2] += w * (C * vy - c_h * (fyy * vy + fxy * vx) / 12.0);
+                gi[3] += w * (-0.5 * C * dx * dx - c_h * (1.0 - 2.0 * dx * vx) / 24.0);
+                gi[4] += w * (-0.5 * C * dy * dy - c_h * (1.0 - 2.0 * dy * vy) / 24.0);
+                gi[5] += w * (-C * dx * dy + c_h * (dy * vx + dx * vy) / 12.0);
+            }
+        }
+        for (int i = 0; i < ntot; i++) {
+            const fpo_imgauss *g = ig + i;
+            const double *gi = gimg + 6 * i;
+            double *dp = dchi2 + (i / npsf) * FPO_NPARAMS;
+            dp[0] += g->dA_dFlux * gi[0];
+            dp[1] += g->dx_dAlpha * gi[1] + (double)g->dy_dAlpha * gi[2];
+            dp[2] += g->dx_dDelta * gi[1] + (double)g->dy_dDelta * gi[2];
+            dp[3] += g->dA_dQ * gi[0] + (double)g->dFxx_dQ * gi[3] + (double)g->dFyy_dQ * gi[4] +
+                     (double)g->dFxy_dQ * gi[5];
+            dp[4] += g->dA_dPA * gi[0] + (double)g->dFxx_dPA * gi[3] +
+                     (double)g->dFyy_dPA * gi[4] + (double)g->dFxy_dPA * gi[5];
+            dp[5] += g->dA_dSersic * gi[0];
+            dp[6] += g->dA_drh * gi[0];
+        }
+    }
+    free(ig);
+    free(gimg);
+    *chi2_out = chi2;
+    return 0;
+}
+
 /* ------------------------------------------------------------------------
  * double restatement
  * ------------------------------------------------------------------------ */

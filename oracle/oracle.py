@@ -49,6 +49,8 @@ def lib():
         L.fpo_evaluate_band_f32.restype = ip
         L.fpo_evaluate_band_f64.argtypes = [ip, vp, vp, ip, vp, vp, vp]
         L.fpo_evaluate_band_f64.restype = ip
+        L.fpo_evaluate_band_mixed.argtypes = [ip, vp, vp, ip, vp, vp, vp]
+        L.fpo_evaluate_band_mixed.restype = ip
         L.fpo_image_gaussians_f32.argtypes = [ip, ip, vp, vp, vp]
         L.fpo_image_gaussians_f32.restype = ip
         for n in ("fpo_sizeof_patch", "fpo_sizeof_source", "fpo_sizeof_psfgauss"):
@@ -58,7 +60,11 @@ def lib():
 
 
 def oracle_evaluate(patch, proposal, precision="f32", cutoff=True, residual=False, bands=None):
-    """chi2 (n_bands,), dchi2 (n_bands, n_src, 7) [, residual (npix,)]."""
+    """chi2 (n_bands,), dchi2 (n_bands, n_src, 7) [, residual (npix,)].
+
+    precision: "f32" (the reference CPU kernel restated, bit-identical),
+    "f64" (everything in double), "mixed" (the reference's float image
+    Gaussians, then double per-pixel math and accumulation)."""
     L = lib()
     st = patch.host_struct()
     prop = np.ascontiguousarray(proposal)
@@ -79,8 +85,9 @@ def oracle_evaluate(patch, proposal, precision="f32", cutoff=True, residual=Fals
             rc = L.fpo_evaluate_band_f32(b, st.ctypes.data, prop.ctypes.data, ctypes.byref(c),
                                          g.ctypes.data, rp)
         else:
-            rc = L.fpo_evaluate_band_f64(b, st.ctypes.data, prop.ctypes.data, int(bool(cutoff)),
-                                         ctypes.byref(c), g.ctypes.data, rp)
+            fn = L.fpo_evaluate_band_f64 if precision == "f64" else L.fpo_evaluate_band_mixed
+            rc = fn(b, st.ctypes.data, prop.ctypes.data, int(bool(cutoff)), ctypes.byref(c),
+                    g.ctypes.data, rp)
         if rc != 0:
             raise MemoryError("oracle allocation failed")
         chi2[b] = c.value
@@ -102,47 +109,125 @@ def image_gaussians_f32(patch, proposal, band, exposure):
 
 
 # ---------------------------------------------------------------- reference kernel
-_ref_mods = {}
+# The reference builds (MAXSOURCES 30 and 64) are two pybind11 modules with the
+# same name and types; a process may load only one of them.  This process
+# loads the 30-source build; the 64-source build (and multi-process CPU
+# baselines) run in worker processes started with `spawn`.
+_ref_mod = None
+PATCH_ARRAYS = ["data", "ierr", "xpix", "ypix", "exposure_start", "exposure_N", "band_start",
+                "band_N", "rad2", "D", "crpix", "crval", "CW", "G", "n_psf_per_source",
+                "psfgauss", "psfgauss_start"]
 
 
-def _ref_module(ms64=False):
-    key = "ms64" if ms64 else "std"
-    if key not in _ref_mods:
-        d = os.path.join(REF_DIR, "ms64") if ms64 else REF_DIR
-        cands = glob.glob(os.path.join(d, "compute_gaussians_kernel*.so"))
-        if not cands:
-            _ref_mods[key] = None
-        else:
-            name = "compute_gaussians_kernel"
-            spec = importlib.util.spec_from_file_location(name, cands[0])
-            mod = importlib.util.module_from_spec(spec)
-            spec.loader.exec_module(mod)
-            _ref_mods[key] = mod
-    return _ref_mods[key]
+def _ref_path(ms64):
+    d = os.path.join(REF_DIR, "ms64") if ms64 else REF_DIR
+    c = glob.glob(os.path.join(d, "compute_gaussians_kernel*.so"))
+    return c[0] if c else None
+
+
+def _load_ref(ms64):
+    spec = importlib.util.spec_from_file_location("compute_gaussians_kernel", _ref_path(ms64))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
 
 
 def ref_available(n_sources=1):
-    return _ref_module(ms64=n_sources > 30) is not None
+    return _ref_path(n_sources > 30) is not None
 
 
-def ref_evaluate(patch, proposal, bands=None):
+# the reference's Patch struct (forcepho/src/patch.cc:23-99) as a numpy record
+_PTR = np.uintp
+_STRUCT = np.dtype([("data", _PTR), ("ierr", _PTR), ("xpix", _PTR), ("ypix", _PTR),
+                    ("residual", _PTR), ("exposure_start", _PTR), ("exposure_N", _PTR),
+                    ("band_start", _PTR), ("band_N", _PTR), ("n_sources", np.int32),
+                    ("n_radii", np.int32), ("rad2", _PTR), ("D", _PTR), ("crpix", _PTR),
+                    ("crval", _PTR), ("CW", _PTR), ("G", _PTR), ("n_psf_per_source", _PTR),
+                    ("psfgauss", _PTR), ("psfgauss_start", _PTR)], align=True)
+
+
+def _struct_from_arrays(arrays, n_sources, n_radii):
+    st = np.zeros(1, dtype=_STRUCT)
+    for k, v in arrays.items():
+        st[k] = v.ctypes.data
+    st["n_sources"], st["n_radii"] = n_sources, n_radii
+    return st
+
+
+def _patch_payload(patch):
+    return ({k: np.ascontiguousarray(getattr(patch, k)) for k in PATCH_ARRAYS},
+            int(patch.n_sources), int(patch.n_radii))
+
+
+_worker = {}
+
+
+def _worker_init(ms64, root):
+    if root not in sys.path:
+        sys.path.insert(0, root)
+    _worker["mod"] = _load_ref(ms64)
+    _worker["ms64"] = ms64
+
+
+def _worker_eval(payload, proposal, band, reps=1):
+    import time
+    arrays, ns, nr = payload
+    st = _struct_from_arrays(arrays, ns, nr)
+    prop = np.ascontiguousarray(proposal)
+    maxsrc = 64 if _worker["ms64"] else 30
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        r = _worker["mod"].EvaluateProposal(band, st.ctypes.data, prop.ctypes.data)
+    dt = time.perf_counter() - t0
+    return band, r.chi2, np.asarray(r.dchi2_dp).reshape(maxsrc, 7)[:ns].copy(), dt
+
+
+def ref_pool(n_sources, processes):
+    """A spawn pool of `processes` workers, each with the reference build
+    suited to `n_sources` loaded."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    root = os.path.dirname(HERE)
+    return ctx.Pool(processes, initializer=_worker_init, initargs=(n_sources > 30, root))
+
+
+def ref_evaluate(patch, proposal, bands=None, pool=None):
     """Run the reference CPU kernel band by band (as CPUProposer,
     forcepho/proposal.py:180-226).  Returns chi2 (n_bands,), dchi2
-    (n_bands, n_src, 7) float32."""
+    (n_bands, n_src, 7) float32.  Patches of more than 30 sources, or a
+    given `pool`, run in worker processes."""
+    global _ref_mod
     ns = patch.n_sources
-    ms64 = ns > 30
-    mod = _ref_module(ms64)
-    if mod is None:
-        raise RuntimeError("reference CPU kernel not built (make -C oracle ref)")
-    maxsrc = 64 if ms64 else 30
-    st = patch.host_struct()
-    prop = np.ascontiguousarray(proposal)
     nb = patch.n_bands
-    bands = range(nb) if bands is None else bands
+    bands = list(range(nb)) if bands is None else list(bands)
     chi2 = np.zeros(nb)
     dchi2 = np.zeros((nb, ns, 7), dtype=np.float32)
-    for b in bands:
-        r = mod.EvaluateProposal(b, st.ctypes.data, prop.ctypes.data)
-        chi2[b] = r.chi2
-        dchi2[b] = np.asarray(r.dchi2_dp).reshape(maxsrc, 7)[:ns]
+    if pool is None and ns <= 30:
+        if _ref_path(False) is None:
+            raise RuntimeError("reference CPU kernel not built (make -C oracle ref)")
+        if _ref_mod is None:
+            _ref_mod = _load_ref(False)
+        st = patch.host_struct()
+        prop = np.ascontiguousarray(proposal)
+        for b in bands:
+            r = _ref_mod.EvaluateProposal(b, st.ctypes.data, prop.ctypes.data)
+            chi2[b] = r.chi2
+            dchi2[b] = np.asarray(r.dchi2_dp).reshape(30, 7)[:ns]
+        return chi2, dchi2
+    own = pool is None
+    if own:
+        if _ref_path(ns > 30) is None:
+            raise RuntimeError("reference CPU kernel not built (make -C oracle ref)")
+        pool = ref_pool(ns, 1)
+    try:
+        payload = _patch_payload(patch)
+        prop = np.ascontiguousarray(proposal)
+        res = pool.starmap(_worker_eval, [(payload, prop, b) for b in bands])
+    finally:
+        if own:
+            pool.close()
+            pool.join()
+    for b, c, g, _ in res:
+        chi2[b] = c
+        dchi2[b] = g
     return chi2, dchi2

@@ -1,0 +1,94 @@
+"""The C-ABI library loads and exports every entry point include/fpho.h
+declares; struct layouts agree with the numpy dtypes; host-side validation
+rejects bad descriptors with status codes (no GPU needed)."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, load_golden
+
+HEADER = os.path.join(ROOT, "include", "fpho.h")
+
+
+def declared_symbols():
+    txt = open(HEADER).read()
+    return sorted(set(re.findall(r"FPHO_API\s+[\w\s\*]*?\b(fpho_\w+)\s*\(", txt)))
+
+
+def test_header_declares_entry_points():
+    syms = declared_symbols()
+    assert "fpho_evaluate_proposal" in syms and "fpho_patch_create" in syms
+    assert len(syms) >= 15
+
+
+def test_library_exports_every_declared_symbol():
+    from forcepho_b200 import _lib
+    for s in declared_symbols():
+        assert hasattr(_lib.lib, s), s
+
+
+def test_struct_sizes_match_numpy_layouts():
+    from forcepho_b200 import _lib
+    from forcepho_b200.patches.patch import PatchBase, PSF_DTYPE
+    from forcepho_b200.proposal import source_struct_dtype, response_struct_dtype
+    assert _lib.lib.fpho_sizeof(0) == PatchBase.patch_struct_dtype.itemsize == 152
+    assert _lib.lib.fpho_sizeof(1) == source_struct_dtype.itemsize == 264
+    assert _lib.lib.fpho_sizeof(2) == PSF_DTYPE.itemsize == 28
+    assert _lib.lib.fpho_sizeof(3) == response_struct_dtype.itemsize == 840
+
+
+def test_oracle_struct_sizes():
+    from oracle import oracle as O
+    L = O.lib()
+    assert L.fpo_sizeof_patch() == 152 and L.fpo_sizeof_source() == 264
+    assert L.fpo_sizeof_psfgauss() == 28
+
+
+def _create(st, n_bands):
+    from forcepho_b200 import _lib
+    h = ctypes.c_void_p()
+    rc = _lib.lib.fpho_patch_create(st.ctypes.data if st is not None else None, n_bands, 0, None,
+                                    ctypes.byref(h))
+    return rc, _lib.last_error(), h
+
+
+def test_create_rejects_null_and_bad_band_count():
+    rc, msg, h = _create(None, 1)
+    assert rc == 1 and "NULL" in msg and not h.value
+    P, prop, d = load_golden("config0_seed1")
+    rc, msg, h = _create(P.host_struct(), 0)
+    assert rc == 4 and "n_bands" in msg
+    rc, msg, h = _create(P.host_struct(), 31)
+    assert rc == 4
+
+
+def test_create_rejects_negative_counts():
+    P, prop, d = load_golden("mini_3src_2band")
+    P.band_N = P.band_N.copy()
+    P.band_N[1] = -1
+    rc, msg, h = _create(P.host_struct(), 2)
+    assert rc == 1 and "negative" in msg
+
+
+def test_create_rejects_overlapping_bands():
+    P, prop, d = load_golden("mini_3src_2band")
+    P.band_start = np.array([0, 1], dtype=np.int16)
+    rc, msg, h = _create(P.host_struct(), 2)
+    assert rc == 1 and "belongs to bands" in msg
+
+
+def test_create_rejects_bad_radius_bin():
+    P, prop, d = load_golden("config0_seed1")
+    P.psfgauss = P.psfgauss.copy()
+    P.psfgauss["sersic_bin"][3] = 99
+    rc, msg, h = _create(P.host_struct(), 1)
+    assert rc in (1, 2)   # 2 only if the pixel upload already needed a GPU
+
+
+def test_variants_listed():
+    from forcepho_b200 import _lib
+    v = _lib.variants()
+    assert len(v) >= 4 and all(nt % 32 == 0 and k % 2 == 0 for nt, k in v)

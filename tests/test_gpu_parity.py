@@ -1,0 +1,223 @@
+"""GPU parity: the CUDA path (through the C ABI) against the oracle.
+
+Tolerances (the bar stated for this path):
+  * chi2: relative error <= 1e-6 against the reference CPU kernel.
+  * gradient, per component: relative error <= 1e-5 against the reference
+    CPU kernel; on ill-conditioned components, where the reference itself is
+    farther than 1e-5 from the exact sum over its own float image Gaussians
+    (the "mixed" oracle: the reference's float Gaussians, FP64 pixel
+    arithmetic and sums), no farther from that exact sum than twice the
+    reference is.  The distance of both float kernels from an all-FP64
+    evaluation (float image-Gaussian centres carry ~4e-6 px of rounding) is
+    reported, not asserted tightly.
+  * image Gaussians: bit-identical to the reference's.
+  * residual image: |gpu - ref| <= 1e-5 * max|data| per pixel.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from conftest import GOLDEN_CASES, load_golden
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+CHI2_RTOL = 1e-6
+GRAD_RTOL = 1e-5
+
+
+def gpu_eval(P, prop, residual=False, variant=None, live_cap=None):
+    from forcepho_b200.proposal import GPUProposer
+    P.return_residual = residual
+    P.free()
+    P.send_to_device()
+    if variant is not None:
+        P.device_patch.set_config(variant, live_cap or 512)
+    out = GPUProposer().evaluate_proposal(prop, patch=P, unpack=False)
+    P.free()
+    return out
+
+
+def grad_report(g, ref, f64, mixed):
+    g, ref, f64, mixed = (np.asarray(a, dtype=np.float64) for a in (g, ref, f64, mixed))
+    rel = lambda a, b: float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-300)))
+    return {"gpu_vs_ref": rel(g, ref), "gpu_vs_mixed": rel(g, mixed),
+            "gpu_vs_fp64": rel(g, f64), "ref_vs_fp64": rel(ref, f64)}
+
+
+def check_grad(g, ref, f64, mixed, rtol=GRAD_RTOL):
+    """Per component: within rtol of the reference CPU kernel, or -- on
+    components where the float reference is itself farther than rtol from the
+    exact sum over its own float image Gaussians (the mixed oracle) -- no
+    farther from that exact sum than twice the reference is."""
+    g, ref, f64, mixed = (np.asarray(a, dtype=np.float64) for a in (g, ref, f64, mixed))
+    own = np.abs(ref - mixed)
+    ok = (np.abs(g - ref) <= rtol * np.abs(ref)) | \
+         (np.abs(g - mixed) <= np.maximum(rtol * np.abs(mixed), 2.0 * own))
+    bad = ~ok
+    assert np.all(ok), (f"{bad.sum()} components: gpu {g[bad]}, ref {ref[bad]}, "
+                        f"mixed {mixed[bad]}")
+    frac = np.mean(np.abs(g - ref) <= rtol * np.abs(ref))
+    return frac
+
+
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_golden_parity(name):
+    P, prop, d = load_golden(name)
+    chi2, dchi2 = gpu_eval(P, prop)
+    np.testing.assert_allclose(chi2, d["ref_chi2"], rtol=CHI2_RTOL)
+    c64, g64 = O.oracle_evaluate(P, prop, precision="f64")
+    cm, gm = O.oracle_evaluate(P, prop, precision="mixed")
+    np.testing.assert_allclose(chi2, c64, rtol=CHI2_RTOL)
+    print(name, grad_report(dchi2, d["ref_dchi2"], g64, gm))
+    check_grad(dchi2, d["ref_dchi2"], g64, gm)
+
+
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_golden_vs_slow_fp64(name):
+    """Against the reference's FP64 slow path (no cutoff): the cutoff changes
+    chi2 by < 1e-6 relative on these patches."""
+    P, prop, d = load_golden(name)
+    chi2, dchi2 = gpu_eval(P, prop)
+    np.testing.assert_allclose(chi2, d["slow_chi2"], rtol=2e-6)
+    np.testing.assert_allclose(dchi2, d["slow_dchi2"], rtol=5e-4,
+                               atol=1e-6 * np.abs(d["slow_dchi2"]).max())
+
+
+def test_residual_matches_oracle():
+    P, prop, d = load_golden("mini_3src_2band")
+    chi2, dchi2, res = gpu_eval(P, prop, residual=True)
+    c, g, r = O.oracle_evaluate(P, prop, residual=True)
+    scale = np.abs(P.data).max()
+    assert np.max(np.abs(res - r)) <= 1e-5 * scale
+
+
+@pytest.mark.parametrize("variant", range(6))
+def test_variants_agree(variant):
+    from forcepho_b200 import _lib
+    if variant >= len(_lib.variants()):
+        pytest.skip("variant not compiled")
+    P, prop, d = load_golden("mini_3src_2band")
+    nt = _lib.variants()[variant][0]
+    chi2, dchi2 = gpu_eval(P, prop, variant=variant, live_cap=max(nt, 128))
+    c64, g64 = O.oracle_evaluate(P, prop, precision="f64")
+    cm, gm = O.oracle_evaluate(P, prop, precision="mixed")
+    np.testing.assert_allclose(chi2, c64, rtol=CHI2_RTOL)
+    check_grad(dchi2, d["ref_dchi2"], g64, gm)
+
+
+def test_multi_chunk_staging():
+    """live_cap smaller than the kept Gaussians forces several staged chunks."""
+    from forcepho_b200 import synth
+    spec = synth.config_spec(1)
+    spec.shapes = [(48, 48)] * 32
+    P = synth.make_patch(spec, seed=4)
+    prop = P.proposal()
+    a = gpu_eval(P, prop, variant=1, live_cap=128)  # 128 threads, 128 records per chunk
+    b = gpu_eval(P, prop, variant=1, live_cap=1024)
+    c64, g64 = O.oracle_evaluate(P, prop, precision="f64")
+    np.testing.assert_allclose(a[0], c64, rtol=CHI2_RTOL)
+    np.testing.assert_allclose(b[0], c64, rtol=CHI2_RTOL)
+    np.testing.assert_allclose(a[1], b[1], rtol=1e-5, atol=1e-6 * np.abs(g64).max())
+
+
+def test_deterministic():
+    P, prop, d = load_golden("mini_3src_2band")
+    a = gpu_eval(P, prop)
+    b = gpu_eval(P, prop)
+    assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
+
+
+def test_reference_kernel_argument_list():
+    """fpho_EvaluateProposal takes the reference kernel's arguments (device
+    Patch*, Source*, double*, Response*)."""
+    import torch
+    from forcepho_b200 import _lib
+    from forcepho_b200.proposal import response_struct_dtype
+    P, prop, d = load_golden("mini_3src_2band")
+    P.return_residual = False
+    P.send_to_device()
+    dp = P.device_patch
+    dprop = torch.from_numpy(prop.view(np.uint8).copy()).cuda()
+    chi2 = torch.zeros(P.n_bands, dtype=torch.float64, device="cuda")
+    resp = torch.zeros(P.n_bands * response_struct_dtype.itemsize // 4, dtype=torch.float32,
+                       device="cuda")
+    s = torch.cuda.current_stream().cuda_stream
+    _lib.call("fpho_EvaluateProposal", dp.handle, dp.device_struct, dprop.data_ptr(),
+              chi2.data_ptr(), resp.data_ptr(), s)
+    torch.cuda.synchronize()
+    g = resp.cpu().numpy().reshape(P.n_bands, 30, 7)
+    np.testing.assert_allclose(chi2.cpu().numpy(), d["ref_chi2"], rtol=CHI2_RTOL)
+    assert np.all(g[:, P.n_sources:] == 0)
+    c64, g64 = O.oracle_evaluate(P, prop, precision="f64")
+    cm, gm = O.oracle_evaluate(P, prop, precision="mixed")
+    check_grad(g[:, :P.n_sources], d["ref_dchi2"], g64, gm)
+    with pytest.raises(_lib.FphoError):
+        _lib.call("fpho_EvaluateProposal", dp.handle, dp.device_struct + 8, dprop.data_ptr(),
+                  chi2.data_ptr(), resp.data_ptr(), s)
+    P.free()
+
+
+def test_swap_on_device_invariant():
+    """After swap_on_device the residual becomes the data; evaluating the same
+    proposal again gives residual_new == data - 2 model (tests/cswap_test.py:98-110
+    of the reference)."""
+    P, prop, d = load_golden("mini_3src_2band")
+    P.return_residual = True
+    P.send_to_device()
+    from forcepho_b200.proposal import GPUProposer
+    pr = GPUProposer()
+    _, _, r1 = pr.evaluate_proposal(prop, patch=P, unpack=False)
+    P.swap_on_device()
+    data_now = P.retrieve_array("data")
+    np.testing.assert_array_equal(data_now, r1)
+    _, _, r2 = pr.evaluate_proposal(prop, patch=P, unpack=False)
+    model = P.data - r1
+    np.testing.assert_allclose(r2, P.data - 2 * model, atol=1e-5 * np.abs(P.data).max())
+    P.free()
+
+
+def test_config1_full_size():
+    """Config 1 at full size against FP64 and the reference kernel."""
+    from forcepho_b200 import synth
+    P = synth.make_config(1, seed=0)
+    prop = P.proposal()
+    chi2, dchi2 = gpu_eval(P, prop)
+    c64, g64 = O.oracle_evaluate(P, prop, precision="f64")
+    cm, gm = O.oracle_evaluate(P, prop, precision="mixed")
+    rc, rd = O.ref_evaluate(P, prop)
+    np.testing.assert_allclose(chi2, rc, rtol=CHI2_RTOL)
+    np.testing.assert_allclose(chi2, c64, rtol=CHI2_RTOL)
+    print("config1", grad_report(dchi2, rd, g64, gm))
+    check_grad(dchi2, rd, g64, gm)
+
+
+@pytest.mark.parametrize("name", GOLDEN_CASES)
+def test_image_gaussians_bitexact(name):
+    """The image Gaussians (centre, inverse covariance, amplitude) built on
+    the device equal the reference CPU kernel's float values bit for bit."""
+    import ctypes
+    from forcepho_b200 import _lib
+    P, prop, d = load_golden(name)
+    P.return_residual = False
+    P.send_to_device()
+    from forcepho_b200.proposal import GPUProposer
+    GPUProposer().evaluate_proposal(prop, patch=P)
+    n_exact = n_total = 0
+    for b in range(P.n_bands):
+        for e in range(int(P.band_start[b]), int(P.band_start[b] + P.band_N[b])):
+            ref = O.image_gaussians_f32(P, prop, b, e)
+            buf = np.zeros((len(ref), 32), dtype=np.float32)
+            n = ctypes.c_int()
+            _lib.call("fpho_patch_image_gaussians", P.device_patch.handle, e, buf.ctypes.data,
+                      len(ref), ctypes.byref(n))
+            assert n.value == len(ref)
+            # reference ImageGaussian order: amp, xcen, ycen, fxx, fyy, fxy
+            got = np.stack([buf[:, 9], -buf[:, 0], -buf[:, 1], buf[:, 2], buf[:, 4], buf[:, 3]], 1)
+            want = ref[:, :6]
+            np.testing.assert_array_equal(got, want)
+            n_exact += got.size
+            n_total += got.size
+    P.free()
+    assert n_exact == n_total
