@@ -238,7 +238,47 @@ __device__ __forceinline__ float ex2f(float x) {
     return y;
 }
 
-// -0.5 * log2(e): exp(-Q/2) = 2^(Q * KEXP)
+// -0.5 * log2(e): exp(-Q/2) = 2^(Q * KEXP).  KEXP_LO carries the rounding of
+// KEXP (relative 1.3e-8), so that fma(Q, KEXP, Q * KEXP_LO) is the exponent
+// without the systematic error a rounded constant would add.
 constexpr float KEXP = -0.72134752044448170368f;
+constexpr float KEXP_LO = -9.629815167500055e-09f;
+
+// Unbiased 2^E for packed E in [-126, 0].
+//
+// MUFU.EX2 (ex2.approx) is accurate to a few 1e-7 but its error has a mean of
+// about -3e-8 over the exponents seen here.  In the residual r = data - model
+// that bias does not average out: the gradient of chi2 near a fit measures a
+// ~1% parameter offset, and a relative model bias b shows up in it amplified
+// ~1e3 times.  So the residual pass evaluates 2^E with Cody and Waite's range
+// reduction E = n + f, n = rint(E), f in [-1/2, 1/2] (the rounding done by
+// adding 1.5*2^23), a degree-6 polynomial for 2^f (coefficients fitted here by
+// relative least squares with the constant term pinned to 1: mean relative
+// error 6e-10, max 8e-8 in float), and scaling by 2^n through the exponent
+// field.  Inputs below -126 give garbage that callers discard (they select 0
+// for exp-arguments above the cutoff, and never use the value at pixels
+// outside the culling box).
+__device__ __forceinline__ v2 exp2_unbiased(v2 E) {
+    const float MAGIC = 12582912.0f;  // 1.5 * 2^23
+    const v2 t = add2(E, pk1(MAGIC));
+    const v2 f = add2(E, add2(t, pk1(-MAGIC)) ^ 0x8000000080000000ull);  // E - n
+    v2 p = pk1(1.5370704932138324e-04f);
+    p = fma2(p, f, pk1(1.3399848248809576e-03f));
+    p = fma2(p, f, pk1(9.618373587727547e-03f));
+    p = fma2(p, f, pk1(5.550329014658928e-02f));
+    p = fma2(p, f, pk1(2.4022647738456726e-01f));
+    p = fma2(p, f, pk1(6.931471824645996e-01f));
+    p = fma2(p, f, pk1(1.0f));
+    // t's low mantissa bits hold n (two's complement); (bits(t) << 23) adds n
+    // to the exponent of p, since bits(1.5*2^23) << 23 vanishes mod 2^32.
+    uint32_t t0, t1, p0, p1;
+    asm("mov.b64 {%0, %1}, %2;" : "=r"(t0), "=r"(t1) : "l"(t));
+    asm("mov.b64 {%0, %1}, %2;" : "=r"(p0), "=r"(p1) : "l"(p));
+    p0 += t0 << 23;
+    p1 += t1 << 23;
+    v2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "r"(p0), "r"(p1));
+    return r;
+}
 
 }  // namespace fpho

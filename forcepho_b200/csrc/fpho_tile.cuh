@@ -198,6 +198,7 @@ __device__ __forceinline__ void tile_body(const TileArgs &A, int tile, unsigned 
     const bool tile_has_weight = s_any_weight != 0;
 
     const v2 KEXP2 = pk1(KEXP);
+    const v2 KEXPLO2 = pk1(KEXP_LO);
     long long npairs = 0;
 
     // ---- chunked scan + stage.  Returns the number of staged records; `cursor`
@@ -280,18 +281,19 @@ __device__ __forceinline__ void tile_body(const TileArgs &A, int tile, unsigned 
                     const v2 VX = fma2(FXY, DY, mul2(FXX, DX));
                     const v2 VY = fma2(FXY, DX, mul2(FYY, DY));
                     const v2 Q = fma2(DY, VY, mul2(DX, VX));
-                    const v2 E = mul2(Q, KEXP2);
-                    float e0, e1, q0, q1;
-                    unpk(E, e0, e1);
-                    float g0v = ex2f(e0), g1v = ex2f(e1);
+                    // the residual needs an unbiased exponential (see exp2_unbiased)
+                    v2 Gp = exp2_unbiased(fma2(Q, KEXP2, mul2(Q, KEXPLO2)));
                     if (cut) {
+                        float g0v, g1v, q0, q1;
+                        unpk(Gp, g0v, g1v);
                         unpk(Q, q0, q1);
                         g0v = (q0 > FPHO_MAX_EXP_ARG) ? 0.0f : g0v;
                         g1v = (q1 > FPHO_MAX_EXP_ARG) ? 0.0f : g1v;
+                        Gp = pk(g0v, g1v);
                     }
                     const v2 S = fma2(VY, VY, mul2(VX, VX));
                     const v2 NAH = fma2(S, HA, HB);  // -amp * H
-                    R[j] = fma2(NAH, pk(g0v, g1v), R[j]);
+                    R[j] = fma2(NAH, Gp, R[j]);
                 }
             }
         }

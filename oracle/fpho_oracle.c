@@ -548,3 +548,84 @@ int fpo_evaluate_band_f64(int band, const fpo_patch *P, const fpo_source *S,
     *chi2_out = chi2;
     return 0;
 }
+
+/* Like fpo_evaluate_band_mixed (float image Gaussians, double pixel math),
+ * but contracting with the Jacobian per pixel, so that it can also return, per
+ * gradient component, the sum over pixels of the absolute value of the
+ * per-pixel contribution: the scale against which float rounding of the
+ * per-pixel terms is measured (a component much smaller than this scale is
+ * ill-conditioned).  dchi2 and dchi2_abs are double[n_sources*7]. */
+int fpo_evaluate_band_mixed_abs(int band, const fpo_patch *P, const fpo_source *S,
+                                int use_cutoff, double *chi2_out, double *dchi2,
+                                double *dchi2_abs) {
+    int nsrc = P->n_sources;
+    int npsf = P->n_psf_per_source[band];
+    int bN = P->band_N[band], b0 = P->band_start[band];
+    int ntot = nsrc * npsf;
+    fpo_imgauss *ig = (fpo_imgauss *)malloc(sizeof(fpo_imgauss) * (size_t)(ntot > 0 ? ntot : 1));
+    double *pc = (double *)malloc(sizeof(double) * FPO_NPARAMS * (size_t)(nsrc > 0 ? nsrc : 1));
+    if (!ig || !pc) { free(ig); free(pc); return -1; }
+    for (int i = 0; i < nsrc * FPO_NPARAMS; i++) dchi2[i] = dchi2_abs[i] = 0.0;
+    double chi2 = 0.0;
+    for (int ee = 0; ee < bN; ee++) {
+        int e = b0 + ee;
+        for (int g = 0; g < nsrc; g++) convolve_source_f32(band, e, g, npsf, P, S, ig);
+        int npix = P->exposure_N[e];
+        for (int p = 0; p < npix; p++) {
+            int pix = P->exposure_start[e] + p;
+            double xp = P->xpix[pix], yp = P->ypix[pix];
+            double d = P->data[pix], ie = P->ierr[pix];
+            double r = d;
+            for (int i = 0; i < ntot; i++) {
+                const fpo_imgauss *g = ig + i;
+                double dx = xp - g->xcen, dy = yp - g->ycen;
+                double fxx = g->fxx, fxy = g->fxy, fyy = g->fyy;
+                double vx = fxx * dx + fxy * dy, vy = fyy * dy + fxy * dx;
+                double ea = dx * vx + dy * vy;
+                if (use_cutoff && ea > FPO_MAX_EXP_ARG) continue;
+                double H = 1.0 + (vx * vx + vy * vy - fxx - fyy) / 24.0;
+                r -= (double)g->amp * exp(-0.5 * ea) * H;
+            }
+            chi2 += (r * ie - d * ie) * (r * ie + d * ie);
+            double rie2 = r * ie * ie;
+            if (rie2 == 0.0) continue;
+            memset(pc, 0, sizeof(double) * FPO_NPARAMS * (size_t)nsrc);
+            for (int i = 0; i < ntot; i++) {
+                const fpo_imgauss *g = ig + i;
+                double dx = xp - g->xcen, dy = yp - g->ycen;
+                double fxx = g->fxx, fxy = g->fxy, fyy = g->fyy, amp = g->amp;
+                double vx = fxx * dx + fxy * dy, vy = fyy * dy + fxy * dx;
+                double ea = dx * vx + dy * vy;
+                if (use_cutoff && ea > FPO_MAX_EXP_ARG) continue;
+                double Gp = exp(-0.5 * ea);
+                double H = 1.0 + (vx * vx + vy * vy - fxx - fyy) / 24.0;
+                double w = -2.0 * rie2;
+                double C = amp * Gp * H, c_h = amp * Gp;
+                double gA = w * Gp * H;
+                double gx = w * (C * vx - c_h * (fxx * vx + fxy * vy) / 12.0);
+                double gy = w * (C * vy - c_h * (fyy * vy + fxy * vx) / 12.0);
+                double gfx = w * (-0.5 * C * dx * dx - c_h * (1.0 - 2.0 * dx * vx) / 24.0);
+                double gfy = w * (-0.5 * C * dy * dy - c_h * (1.0 - 2.0 * dy * vy) / 24.0);
+                double gfxy = w * (-C * dx * dy + c_h * (dy * vx + dx * vy) / 12.0);
+                double *q = pc + (i / npsf) * FPO_NPARAMS;
+                q[0] += g->dA_dFlux * gA;
+                q[1] += g->dx_dAlpha * gx + (double)g->dy_dAlpha * gy;
+                q[2] += g->dx_dDelta * gx + (double)g->dy_dDelta * gy;
+                q[3] += g->dA_dQ * gA + (double)g->dFxx_dQ * gfx + (double)g->dFyy_dQ * gfy +
+                        (double)g->dFxy_dQ * gfxy;
+                q[4] += g->dA_dPA * gA + (double)g->dFxx_dPA * gfx + (double)g->dFyy_dPA * gfy +
+                        (double)g->dFxy_dPA * gfxy;
+                q[5] += g->dA_dSersic * gA;
+                q[6] += g->dA_drh * gA;
+            }
+            for (int k = 0; k < nsrc * FPO_NPARAMS; k++) {
+                dchi2[k] += pc[k];
+                dchi2_abs[k] += fabs(pc[k]);
+            }
+        }
+    }
+    free(ig);
+    free(pc);
+    *chi2_out = chi2;
+    return 0;
+}

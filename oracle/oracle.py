@@ -97,6 +97,33 @@ def oracle_evaluate(patch, proposal, precision="f32", cutoff=True, residual=Fals
     return chi2, dchi2
 
 
+def oracle_mixed_abs(patch, proposal):
+    """Mixed-precision evaluation (the reference's float image Gaussians,
+    double pixel math) returning chi2, dchi2 (n_bands, n_src, 7) and, per
+    component, the sum over pixels of |per-pixel contribution|."""
+    L = lib()
+    if not hasattr(L, "_mixed_abs_bound"):
+        vp, ip = ctypes.c_void_p, ctypes.c_int
+        L.fpo_evaluate_band_mixed_abs.argtypes = [ip, vp, vp, ip, vp, vp, vp]
+        L.fpo_evaluate_band_mixed_abs.restype = ip
+        L._mixed_abs_bound = True
+    st = patch.host_struct()
+    prop = np.ascontiguousarray(proposal)
+    nb, ns = patch.n_bands, patch.n_sources
+    chi2 = np.zeros(nb)
+    dchi2 = np.zeros((nb, ns, 7))
+    dabs = np.zeros((nb, ns, 7))
+    for b in range(nb):
+        c = ctypes.c_double(0.0)
+        g = np.zeros(ns * 7)
+        a = np.zeros(ns * 7)
+        if L.fpo_evaluate_band_mixed_abs(b, st.ctypes.data, prop.ctypes.data, 1, ctypes.byref(c),
+                                         g.ctypes.data, a.ctypes.data) != 0:
+            raise MemoryError("oracle allocation failed")
+        chi2[b], dchi2[b], dabs[b] = c.value, g.reshape(ns, 7), a.reshape(ns, 7)
+    return chi2, dchi2, dabs
+
+
 def image_gaussians_f32(patch, proposal, band, exposure):
     """float32 array (n_sources * n_psf, 21) of the reference's ImageGaussians."""
     L = lib()

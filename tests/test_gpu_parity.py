@@ -46,20 +46,26 @@ def grad_report(g, ref, f64, mixed):
             "gpu_vs_fp64": rel(g, f64), "ref_vs_fp64": rel(ref, f64)}
 
 
-def check_grad(g, ref, f64, mixed, rtol=GRAD_RTOL):
-    """Per component: within rtol of the reference CPU kernel, or -- on
-    components where the float reference is itself farther than rtol from the
-    exact sum over its own float image Gaussians (the mixed oracle) -- no
-    farther from that exact sum than twice the reference is."""
-    g, ref, f64, mixed = (np.asarray(a, dtype=np.float64) for a in (g, ref, f64, mixed))
+ABS_RTOL = 1e-6
+
+
+def check_grad(g, ref, P, prop, rtol=GRAD_RTOL):
+    """Per component: within rtol of the reference CPU kernel; or, on an
+    ill-conditioned component (one much smaller than the sum of the absolute
+    values of its per-pixel contributions, where the float reference is itself
+    off the exact value by more than rtol), within ABS_RTOL of that sum -- or
+    twice the reference's own error -- of the exact sum over the reference's
+    float image Gaussians.  Returns the fraction meeting the plain bar."""
+    _, mixed, scale = O.oracle_mixed_abs(P, prop)
+    g, ref = (np.asarray(a, dtype=np.float64) for a in (g, ref))
     own = np.abs(ref - mixed)
     ok = (np.abs(g - ref) <= rtol * np.abs(ref)) | \
-         (np.abs(g - mixed) <= np.maximum(rtol * np.abs(mixed), 2.0 * own))
+         (np.abs(g - mixed) <= np.maximum.reduce([rtol * np.abs(mixed), 2.0 * own,
+                                                  ABS_RTOL * scale]))
     bad = ~ok
     assert np.all(ok), (f"{bad.sum()} components: gpu {g[bad]}, ref {ref[bad]}, "
-                        f"mixed {mixed[bad]}")
-    frac = np.mean(np.abs(g - ref) <= rtol * np.abs(ref))
-    return frac
+                        f"mixed {mixed[bad]}, scale {scale[bad]}")
+    return float(np.mean(np.abs(g - ref) <= rtol * np.abs(ref)))
 
 
 @pytest.mark.parametrize("name", GOLDEN_CASES)
@@ -71,7 +77,8 @@ def test_golden_parity(name):
     cm, gm = O.oracle_evaluate(P, prop, precision="mixed")
     np.testing.assert_allclose(chi2, c64, rtol=CHI2_RTOL)
     print(name, grad_report(dchi2, d["ref_dchi2"], g64, gm))
-    check_grad(dchi2, d["ref_dchi2"], g64, gm)
+    frac = check_grad(dchi2, d["ref_dchi2"], P, prop)
+    print(name, "fraction within 1e-5 of the reference:", frac)
 
 
 @pytest.mark.parametrize("name", GOLDEN_CASES)
@@ -104,7 +111,7 @@ def test_variants_agree(variant):
     c64, g64 = O.oracle_evaluate(P, prop, precision="f64")
     cm, gm = O.oracle_evaluate(P, prop, precision="mixed")
     np.testing.assert_allclose(chi2, c64, rtol=CHI2_RTOL)
-    check_grad(dchi2, d["ref_dchi2"], g64, gm)
+    check_grad(dchi2, d["ref_dchi2"], P, prop)
 
 
 def test_multi_chunk_staging():
@@ -152,7 +159,7 @@ def test_reference_kernel_argument_list():
     assert np.all(g[:, P.n_sources:] == 0)
     c64, g64 = O.oracle_evaluate(P, prop, precision="f64")
     cm, gm = O.oracle_evaluate(P, prop, precision="mixed")
-    check_grad(g[:, :P.n_sources], d["ref_dchi2"], g64, gm)
+    check_grad(g[:, :P.n_sources], d["ref_dchi2"], P, prop)
     with pytest.raises(_lib.FphoError):
         _lib.call("fpho_EvaluateProposal", dp.handle, dp.device_struct + 8, dprop.data_ptr(),
                   chi2.data_ptr(), resp.data_ptr(), s)
@@ -190,7 +197,8 @@ def test_config1_full_size():
     np.testing.assert_allclose(chi2, rc, rtol=CHI2_RTOL)
     np.testing.assert_allclose(chi2, c64, rtol=CHI2_RTOL)
     print("config1", grad_report(dchi2, rd, g64, gm))
-    check_grad(dchi2, rd, g64, gm)
+    frac = check_grad(dchi2, rd, P, prop)
+    print("config1 fraction within 1e-5 of the reference:", frac)
 
 
 @pytest.mark.parametrize("name", GOLDEN_CASES)
