@@ -19,17 +19,25 @@ namespace fpho {
 
 // ---------------------------------------------------------------- records
 constexpr int GREC = 32;  // floats per image-Gaussian record
+// Floats 0..15 hold the eight per-pixel-loop parameters, each stored twice so
+// that one 16-byte shared-memory load yields two packed f32x2 operands (both
+// lanes of a pair of pixels use the same Gaussian).  Floats 16..30 hold the
+// Jacobian of (A, x, y, fxx, fyy, fxy) w.r.t. (flux, ra, dec, q, pa, n, rh) as
+// scalars; the rows acting on x, y and F are pre-multiplied by amp.
 enum RecField : int {
-    R_NXC = 0, R_NYC = 1, R_FXX = 2, R_FXY = 3,      // -xcen, -ycen, F11, F21
-    R_FYY = 4, R_HA = 5, R_HB = 6, R_C0 = 7,          // F22, -amp/24, -amp*c0, c0
-    R_SRC = 8, R_AMP = 9, R_SXX = 10, R_SYY = 11,     // source (int bits), amp, Sigma11, Sigma22
-    // Jacobian of (A, x, y, fxx, fyy, fxy) w.r.t. (flux, ra, dec, q, pa, n, rh);
-    // rows acting on x, y and F are pre-multiplied by amp (see tile kernel).
-    R_JA_FLUX = 12, R_JA_Q = 13, R_JA_PA = 14, R_JA_N = 15,
-    R_JA_RH = 16, R_JX_RA = 17, R_JY_RA = 18, R_JX_DEC = 19,
-    R_JY_DEC = 20, R_JFXX_Q = 21, R_JFXY_Q = 22, R_JFYY_Q = 23,
-    R_JFXX_PA = 24, R_JFXY_PA = 25, R_JFYY_PA = 26,
-    // 27..31 unused
+    R_NXC = 0,    // -xcen (x2)
+    R_NYC = 2,    // -ycen (x2)
+    R_FXX = 4,    // F11 (x2)
+    R_FXY = 6,    // F21 (x2)
+    R_FYY = 8,    // F22 (x2)
+    R_AMP = 10,   // amp (x2)
+    R_HB = 12,    // -amp * c0 (x2)
+    R_C0 = 14,    // c0 (x2)
+    R_JA_FLUX = 16, R_JA_Q = 17, R_JA_PA = 18, R_JA_N = 19,
+    R_JA_RH = 20, R_JX_RA = 21, R_JY_RA = 22, R_JX_DEC = 23,
+    R_JY_DEC = 24, R_JFXX_Q = 25, R_JFXY_Q = 26, R_JFYY_Q = 27,
+    R_JFXX_PA = 28, R_JFXY_PA = 29, R_JFYY_PA = 30,
+    R_SRC = 31,   // source index (int bits)
 };
 // c0 = 1 - (fxx + fyy)/24, so that H = 1 + (|v|^2 - fxx - fyy)/24 = |v|^2/24 + c0.
 
@@ -176,14 +184,14 @@ __device__ __forceinline__ void build_one_gaussian(const PatchView &pv, const fp
     const float tf = fm(tmp, flux);
 
     float4 *r4 = reinterpret_cast<float4 *>(rec);
-    r4[0] = make_float4(-xc, -yc, F.a, F.c);
-    r4[1] = make_float4(F.d, -amp * (1.0f / 24.0f), -amp * c0, c0);
-    r4[2] = make_float4(__int_as_float(s), amp, Sig.a, Sig.d);
-    r4[3] = make_float4(fm(tmp, samp), jA[0], jA[1], fm(tf, gal.damplitude_dnsersic[k]));
-    r4[4] = make_float4(fm(tf, gal.damplitude_drh[k]), amp * CW.a, amp * CW.c, amp * CW.b);
-    r4[5] = make_float4(amp * CW.d, amp * jF[0][0], amp * jF[0][1], amp * jF[0][2]);
-    r4[6] = make_float4(amp * jF[1][0], amp * jF[1][1], amp * jF[1][2], 0.0f);
-    r4[7] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    r4[0] = make_float4(-xc, -xc, -yc, -yc);
+    r4[1] = make_float4(F.a, F.a, F.c, F.c);
+    r4[2] = make_float4(F.d, F.d, amp, amp);
+    r4[3] = make_float4(-amp * c0, -amp * c0, c0, c0);
+    r4[4] = make_float4(fm(tmp, samp), jA[0], jA[1], fm(tf, gal.damplitude_dnsersic[k]));
+    r4[5] = make_float4(fm(tf, gal.damplitude_drh[k]), amp * CW.a, amp * CW.c, amp * CW.b);
+    r4[6] = make_float4(amp * CW.d, amp * jF[0][0], amp * jF[0][1], amp * jF[0][2]);
+    r4[7] = make_float4(amp * jF[1][0], amp * jF[1][1], amp * jF[1][2], __int_as_float(s));
 
     // exp-argument <= 36 ellipse: half-widths 6 sqrt(Sigma11), 6 sqrt(Sigma22)
     const float wx = 6.0f * sqrtf(fmaxf(Sig.a, 0.0f)) * (1.0f + CULL_REL) + CULL_ABS;

@@ -141,6 +141,95 @@ struct TileSmem {
     }
 };
 
+// ------------------------------------------------------------ per-Gaussian helpers
+// Two packed operands from one 16-byte shared-memory load.
+__device__ __forceinline__ void ld2(const float *p, v2 &a, v2 &b) {
+    const ulonglong2 t = *reinterpret_cast<const ulonglong2 *>(p);
+    a = t.x;
+    b = t.y;
+}
+
+// Pass 1 for one Gaussian over the thread's KP pixel pairs: R -= amp G H.
+template <int KP, bool CUT>
+__device__ __forceinline__ void residual_pairs(const v2 (&X)[KP], const v2 (&Y)[KP], v2 (&R)[KP],
+                                               v2 NXC, v2 NYC, v2 FXX, v2 FXY, v2 FYY, v2 HA,
+                                               v2 HB, v2 KEXP2, v2 KEXPLO2) {
+#pragma unroll
+    for (int j = 0; j < KP; ++j) {
+        const v2 DX = add2(X[j], NXC), DY = add2(Y[j], NYC);
+        const v2 VX = fma2(FXY, DY, mul2(FXX, DX));
+        const v2 VY = fma2(FXY, DX, mul2(FYY, DY));
+        const v2 Q = fma2(DY, VY, mul2(DX, VX));
+        // the residual needs an unbiased exponential (see exp2_unbiased)
+        v2 Gp = exp2_unbiased(fma2(Q, KEXP2, mul2(Q, KEXPLO2)));
+        if (CUT) {
+            float g0, g1, q0, q1;
+            unpk(Gp, g0, g1);
+            unpk(Q, q0, q1);
+            Gp = pk(q0 > FPHO_MAX_EXP_ARG ? 0.0f : g0, q1 > FPHO_MAX_EXP_ARG ? 0.0f : g1);
+        }
+        const v2 S = fma2(VY, VY, mul2(VX, VX));
+        R[j] = fma2(fma2(S, HA, HB), Gp, R[j]);  // fma(S, -amp/24, -amp c0) = -amp H
+    }
+}
+
+// Pass 2 for one Gaussian over the thread's KP pixel pairs: the twelve sums
+// from which the model's derivatives w.r.t. (A, x, y, fxx, fyy, fxy) follow.
+struct GradSums {
+    v2 A, HVx, HVy, Vx, Vy, HXX, HXY, HYY, W, T1, T2, T3;
+};
+template <int KP, bool CUT>
+__device__ __forceinline__ void gradient_pairs(const v2 (&X)[KP], const v2 (&Y)[KP],
+                                               const v2 (&R2)[KP], v2 NXC, v2 NYC, v2 FXX,
+                                               v2 FXY, v2 FYY, v2 C0, v2 C24, v2 KEXP2,
+                                               GradSums &s) {
+    s = GradSums{0ull, 0ull, 0ull, 0ull, 0ull, 0ull, 0ull, 0ull, 0ull, 0ull, 0ull, 0ull};
+#pragma unroll
+    for (int j = 0; j < KP; ++j) {
+        const v2 DX = add2(X[j], NXC), DY = add2(Y[j], NYC);
+        const v2 VX = fma2(FXY, DY, mul2(FXX, DX));
+        const v2 VY = fma2(FXY, DX, mul2(FYY, DY));
+        const v2 T1 = mul2(DX, VX);
+        const v2 Q = fma2(DY, VY, T1);
+        float e0, e1;
+        unpk(mul2(Q, KEXP2), e0, e1);
+        float g0 = ex2f(e0), g1 = ex2f(e1);
+        if (CUT) {
+            float q0, q1;
+            unpk(Q, q0, q1);
+            g0 = q0 > FPHO_MAX_EXP_ARG ? 0.0f : g0;
+            g1 = q1 > FPHO_MAX_EXP_ARG ? 0.0f : g1;
+        }
+        const v2 S = fma2(VY, VY, mul2(VX, VX));
+        const v2 H = fma2(S, C24, C0);
+        const v2 W = mul2(R2[j], pk(g0, g1));
+        const v2 WH = mul2(W, H);
+        s.A = add2(s.A, WH);
+        s.HVx = fma2(WH, VX, s.HVx);
+        s.HVy = fma2(WH, VY, s.HVy);
+        s.Vx = fma2(W, VX, s.Vx);
+        s.Vy = fma2(W, VY, s.Vy);
+        const v2 HDX = mul2(WH, DX);
+        s.HXX = fma2(HDX, DX, s.HXX);
+        s.HXY = fma2(HDX, DY, s.HXY);
+        s.HYY = fma2(mul2(WH, DY), DY, s.HYY);
+        s.W = add2(s.W, W);
+        s.T1 = fma2(W, T1, s.T1);
+        s.T2 = fma2(W, mul2(DY, VY), s.T2);
+        s.T3 = fma2(W, fma2(DX, VY, mul2(DY, VX)), s.T3);
+    }
+}
+
+__device__ __forceinline__ float lanesum(v2 v) {
+    float a, b;
+    unpk(v, a, b);
+    return a + b;
+}
+
+// live_flag bits
+constexpr int FLAG_CUT = 1;        // the exp-argument can exceed 36 inside the tile
+constexpr int FLAG_LAST_SRC = 2;   // last kept Gaussian of its source in the chunk
+
 // ------------------------------------------------------------ the tile body
 template <int NT, int K>
 __device__ __forceinline__ void tile_body(const TileArgs &A, int tile, unsigned char *smem,
@@ -168,7 +257,7 @@ __device__ __forceinline__ void tile_body(const TileArgs &A, int tile, unsigned 
 
     for (int j = tid; j < NW * stride; j += NT) wacc[j] = 0.0f;
 
-    // ---- load this thread's pixels (packed pairs: pixel j and j+1 of the thread)
+    // ---- this thread's pixels: pair j holds local pixels tid + 2j*NT and tid + (2j+1)*NT
     const float xmid = 0.5f * (bb.x + bb.y), ymid = 0.5f * (bb.z + bb.w);
     v2 X[KP], Y[KP], R[KP], R2[KP];
     float D[K], IE[K];
@@ -197,12 +286,13 @@ __device__ __forceinline__ void tile_body(const TileArgs &A, int tile, unsigned 
     __syncthreads();
     const bool tile_has_weight = s_any_weight != 0;
 
-    const v2 KEXP2 = pk1(KEXP);
-    const v2 KEXPLO2 = pk1(KEXP_LO);
+    const v2 KEXP2 = pk1(KEXP), KEXPLO2 = pk1(KEXP_LO);
+    const v2 CM24 = pk1(-1.0f / 24.0f), C24 = pk1(1.0f / 24.0f);
     long long npairs = 0;
 
-    // ---- chunked scan + stage.  Returns the number of staged records; `cursor`
-    // advances through [g0, g1).
+    // ---- chunked scan + stage: keeps the exposure's Gaussians whose culling
+    // box overlaps the tile, in order, up to `cap` per chunk; `cursor` advances
+    // through [g0, g1).  Returns the number of staged records.
     auto scan_and_stage = [&](int &cursor) -> int {
         int n = 0;
         while (cursor < g1 && n + NT <= cap) {
@@ -237,7 +327,8 @@ __device__ __forceinline__ void tile_body(const TileArgs &A, int tile, unsigned 
         }
         mbar_wait_bounded(mbar, phase, A.err);
         phase ^= 1u;
-        // per (tile, Gaussian): can the exp-argument cross 36 inside the tile?
+        // per kept Gaussian: can the exp-argument cross 36 inside the tile (its
+        // maximum over the box is at a corner), and is it its source's last?
         for (int i = tid; i < n; i += NT) {
             const float *r = recs + (size_t)i * GREC;
             const float nxc = r[R_NXC], nyc = r[R_NYC];
@@ -250,7 +341,10 @@ __device__ __forceinline__ void tile_body(const TileArgs &A, int tile, unsigned 
                 const float q = dx * (fxx * dx + fxy * dy) + dy * (fyy * dy + fxy * dx);
                 qmax = fmaxf(qmax, q);
             }
-            live_flag[i] = (qmax * (1.0f + CULL_REL) + CULL_ABS >= FPHO_MAX_EXP_ARG) ? 1 : 0;
+            const int src = __float_as_int(r[R_SRC]);
+            const int nxt = (i + 1 < n) ? __float_as_int(recs[(size_t)(i + 1) * GREC + R_SRC]) : -1;
+            live_flag[i] = ((qmax * (1.0f + CULL_REL) + CULL_ABS >= FPHO_MAX_EXP_ARG) ? FLAG_CUT : 0) |
+                           ((nxt != src) ? FLAG_LAST_SRC : 0);
         }
         __syncthreads();
         return n;
@@ -270,31 +364,19 @@ __device__ __forceinline__ void tile_body(const TileArgs &A, int tile, unsigned 
             n_last = n;
             npairs += (long long)n;
             for (int i = 0; i < n; ++i) {
-                const float4 *r4 = reinterpret_cast<const float4 *>(recs + (size_t)i * GREC);
-                const float4 a = r4[0], b = r4[1];
-                const v2 NXC = pk1(a.x), NYC = pk1(a.y), FXX = pk1(a.z), FXY = pk1(a.w);
-                const v2 FYY = pk1(b.x), HA = pk1(b.y), HB = pk1(b.z);
-                const bool cut = live_flag[i] != 0;
-#pragma unroll
-                for (int j = 0; j < KP; ++j) {
-                    const v2 DX = add2(X[j], NXC), DY = add2(Y[j], NYC);
-                    const v2 VX = fma2(FXY, DY, mul2(FXX, DX));
-                    const v2 VY = fma2(FXY, DX, mul2(FYY, DY));
-                    const v2 Q = fma2(DY, VY, mul2(DX, VX));
-                    // the residual needs an unbiased exponential (see exp2_unbiased)
-                    v2 Gp = exp2_unbiased(fma2(Q, KEXP2, mul2(Q, KEXPLO2)));
-                    if (cut) {
-                        float g0v, g1v, q0, q1;
-                        unpk(Gp, g0v, g1v);
-                        unpk(Q, q0, q1);
-                        g0v = (q0 > FPHO_MAX_EXP_ARG) ? 0.0f : g0v;
-                        g1v = (q1 > FPHO_MAX_EXP_ARG) ? 0.0f : g1v;
-                        Gp = pk(g0v, g1v);
-                    }
-                    const v2 S = fma2(VY, VY, mul2(VX, VX));
-                    const v2 NAH = fma2(S, HA, HB);  // -amp * H
-                    R[j] = fma2(NAH, Gp, R[j]);
-                }
+                const float *r = recs + (size_t)i * GREC;
+                v2 NXC, NYC, FXX, FXY, FYY, AMP, HB, C0;
+                ld2(r + R_NXC, NXC, NYC);
+                ld2(r + R_FXX, FXX, FXY);
+                ld2(r + R_FYY, FYY, AMP);
+                ld2(r + R_HB, HB, C0);
+                const v2 HA = mul2(AMP, CM24);
+                if (live_flag[i] & FLAG_CUT)
+                    residual_pairs<KP, true>(X, Y, R, NXC, NYC, FXX, FXY, FYY, HA, HB, KEXP2,
+                                             KEXPLO2);
+                else
+                    residual_pairs<KP, false>(X, Y, R, NXC, NYC, FXX, FXY, FYY, HA, HB, KEXP2,
+                                              KEXPLO2);
             }
         }
     }
@@ -326,11 +408,11 @@ __device__ __forceinline__ void tile_body(const TileArgs &A, int tile, unsigned 
 
     // ------------------------------------------------------------ pass 2
     if (tile_has_weight) {
-        const v2 C24 = pk1(1.0f / 24.0f);
         // re-use the staged chunk if the kept set fit in one, otherwise rescan
         int cursor2 = g0;
         bool first = true;
         const bool reuse = (npairs == (long long)n_last);
+        float P[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         while (first || cursor2 < g1) {
             int n;
             if (first && reuse) {
@@ -341,87 +423,48 @@ __device__ __forceinline__ void tile_body(const TileArgs &A, int tile, unsigned 
                 n = scan_and_stage(cursor2);
             }
             first = false;
-            v2 P[7];
-#pragma unroll
-            for (int k = 0; k < 7; ++k) P[k] = 0ull;
             for (int i = 0; i < n; ++i) {
-                const float4 *r4 = reinterpret_cast<const float4 *>(recs + (size_t)i * GREC);
-                const float4 a = r4[0], b = r4[1];
-                const v2 NXC = pk1(a.x), NYC = pk1(a.y), FXX = pk1(a.z), FXY = pk1(a.w);
-                const v2 FYY = pk1(b.x), C0 = pk1(b.w);
-                const bool cut = live_flag[i] != 0;
-                v2 aA = 0ull, aHVx = 0ull, aHVy = 0ull, aVx = 0ull, aVy = 0ull;
-                v2 aHXX = 0ull, aHXY = 0ull, aHYY = 0ull, aW = 0ull;
-                v2 aT1 = 0ull, aT2 = 0ull, aT3 = 0ull;
-#pragma unroll
-                for (int j = 0; j < KP; ++j) {
-                    const v2 DX = add2(X[j], NXC), DY = add2(Y[j], NYC);
-                    const v2 VX = fma2(FXY, DY, mul2(FXX, DX));
-                    const v2 VY = fma2(FXY, DX, mul2(FYY, DY));
-                    const v2 T1 = mul2(DX, VX);
-                    const v2 Q = fma2(DY, VY, T1);
-                    const v2 E = mul2(Q, KEXP2);
-                    float e0, e1, q0, q1;
-                    unpk(E, e0, e1);
-                    float g0v = ex2f(e0), g1v = ex2f(e1);
-                    if (cut) {
-                        unpk(Q, q0, q1);
-                        g0v = (q0 > FPHO_MAX_EXP_ARG) ? 0.0f : g0v;
-                        g1v = (q1 > FPHO_MAX_EXP_ARG) ? 0.0f : g1v;
-                    }
-                    const v2 S = fma2(VY, VY, mul2(VX, VX));
-                    const v2 H = fma2(S, C24, C0);
-                    const v2 W = mul2(R2[j], pk(g0v, g1v));
-                    const v2 WH = mul2(W, H);
-                    aA = add2(aA, WH);
-                    aHVx = fma2(WH, VX, aHVx);
-                    aHVy = fma2(WH, VY, aHVy);
-                    aVx = fma2(W, VX, aVx);
-                    aVy = fma2(W, VY, aVy);
-                    const v2 HDX = mul2(WH, DX);
-                    aHXX = fma2(HDX, DX, aHXX);
-                    aHXY = fma2(HDX, DY, aHXY);
-                    aHYY = fma2(mul2(WH, DY), DY, aHYY);
-                    aW = add2(aW, W);
-                    aT1 = fma2(W, T1, aT1);
-                    aT2 = fma2(W, mul2(DY, VY), aT2);
-                    aT3 = fma2(W, fma2(DX, VY, mul2(DY, VX)), aT3);
-                }
+                const float *r = recs + (size_t)i * GREC;
+                v2 NXC, NYC, FXX, FXY, FYY, AMP, HB, C0;
+                ld2(r + R_NXC, NXC, NYC);
+                ld2(r + R_FXX, FXX, FXY);
+                ld2(r + R_FYY, FYY, AMP);
+                ld2(r + R_HB, HB, C0);
+                const int flag = live_flag[i];
+                GradSums s;
+                if (flag & FLAG_CUT)
+                    gradient_pairs<KP, true>(X, Y, R2, NXC, NYC, FXX, FXY, FYY, C0, C24, KEXP2, s);
+                else
+                    gradient_pairs<KP, false>(X, Y, R2, NXC, NYC, FXX, FXY, FYY, C0, C24, KEXP2, s);
                 // image-space gradient of this Gaussian over the thread's pixels
-                // (amp factors are folded into the Jacobian rows)
-                const v2 C12 = pk1(1.0f / 12.0f), CM12 = pk1(-1.0f / 12.0f);
-                const v2 CMH = pk1(-0.5f), CM24 = pk1(-1.0f / 24.0f), CM1 = pk1(-1.0f);
-                const v2 gA = aA;
-                const v2 gx = fma2(CM12, fma2(FXY, aVy, mul2(FXX, aVx)), aHVx);
-                const v2 gy = fma2(CM12, fma2(FXY, aVx, mul2(FYY, aVy)), aHVy);
-                const v2 wq = mul2(aW, CM24);
-                const v2 gfxx = fma2(C12, aT1, fma2(CMH, aHXX, wq));
-                const v2 gfyy = fma2(C12, aT2, fma2(CMH, aHYY, wq));
-                const v2 gfxy = fma2(C12, aT3, mul2(CM1, aHXY));
-                const float4 j3 = r4[3], j4 = r4[4], j5 = r4[5], j6 = r4[6];
-                P[0] = fma2(pk1(j3.x), gA, P[0]);
-                P[1] = fma2(pk1(j4.z), gy, fma2(pk1(j4.y), gx, P[1]));
-                P[2] = fma2(pk1(j5.x), gy, fma2(pk1(j4.w), gx, P[2]));
-                P[3] = fma2(pk1(j5.w), gfyy,
-                            fma2(pk1(j5.z), gfxy, fma2(pk1(j5.y), gfxx, fma2(pk1(j3.y), gA, P[3]))));
-                P[4] = fma2(pk1(j6.z), gfyy,
-                            fma2(pk1(j6.y), gfxy, fma2(pk1(j6.x), gfxx, fma2(pk1(j3.z), gA, P[4]))));
-                P[5] = fma2(pk1(j3.w), gA, P[5]);
-                P[6] = fma2(pk1(j4.x), gA, P[6]);
+                // (amp factors are folded into the Jacobian rows), in scalars
+                const float fxx = lo(FXX), fxy = lo(FXY), fyy = lo(FYY);
+                const float sVx = lanesum(s.Vx), sVy = lanesum(s.Vy), sW = lanesum(s.W);
+                const float gA = lanesum(s.A);
+                const float gx = lanesum(s.HVx) - (fxx * sVx + fxy * sVy) * (1.0f / 12.0f);
+                const float gy = lanesum(s.HVy) - (fxy * sVx + fyy * sVy) * (1.0f / 12.0f);
+                const float gfxx = lanesum(s.T1) * (1.0f / 12.0f) - 0.5f * lanesum(s.HXX) -
+                                   sW * (1.0f / 24.0f);
+                const float gfyy = lanesum(s.T2) * (1.0f / 12.0f) - 0.5f * lanesum(s.HYY) -
+                                   sW * (1.0f / 24.0f);
+                const float gfxy = lanesum(s.T3) * (1.0f / 12.0f) - lanesum(s.HXY);
+                const float4 j0 = *reinterpret_cast<const float4 *>(r + 16);
+                const float4 j1 = *reinterpret_cast<const float4 *>(r + 20);
+                const float4 j2 = *reinterpret_cast<const float4 *>(r + 24);
+                const float4 j3 = *reinterpret_cast<const float4 *>(r + 28);
+                P[0] = fmaf(j0.x, gA, P[0]);
+                P[1] = fmaf(j1.z, gy, fmaf(j1.y, gx, P[1]));
+                P[2] = fmaf(j2.x, gy, fmaf(j1.w, gx, P[2]));
+                P[3] = fmaf(j2.w, gfyy, fmaf(j2.z, gfxy, fmaf(j2.y, gfxx, fmaf(j0.y, gA, P[3]))));
+                P[4] = fmaf(j3.z, gfyy, fmaf(j3.y, gfxy, fmaf(j3.x, gfxx, fmaf(j0.z, gA, P[4]))));
+                P[5] = fmaf(j0.w, gA, P[5]);
+                P[6] = fmaf(j1.x, gA, P[6]);
                 // flush at a source boundary or at the end of the chunk
-                const int src = __float_as_int(r4[2].x);
-                const int nsrc_next =
-                    (i + 1 < n) ? __float_as_int(recs[(size_t)(i + 1) * GREC + R_SRC]) : -1;
-                if (nsrc_next != src) {
-                    float v[8];
+                if (flag & FLAG_LAST_SRC) {
+                    const int src = __float_as_int(j3.w);
+                    float v[8] = {P[0], P[1], P[2], P[3], P[4], P[5], P[6], 0.0f};
 #pragma unroll
-                    for (int k = 0; k < 7; ++k) {
-                        float l, h;
-                        unpk(P[k], l, h);
-                        v[k] = l + h;
-                        P[k] = 0ull;
-                    }
-                    v[7] = 0.0f;
+                    for (int k = 0; k < 7; ++k) P[k] = 0.0f;
                     const float tot = warp_reduce7(v, lane);
                     const int k = reduce7_index(lane);
                     if ((lane & 3) == 0 && k < 7) wacc[warp * stride + src * 7 + k] += tot;

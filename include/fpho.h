@@ -203,10 +203,11 @@ FPHO_API int fpho_patch_set_config(fpho_patch *p, int variant, int live_cap, voi
  * evaluation (synchronizes).  last_count may be NULL. */
 FPHO_API int fpho_patch_count_pairs(fpho_patch *p, int enable, long long *last_count);
 
-/* Copy the image-Gaussian records (32 floats each: -xcen, -ycen, fxx, fxy,
- * fyy, -amp/24, -amp*c0, c0, source, amp, ... Jacobian) that the last
- * evaluation built for one exposure to host memory; *n_out receives the
- * number of records.  Synchronizes the device. */
+/* Copy the image-Gaussian records that the last evaluation built for one
+ * exposure to host memory (32 floats each: -xcen, -ycen, fxx, fxy, fyy, amp,
+ * -amp*c0 and c0 = 1 - (fxx+fyy)/24, each stored twice, in floats 0..15; the
+ * 15-term Jacobian in floats 16..30; the source index as int bits in float
+ * 31); *n_out receives the number of records.  Synchronizes the device. */
 FPHO_API int fpho_patch_image_gaussians(fpho_patch *p, int exposure, float *host_out,
                                         int max_records, int *n_out);
 

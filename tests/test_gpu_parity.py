@@ -222,7 +222,8 @@ def test_image_gaussians_bitexact(name):
                       len(ref), ctypes.byref(n))
             assert n.value == len(ref)
             # reference ImageGaussian order: amp, xcen, ycen, fxx, fyy, fxy
-            got = np.stack([buf[:, 9], -buf[:, 0], -buf[:, 1], buf[:, 2], buf[:, 4], buf[:, 3]], 1)
+            got = np.stack([buf[:, 10], -buf[:, 0], -buf[:, 2], buf[:, 4], buf[:, 8], buf[:, 6]],
+                           1)
             want = ref[:, :6]
             np.testing.assert_array_equal(got, want)
             n_exact += got.size
