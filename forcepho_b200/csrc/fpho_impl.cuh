@@ -211,14 +211,10 @@ __device__ __forceinline__ v2 pk(float lo, float hi) {
 }
 __device__ __forceinline__ v2 pk1(float x) { return pk(x, x); }
 __device__ __forceinline__ float lo(v2 v) {
-    float a, b;
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
-    return a;
+    return __uint_as_float(static_cast<unsigned int>(v & 0xffffffffull));
 }
 __device__ __forceinline__ float hi(v2 v) {
-    float a, b;
-    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
-    return b;
+    return __uint_as_float(static_cast<unsigned int>(v >> 32));
 }
 __device__ __forceinline__ void unpk(v2 v, float &a, float &b) {
     asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));

@@ -1,0 +1,79 @@
+// fpho_kernels.cuh -- small kernels around the tile kernel, included (with
+// internal linkage) by every translation unit that launches them.
+#pragma once
+
+#include "fpho_impl.cuh"
+
+namespace fpho {
+
+// One thread per image Gaussian of exposure blockIdx.y: record + culling box.
+static __global__ void build_image_gaussians(PatchView pv, const fpho_source *src, float *gtab,
+                                             float4 *gbox) {
+    const int e = blockIdx.y;
+    const int g0 = pv.gauss_start[e];
+    const int n = pv.gauss_start[e + 1] - g0;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int npsf = pv.exp_npsf[e];
+    const int s = i / npsf, p = i - s * npsf;
+    build_one_gaussian(pv, src, e, s, p, gtab + (size_t)(g0 + i) * GREC, gbox + g0 + i);
+}
+
+// Bounding boxes of every tile: over all pixels and over pixels with
+// ierr != 0.  If n_tiles_dev is given, blocks at or beyond *n_tiles_dev exit.
+static __global__ void tile_bboxes(PatchView pv, const TileDesc *tiles, float4 *tbox_all,
+                                   float4 *tbox_w, const int *n_tiles_dev) {
+    if (n_tiles_dev && (int)blockIdx.x >= *n_tiles_dev) return;
+    const TileDesc td = tiles[blockIdx.x];
+    float ax0 = INFINITY, ax1 = -INFINITY, ay0 = INFINITY, ay1 = -INFINITY;
+    float wx0 = INFINITY, wx1 = -INFINITY, wy0 = INFINITY, wy1 = -INFINITY;
+    for (int i = threadIdx.x; i < td.count; i += blockDim.x) {
+        const int pix = td.pix_begin + i;
+        const float x = pv.xpix[pix], y = pv.ypix[pix];
+        ax0 = fminf(ax0, x); ax1 = fmaxf(ax1, x);
+        ay0 = fminf(ay0, y); ay1 = fmaxf(ay1, y);
+        if (pv.ierr[pix] != 0.0f) {
+            wx0 = fminf(wx0, x); wx1 = fmaxf(wx1, x);
+            wy0 = fminf(wy0, y); wy1 = fmaxf(wy1, y);
+        }
+    }
+    __shared__ float red[8][32];
+    float v[8] = {ax0, -ax1, ay0, -ay1, wx0, -wx1, wy0, -wy1};
+#pragma unroll
+    for (int k = 0; k < 8; ++k)
+        for (int o = 16; o > 0; o >>= 1) v[k] = fminf(v[k], __shfl_xor_sync(0xffffffffu, v[k], o));
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (lane == 0)
+        for (int k = 0; k < 8; ++k) red[k][warp] = v[k];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const int nw = blockDim.x / 32;
+        for (int k = 0; k < 8; ++k)
+            for (int w = 1; w < nw; ++w) red[k][0] = fminf(red[k][0], red[k][w]);
+        tbox_all[blockIdx.x] = make_float4(red[0][0], -red[1][0], red[2][0], -red[3][0]);
+        tbox_w[blockIdx.x] = make_float4(red[4][0], -red[5][0], red[6][0], -red[7][0]);
+    }
+}
+
+// Sum tile partials per band in double.  grid (n_bands, ceil(out_stride/128)).
+static __global__ void reduce_bands(const int *tile_band_start, const double *pchi2,
+                                    const float *pgrad, int stride, double *chi2_out,
+                                    float *dchi2_out, int out_stride) {
+    const int b = blockIdx.x;
+    const int t0 = tile_band_start[b], t1 = tile_band_start[b + 1];
+    const int j = blockIdx.y * blockDim.x + threadIdx.x;
+    if (j < out_stride) {
+        double acc = 0.0;
+        if (j < stride)
+            for (int t = t0; t < t1; ++t) acc += (double)pgrad[(size_t)t * stride + j];
+        dchi2_out[(size_t)b * out_stride + j] = (float)acc;
+    }
+    if (blockIdx.y == 0 && threadIdx.x < 32) {
+        double c = 0.0;
+        for (int t = t0 + threadIdx.x; t < t1; t += 32) c += pchi2[t];
+        for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+        if (threadIdx.x == 0) chi2_out[b] = c;
+    }
+}
+
+}  // namespace fpho
