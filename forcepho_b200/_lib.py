@@ -63,6 +63,9 @@ _SIGS = {
                                        c_uint, c_void_p]),
     "fpho_EvaluateProposal": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                       c_void_p]),
+    "fpho_evaluate_proposal_noalloc": (c_int, [c_void_p, c_int, c_int, ctypes.c_int64, c_int,
+                                               c_void_p, c_void_p, c_void_p, c_int, c_void_p,
+                                               c_void_p]),
     "fpho_patch_time_tiles": (c_int, [c_void_p, c_int]),
     "fpho_patch_image_gaussians": (c_int, [c_void_p, c_int, c_void_p, c_int,
                                            ctypes.POINTER(c_int)]),

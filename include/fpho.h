@@ -183,6 +183,41 @@ FPHO_API int fpho_evaluate_proposal(fpho_patch *p, const fpho_source *proposal, 
 FPHO_API int fpho_EvaluateProposal(fpho_patch *p, const void *dev_patch_struct, const void *dev_proposal,
                           void *pchi2, void *pdchi2_dp, void *stream);
 
+/* ---- evaluation without allocation (no counterpart in the reference) ---- */
+
+/* Size of the device array that holds all scratch of
+ * fpho_evaluate_proposal_noalloc (one per device, alive until process exit). */
+#define FPHO_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
+
+/* Same computation as fpho_evaluate_proposal, for callers that cannot
+ * allocate device memory: code running while a CUDA graph is captured,
+ * plugins whose host framework owns every device allocation, services that
+ * must not grow or fragment device memory after start-up.  It calls no
+ * cudaMalloc/cudaFree and no allocating library routine; its scratch (tile
+ * plan, image Gaussians, per-tile partial sums) lives in a file-scope device
+ * array of FPHO_NOALLOC_SCRATCH_BYTES.
+ *   patch         host struct whose array pointers are DEVICE pointers
+ *                 (residual may be NULL; if set, data - model is written there)
+ *   n_bands, n_exp  band and exposure counts of the index arrays
+ *   total_pixels  upper bound on the sum of exposure_N
+ *   max_psf_per_source  upper bound on n_psf_per_source[]
+ *   dev_proposal, dev_chi2, dev_dchi2  device fpho_source[n_sources],
+ *                 double[n_bands], float[n_bands][dchi2_stride]
+ *   dev_status    optional device int: 0, or error bits (1 a bounded wait gave
+ *                 up, 2 inconsistent index arrays, 4 a size bound was
+ *                 exceeded, 8 a PSF radius bin out of range)
+ * Sizes whose scratch exceeds FPHO_NOALLOC_SCRATCH_BYTES are rejected with
+ * FPHO_ERR_LIMIT.  The first call on a device looks up the array's address
+ * and sets a kernel attribute: make it before any stream capture.  All calls
+ * share the array, which keeps the last call's contents; calls that overlap
+ * on the GPU race and must be serialized.  The call is asynchronous. */
+FPHO_API int fpho_evaluate_proposal_noalloc(const fpho_patch_struct *patch, int n_bands,
+                                            int n_exp, int64_t total_pixels,
+                                            int max_psf_per_source,
+                                            const fpho_source *dev_proposal, double *dev_chi2,
+                                            float *dev_dchi2, int dchi2_stride, int *dev_status,
+                                            void *stream);
+
 /* Read (and keep) the error word of the last evaluation: bit 0 set when a
  * bounded wait on a bulk copy gave up.  Synchronizes the device. */
 FPHO_API int fpho_patch_error_word(fpho_patch *p, int *out);
