@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--variant", type=int, default=None)
     ap.add_argument("--live-cap", type=int, default=None)
+    ap.add_argument("--batch-patches", type=int, default=256,
+                    help="patches of the batched leg (config 3); 0 skips it")
     return ap.parse_args()
 
 
@@ -193,6 +195,78 @@ def probe_fp32(torch, lib):
     return res[0] / 1e12, res[1] / 1e9
 
 
+def batched_leg(args, torch, lib, steps):
+    """Config 3: 256 uneven patches.  Batched evaluation (one persistent launch
+    per step, replayed from a CUDA graph) against the plain form (one
+    fpho_evaluate_proposal per patch), both on device-resident buffers."""
+    from forcepho_b200 import synth
+    from forcepho_b200.batch import PatchBatch
+    patches = synth.make_config(3, seed=args.seed + 3, render=synth.render_model_gpu,
+                                n_patches=args.batch_patches)
+    for P in patches:
+        P.return_residual = False
+        P.send_to_device()
+    batch = PatchBatch(patches)
+    dprop, chi2, dchi2 = batch.device_buffers()
+    s = torch.cuda.current_stream()
+    nominal = int(sum(P.pairs_per_eval for P in patches))
+    batch.count_pairs(True)
+    batch.evaluate_device(dprop, chi2, dchi2)
+    torch.cuda.synchronize()
+    evaluated = batch.count_pairs(False)
+    graph = batch.capture_graph(dprop, chi2, dchi2)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    def timed(fn, n):
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(n)]
+        for e0, e1 in evs:
+            flush.zero_()
+            e0.record(s)
+            fn()
+            e1.record(s)
+        torch.cuda.synchronize()
+        return float(np.sum([a.elapsed_time(b) for a, b in evs])) / n
+
+    for _ in range(3):
+        graph.replay()
+    ms_batched = timed(graph.replay, steps)
+
+    # plain: one launch sequence per patch, device buffers per patch
+    bufs = []
+    for P in patches:
+        q = torch.from_numpy(P.proposal().view(np.uint8).copy()).cuda()
+        c = torch.zeros(P.n_bands, dtype=torch.float64, device="cuda")
+        g = torch.zeros(P.n_bands * P.n_sources * 7, dtype=torch.float32, device="cuda")
+        bufs.append((P.device_patch.handle, q, c, g, P.n_sources))
+
+    def plain():
+        for h, q, c, g, ns in bufs:
+            lib.call("fpho_evaluate_proposal", h, q.data_ptr(), ns, c.data_ptr(), g.data_ptr(),
+                     7 * ns, 0, s.cuda_stream)
+
+    for _ in range(2):
+        plain()
+    ms_plain = timed(plain, max(3, steps // 4))
+    n = len(patches)
+    out = {"workload": f"config3: {n} patches, sources U{{1..30}}, bands U{{1..8}}, "
+                       "exposures/band U{1..8}, side U[32,200] px",
+           "patches": n, "nominal_pairs_per_step": nominal, "evaluated_pairs_per_step": evaluated,
+           "work_items": batch.n_work, "persistent_grid": batch.grid,
+           "batched_ms_per_step": ms_batched, "plain_ms_per_step": ms_plain,
+           "batched_patch_evals_per_s": n / (ms_batched * 1e-3),
+           "plain_patch_evals_per_s": n / (ms_plain * 1e-3),
+           "batched_pix_gauss_per_s": nominal / (ms_batched * 1e-3),
+           "speedup_batched_vs_plain": ms_plain / ms_batched,
+           "timing": "CUDA events per step, L2 flushed between steps; batched step replayed "
+                     "from a CUDA graph"}
+    del graph
+    batch.free()
+    for P in patches:
+        P.free()
+    return out
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -308,6 +382,10 @@ def run_ours(args):
     achieved = evaluated_pairs * FLOPS_PER_PAIR / tile_s / 1e12
     sfu = evaluated_pairs * 2 / tile_s / 1e9
 
+    batched = None
+    if args.batch_patches > 0:
+        batched = batched_leg(args, torch, _lib, steps=max(3, min(args.steps, 50)))
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cores = len(os.sched_getaffinity(0))
@@ -342,6 +420,7 @@ def run_ours(args):
                          "sfu_gops": sfu, "sfu_peak_gops": ex2_gops, "sfu_frac": sfu / ex2_gops},
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
+            "batched": batched,
         }
         print(json.dumps(line), flush=True)
     P.free()

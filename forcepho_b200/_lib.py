@@ -66,6 +66,13 @@ _SIGS = {
     "fpho_evaluate_proposal_noalloc": (c_int, [c_void_p, c_int, c_int, ctypes.c_int64, c_int,
                                                c_void_p, c_void_p, c_void_p, c_int, c_void_p,
                                                c_void_p]),
+    "fpho_batch_create": (c_int, [c_void_p, c_int, c_int, c_void_p, ctypes.POINTER(c_void_p)]),
+    "fpho_batch_info": (c_int, [c_void_p, c_int64_p]),
+    "fpho_batch_evaluate": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_uint, c_void_p]),
+    "fpho_batch_count_pairs": (c_int, [c_void_p, c_int, ctypes.POINTER(ctypes.c_longlong)]),
+    "fpho_batch_time_tiles": (c_int, [c_void_p, c_int]),
+    "fpho_batch_last_tile_ms": (c_int, [c_void_p, ctypes.POINTER(ctypes.c_float)]),
+    "fpho_batch_free": (c_int, [c_void_p]),
     "fpho_patch_time_tiles": (c_int, [c_void_p, c_int]),
     "fpho_patch_image_gaussians": (c_int, [c_void_p, c_int, c_void_p, c_int,
                                            ctypes.POINTER(c_int)]),

@@ -1,0 +1,426 @@
+// fpho_batch.cu -- many patches evaluated by one persistent launch.
+//
+// A batch is a list of patch handles evaluated together:
+//   batch_gaussians  one launch builds the image Gaussians of every exposure
+//                    of every patch (grid y = (patch, exposure) pairs);
+//   batch_tiles      one persistent launch: each CTA takes (patch, tile) items
+//                    from a work list sorted by decreasing cost (pixels x image
+//                    Gaussians of the tile's exposure), through an atomic
+//                    counter, until the list is exhausted -- patches of 1..30
+//                    sources and 32^2..200^2 pixels balance across the SMs;
+//   batch_reduce     one launch sums the tile partials of every (patch, band)
+//                    in double and resets the work counter for the next call.
+// No kernel waits on another CTA: the counter only hands out indices.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+#include <new>
+#include <numeric>
+#include <vector>
+
+#include "fpho_handle.h"
+#include "fpho_internal.h"
+#include "fpho_kernels.cuh"
+#include "fpho_tile.cuh"
+
+namespace fpho {
+namespace {
+
+constexpr int BT_THREADS = 128;
+constexpr int BT_K = 4;
+
+struct BatchPatch {
+    PatchView pv;
+    float *gtab;
+    float4 *gbox;
+    int prop_off;  // first source of this patch in the concatenated proposal
+};
+
+struct BandJob {
+    int t0, t1;         // tile range of the band in the patch's partials
+    int stride;         // 7 * n_sources of the patch
+    int chi2_index;     // output index into the concatenated chi2
+    long long dchi2_off;  // output offset into the concatenated dchi2
+    const double *pchi2;
+    const float *pgrad;
+};
+
+__global__ void batch_gaussians(const BatchPatch *bps, const int2 *expmap,
+                                const fpho_source *props) {
+    const int2 pe = expmap[blockIdx.y];
+    const BatchPatch &bp = bps[pe.x];
+    const int e = pe.y;
+    const int g0 = bp.pv.gauss_start[e];
+    const int n = bp.pv.gauss_start[e + 1] - g0;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int npsf = bp.pv.exp_npsf[e];
+    const int s = i / npsf, p = i - s * npsf;
+    build_one_gaussian(bp.pv, props + bp.prop_off, e, s, p, bp.gtab + (size_t)(g0 + i) * GREC,
+                       bp.gbox + g0 + i);
+}
+
+template <int NT, int K>
+__global__ void __launch_bounds__(NT) batch_tiles(const TileArgs *args, const int2 *work,
+                                                  int n_work, int *counter) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ uint64_t mbar;
+    __shared__ int s_item;
+    if (threadIdx.x == 0) {
+        mbar_init(&mbar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    uint32_t phase = 0;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+        __syncthreads();
+        const int it = s_item;
+        __syncthreads();  // all threads hold `it` before s_item is rewritten
+        if (it >= n_work) break;
+        const int2 w = work[it];
+        tile_body<NT, K>(args[w.x], w.y, smem, &mbar, phase);
+        __syncthreads();  // shared memory of this tile fully consumed
+    }
+}
+
+__global__ void batch_reduce(const BandJob *jobs, double *chi2, float *dchi2, int *counter) {
+    const BandJob jb = jobs[blockIdx.x];
+    const int j = blockIdx.y * blockDim.x + threadIdx.x;
+    if (j < jb.stride) {
+        double acc = 0.0;
+        for (int t = jb.t0; t < jb.t1; ++t) acc += (double)jb.pgrad[(size_t)t * jb.stride + j];
+        dchi2[jb.dchi2_off + j] = (float)acc;
+    }
+    if (blockIdx.y == 0 && threadIdx.x < 32) {
+        double c = 0.0;
+        for (int t = jb.t0 + threadIdx.x; t < jb.t1; t += 32) c += jb.pchi2[t];
+        for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+        if (threadIdx.x == 0) chi2[jb.chi2_index] = c;
+    }
+    if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) *counter = 0;
+}
+
+std::mutex g_attr_mu;
+size_t g_attr_set[64];
+
+}  // namespace
+}  // namespace fpho
+
+using namespace fpho;
+
+struct fpho_batch {
+    std::vector<fpho_patch *> patches;
+    int live_cap = 256;
+    int n_work = 0, n_exp_total = 0, max_g = 0, n_jobs = 0, max_stride = 0;
+    int n_src_total = 0, n_band_total = 0;
+    long long n_dchi2 = 0;
+    size_t smem = 0;
+    int grid = 0;
+    BatchPatch *d_bps = nullptr;
+    int2 *d_expmap = nullptr;
+    TileArgs *d_args = nullptr;
+    int2 *d_work = nullptr;
+    BandJob *d_jobs = nullptr;
+    int *d_counter = nullptr;
+    int *d_err = nullptr;
+    long long *d_pairs = nullptr;
+    int count_pairs = 0;
+    // staging for host I/O
+    fpho_source *d_props = nullptr;
+    double *d_chi2 = nullptr;
+    float *d_dchi2 = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    std::vector<TileArgs> h_args;
+};
+
+#define CUDA_TRY(call)                                                                  \
+    do {                                                                                \
+        cudaError_t e_ = (call);                                                        \
+        if (e_ != cudaSuccess)                                                          \
+            return set_error(FPHO_ERR_CUDA, "%s failed: %s (%s:%d)", #call,             \
+                             cudaGetErrorString(e_), __FILE__, __LINE__);               \
+    } while (0)
+
+namespace {
+
+template <typename T>
+int balloc(T **p, size_t n) {
+    *p = nullptr;
+    cudaError_t e = cudaMalloc((void **)p, (n ? n : 1) * sizeof(T));
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        return set_error(FPHO_ERR_NOMEM, "cudaMalloc: %s", cudaGetErrorString(e));
+    }
+    return FPHO_OK;
+}
+template <typename T>
+void bfree(T *&p) {
+    if (p) cudaFree((void *)p);
+    p = nullptr;
+}
+
+void destroy_batch(fpho_batch *b) {
+    bfree(b->d_bps); bfree(b->d_expmap); bfree(b->d_args); bfree(b->d_work); bfree(b->d_jobs);
+    bfree(b->d_counter); bfree(b->d_err); bfree(b->d_pairs); bfree(b->d_props);
+    bfree(b->d_chi2); bfree(b->d_dchi2);
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->ev1) cudaEventDestroy(b->ev1);
+    delete b;
+}
+
+}  // namespace
+
+extern "C" int fpho_batch_create(fpho_patch *const *patches, int n, int live_cap, void *stream,
+                                 fpho_batch **out) {
+    clear_error();
+    if (!patches || !out || n < 1) return set_error(FPHO_ERR_INVALID, "bad batch arguments");
+    *out = nullptr;
+    if (live_cap < BT_THREADS || live_cap > 4096)
+        return set_error(FPHO_ERR_INVALID, "live_cap %d outside [%d, 4096]", live_cap, BT_THREADS);
+    // the batched tile kernel is compiled for variant 0 (128 threads x 4 pixels)
+    for (int i = 0; i < n; ++i) {
+        if (!patches[i]) return set_error(FPHO_ERR_INVALID, "patch %d is NULL", i);
+        if (variant_threads(0) != BT_THREADS || variant_tile_pixels(0) != BT_THREADS * BT_K)
+            return set_error(FPHO_ERR_STATE, "variant 0 is not the batched tile shape");
+        int rc = fpho_patch_set_config(patches[i], 0, live_cap, stream);
+        if (rc) return rc;
+    }
+    fpho_batch *b = new (std::nothrow) fpho_batch();
+    if (!b) return set_error(FPHO_ERR_NOMEM, "host allocation failed");
+    b->patches.assign(patches, patches + n);
+    b->live_cap = live_cap;
+    std::vector<BatchPatch> bps(n);
+    std::vector<int2> expmap;
+    std::vector<std::pair<double, int2>> items;
+    std::vector<BandJob> jobs;
+    int rc = FPHO_OK;
+    if (!rc) rc = balloc(&b->d_err, 1);
+    if (!rc) rc = balloc(&b->d_pairs, 1);
+    long long dchi2_off = 0;
+    int src_off = 0, band_off = 0;
+    for (int i = 0; i < n && !rc; ++i) {
+        fpho_patch *p = patches[i];
+        bps[i].pv = make_view(p);
+        bps[i].gtab = p->d_gtab;
+        bps[i].gbox = p->d_gbox;
+        bps[i].prop_off = src_off;
+        for (int e = 0; e < p->n_exp; ++e) {
+            const int ng = p->gauss_start[e + 1] - p->gauss_start[e];
+            if (ng > 0) expmap.push_back(make_int2(i, e));
+            b->max_g = std::max(b->max_g, ng);
+        }
+        TileArgs A;
+        A.pv = bps[i].pv;
+        A.tiles = p->d_tiles;
+        A.tbox_all = p->d_tbox_all;
+        A.tbox_w = p->d_tbox_w;
+        A.gtab = p->d_gtab;
+        A.gbox = p->d_gbox;
+        A.pchi2 = p->d_pchi2;
+        A.pgrad = p->d_pgrad;
+        A.pgrad_stride = 7 * p->n_sources;
+        A.want_residual = 0;
+        A.live_cap = live_cap;
+        A.err = b->d_err;
+        A.pairs = nullptr;
+        b->h_args.push_back(A);
+        b->max_stride = std::max(b->max_stride, 7 * p->n_sources);
+        for (int t = 0; t < p->n_tiles; ++t) {
+            const TileDesc &td = p->h_tiles[t];
+            const int ng = p->gauss_start[td.exposure + 1] - p->gauss_start[td.exposure];
+            items.push_back({(double)td.count * ng, make_int2(i, t)});
+        }
+        for (int bnd = 0; bnd < p->n_bands; ++bnd) {
+            BandJob j;
+            j.t0 = p->tile_band_start[bnd];
+            j.t1 = p->tile_band_start[bnd + 1];
+            j.stride = 7 * p->n_sources;
+            j.chi2_index = band_off + bnd;
+            j.dchi2_off = dchi2_off + (long long)bnd * j.stride;
+            j.pchi2 = p->d_pchi2;
+            j.pgrad = p->d_pgrad;
+            jobs.push_back(j);
+        }
+        src_off += p->n_sources;
+        band_off += p->n_bands;
+        dchi2_off += (long long)p->n_bands * 7 * p->n_sources;
+    }
+    if (!rc && (int)expmap.size() > 65535)
+        rc = set_error(FPHO_ERR_LIMIT, "batch has %zu exposures (max 65535)", expmap.size());
+    // longest tiles first
+    std::stable_sort(items.begin(), items.end(),
+                     [](const std::pair<double, int2> &a, const std::pair<double, int2> &c) {
+                         return a.first > c.first;
+                     });
+    std::vector<int2> work(items.size());
+    for (size_t k = 0; k < items.size(); ++k) work[k] = items[k].second;
+    b->n_work = (int)work.size();
+    b->n_exp_total = (int)expmap.size();
+    b->n_jobs = (int)jobs.size();
+    b->n_src_total = src_off;
+    b->n_band_total = band_off;
+    b->n_dchi2 = dchi2_off;
+    cudaStream_t s = (cudaStream_t)stream;
+    auto up = [&](auto **dst, const auto &vec) -> int {
+        int r = balloc(dst, vec.size());
+        if (r) return r;
+        if (!vec.empty())
+            CUDA_TRY(cudaMemcpyAsync(*dst, vec.data(), vec.size() * sizeof(vec[0]),
+                                     cudaMemcpyHostToDevice, s));
+        return FPHO_OK;
+    };
+    if (!rc) rc = up(&b->d_bps, bps);
+    if (!rc) rc = up(&b->d_expmap, expmap);
+    if (!rc) rc = up(&b->d_args, b->h_args);
+    if (!rc) rc = up(&b->d_work, work);
+    if (!rc) rc = up(&b->d_jobs, jobs);
+    if (!rc) rc = balloc(&b->d_counter, 1);
+    if (!rc && cudaMemsetAsync(b->d_counter, 0, sizeof(int), s) != cudaSuccess)
+        rc = set_error(FPHO_ERR_CUDA, "cudaMemsetAsync failed");
+    if (!rc) {
+        b->smem = tile_smem_bytes(0, live_cap, b->max_stride);
+        if (b->smem > 227 * 1024)
+            rc = set_error(FPHO_ERR_LIMIT, "shared memory %zu exceeds 227 KB", b->smem);
+    }
+    if (!rc) {
+        int dev = 0, sms = 0, per_sm = 0;
+        cudaError_t e = cudaGetDevice(&dev);
+        if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const void *fn = (const void *)batch_tiles<BT_THREADS, BT_K>;
+        if (e == cudaSuccess) {
+            std::lock_guard<std::mutex> lk(g_attr_mu);
+            if (dev < 64 && g_attr_set[dev] < b->smem) {
+                e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)b->smem);
+                if (e == cudaSuccess) g_attr_set[dev] = b->smem;
+            }
+        }
+        if (e == cudaSuccess)
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, BT_THREADS, b->smem);
+        if (e != cudaSuccess)
+            rc = set_error(FPHO_ERR_CUDA, "batch launch setup: %s", cudaGetErrorString(e));
+        else
+            b->grid = std::max(1, std::min(b->n_work, sms * std::max(per_sm, 1)));
+    }
+    if (!rc && cudaStreamSynchronize(s) != cudaSuccess)
+        rc = set_error(FPHO_ERR_CUDA, "cudaStreamSynchronize failed");
+    if (rc) {
+        destroy_batch(b);
+        return rc;
+    }
+    *out = b;
+    return FPHO_OK;
+}
+
+extern "C" int fpho_batch_info(const fpho_batch *b, int64_t out[7]) {
+    clear_error();
+    if (!b || !out) return set_error(FPHO_ERR_INVALID, "NULL argument");
+    out[0] = (int64_t)b->patches.size();
+    out[1] = b->n_src_total;
+    out[2] = b->n_band_total;
+    out[3] = b->n_dchi2;
+    out[4] = b->n_work;
+    out[5] = b->grid;
+    out[6] = b->n_exp_total;
+    return FPHO_OK;
+}
+
+extern "C" int fpho_batch_count_pairs(fpho_batch *b, int enable, long long *last_count) {
+    clear_error();
+    if (!b) return set_error(FPHO_ERR_INVALID, "NULL batch");
+    if (enable != b->count_pairs) {
+        for (auto &A : b->h_args) A.pairs = enable ? b->d_pairs : nullptr;
+        CUDA_TRY(cudaMemcpy(b->d_args, b->h_args.data(), b->h_args.size() * sizeof(TileArgs),
+                            cudaMemcpyHostToDevice));
+        b->count_pairs = enable;
+    }
+    if (last_count) {
+        long long v = 0;
+        CUDA_TRY(cudaMemcpy(&v, b->d_pairs, sizeof(v), cudaMemcpyDeviceToHost));
+        *last_count = v;
+    }
+    return FPHO_OK;
+}
+
+extern "C" int fpho_batch_time_tiles(fpho_batch *b, int enable) {
+    clear_error();
+    if (!b) return set_error(FPHO_ERR_INVALID, "NULL batch");
+    if (enable && !b->ev0) {
+        CUDA_TRY(cudaEventCreate(&b->ev0));
+        CUDA_TRY(cudaEventCreate(&b->ev1));
+    } else if (!enable && b->ev0) {
+        cudaEventDestroy(b->ev0);
+        cudaEventDestroy(b->ev1);
+        b->ev0 = b->ev1 = nullptr;
+    }
+    return FPHO_OK;
+}
+
+extern "C" int fpho_batch_last_tile_ms(fpho_batch *b, float *ms) {
+    clear_error();
+    if (!b || !ms) return set_error(FPHO_ERR_INVALID, "NULL argument");
+    if (!b->ev0) return set_error(FPHO_ERR_STATE, "tile timing is not enabled");
+    CUDA_TRY(cudaEventSynchronize(b->ev1));
+    CUDA_TRY(cudaEventElapsedTime(ms, b->ev0, b->ev1));
+    return FPHO_OK;
+}
+
+static int batch_enqueue(fpho_batch *b, const fpho_source *d_props, double *d_chi2,
+                         float *d_dchi2, cudaStream_t s) {
+    CUDA_TRY(cudaMemsetAsync(b->d_err, 0, sizeof(int), s));
+    if (b->count_pairs) CUDA_TRY(cudaMemsetAsync(b->d_pairs, 0, sizeof(long long), s));
+    if (b->n_exp_total > 0 && b->max_g > 0) {
+        batch_gaussians<<<dim3((b->max_g + 127) / 128, b->n_exp_total), 128, 0, s>>>(
+            b->d_bps, b->d_expmap, d_props);
+        CUDA_TRY(cudaGetLastError());
+    }
+    if (b->ev0) CUDA_TRY(cudaEventRecord(b->ev0, s));
+    if (b->n_work > 0) {
+        batch_tiles<BT_THREADS, BT_K><<<b->grid, BT_THREADS, b->smem, s>>>(b->d_args, b->d_work,
+                                                                          b->n_work, b->d_counter);
+        CUDA_TRY(cudaGetLastError());
+    }
+    if (b->ev1) CUDA_TRY(cudaEventRecord(b->ev1, s));
+    if (b->n_jobs > 0) {
+        batch_reduce<<<dim3(b->n_jobs, (b->max_stride + 127) / 128), 128, 0, s>>>(
+            b->d_jobs, d_chi2, d_dchi2, b->d_counter);
+        CUDA_TRY(cudaGetLastError());
+    }
+    return FPHO_OK;
+}
+
+extern "C" int fpho_batch_evaluate(fpho_batch *b, const fpho_source *proposals, double *chi2,
+                                   float *dchi2, unsigned flags, void *stream) {
+    clear_error();
+    if (!b || !proposals || !chi2 || !dchi2) return set_error(FPHO_ERR_INVALID, "NULL argument");
+    cudaStream_t s = (cudaStream_t)stream;
+    if (!(flags & FPHO_IO_HOST)) return batch_enqueue(b, proposals, chi2, dchi2, s);
+    if (!b->d_props) {
+        int rc;
+        if ((rc = balloc(&b->d_props, (size_t)b->n_src_total))) return rc;
+        if ((rc = balloc(&b->d_chi2, (size_t)b->n_band_total))) return rc;
+        if ((rc = balloc(&b->d_dchi2, (size_t)b->n_dchi2))) return rc;
+    }
+    CUDA_TRY(cudaMemcpyAsync(b->d_props, proposals, sizeof(fpho_source) * b->n_src_total,
+                             cudaMemcpyHostToDevice, s));
+    int rc = batch_enqueue(b, b->d_props, b->d_chi2, b->d_dchi2, s);
+    if (rc) return rc;
+    int err = 0;
+    CUDA_TRY(cudaMemcpyAsync(chi2, b->d_chi2, sizeof(double) * b->n_band_total,
+                             cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaMemcpyAsync(dchi2, b->d_dchi2, sizeof(float) * b->n_dchi2,
+                             cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaMemcpyAsync(&err, b->d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaStreamSynchronize(s));
+    if (err) return set_error(FPHO_ERR_KERNEL, "batched tile kernel reported error word 0x%x", err);
+    return FPHO_OK;
+}
+
+extern "C" int fpho_batch_free(fpho_batch *b) {
+    clear_error();
+    if (b) destroy_batch(b);
+    return FPHO_OK;
+}

@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "fpho_impl.cuh"
+#include "fpho_handle.h"
 #include "fpho_internal.h"
 #include "fpho_kernels.cuh"
 #include "fpho_tile.cuh"
@@ -126,49 +127,7 @@ size_t tile_smem_bytes(int variant, int live_cap, int stride) {
 }  // namespace fpho
 
 // ======================================================================= handle
-struct fpho_patch {
-    // host copies of the index arrays
-    int n_bands = 0, n_exp = 0, n_sources = 0, n_radii = 0;
-    int64_t npix = 0;
-    std::vector<int16_t> band_start, band_N;
-    std::vector<int> exposure_start, exposure_N, n_psf_per_source, psfgauss_start;
-    std::vector<int> exp_band, exp_npsf, gauss_start;
-    int n_gauss = 0;
-    int64_t n_psfrows = 0;
-    bool has_residual = false;
-    // device pixel + index arrays
-    float *d_data = nullptr, *d_ierr = nullptr, *d_xpix = nullptr, *d_ypix = nullptr,
-          *d_residual = nullptr;
-    int *d_exposure_start = nullptr, *d_exposure_N = nullptr;
-    int16_t *d_band_start = nullptr, *d_band_N = nullptr;
-    // device metadata
-    float *d_rad2 = nullptr, *d_D = nullptr, *d_crpix = nullptr, *d_crval = nullptr,
-          *d_CW = nullptr, *d_G = nullptr;
-    int *d_npsf = nullptr, *d_psfgauss_start = nullptr;
-    fpho_psfgauss *d_psfgauss = nullptr;
-    int *d_exp_band = nullptr, *d_exp_npsf = nullptr, *d_gauss_start = nullptr;
-    fpho_patch_struct *d_struct = nullptr;
-    // tile plan
-    int variant = 0, live_cap = 512, n_tiles = 0;
-    std::vector<int> tile_band_start;
-    fpho::TileDesc *d_tiles = nullptr;
-    float4 *d_tbox_all = nullptr, *d_tbox_w = nullptr;
-    int *d_tile_band_start = nullptr;
-    // workspace
-    float *d_gtab = nullptr;
-    float4 *d_gbox = nullptr;
-    double *d_pchi2 = nullptr;
-    float *d_pgrad = nullptr;
-    fpho_source *d_prop = nullptr;
-    double *d_chi2_out = nullptr;
-    float *d_dchi2_out = nullptr;
-    int d_dchi2_cap = 0;
-    int *d_err = nullptr;
-    long long *d_pairs = nullptr;
-    int count_pairs = 0;
-    // optional events recorded around the tile kernel (timing of the dominant kernel)
-    cudaEvent_t ev_tile0 = nullptr, ev_tile1 = nullptr;
-};
+// struct fpho_patch is defined in fpho_handle.h
 
 static void destroy_patch(fpho_patch *p);
 
@@ -384,6 +343,7 @@ int build_plan(fpho_patch *p, cudaStream_t s) {
     }
     p->tile_band_start[p->n_bands] = (int)tiles.size();
     p->n_tiles = (int)tiles.size();
+    p->h_tiles = tiles;
     int rc;
     if ((rc = dupload(&p->d_tiles, tiles.data(), tiles.size(), s))) return rc;
     if ((rc = dupload(&p->d_tile_band_start, p->tile_band_start.data(),

@@ -183,6 +183,37 @@ FPHO_API int fpho_evaluate_proposal(fpho_patch *p, const fpho_source *proposal, 
 FPHO_API int fpho_EvaluateProposal(fpho_patch *p, const void *dev_patch_struct, const void *dev_proposal,
                           void *pchi2, void *pdchi2_dp, void *stream);
 
+/* ---- batched evaluation ------------------------------------------------ */
+
+/* Build a batch of patches evaluated together by one persistent launch (the
+ * reference evaluates one patch per launch, forcepho/proposal.py:133-136, one
+ * patch per MPI child, forcepho/dispatcher.py).  Every patch is switched to
+ * the batched tile shape (variant 0) with `live_cap`; rebuild the batch after
+ * fpho_patch_replace_meta or fpho_patch_set_config on a member.  The patch
+ * handles must outlive the batch. */
+FPHO_API int fpho_batch_create(fpho_patch *const *patches, int n, int live_cap, void *stream,
+                               fpho_batch **out);
+
+/* out[0] patches, out[1] total sources, out[2] total bands, out[3] total dchi2
+ * floats, out[4] work items (tiles), out[5] persistent grid, out[6] exposures. */
+FPHO_API int fpho_batch_info(const fpho_batch *b, int64_t out[7]);
+
+/* Evaluate one proposal per patch.
+ *   proposals  fpho_source[sum n_sources], patch i's sources after patch i-1's
+ *   chi2       double[sum n_bands], patch by patch
+ *   dchi2      float[sum n_bands * n_sources * 7], patch by patch, each
+ *              [n_bands][n_sources][7]
+ *   flags      FPHO_IO_HOST (host buffers; the call synchronizes)
+ * A batch is used by one stream at a time. */
+FPHO_API int fpho_batch_evaluate(fpho_batch *b, const fpho_source *proposals, double *chi2,
+                                 float *dchi2, unsigned flags, void *stream);
+
+/* As the patch versions: evaluated-pair counting and timing of the tile kernel. */
+FPHO_API int fpho_batch_count_pairs(fpho_batch *b, int enable, long long *last_count);
+FPHO_API int fpho_batch_time_tiles(fpho_batch *b, int enable);
+FPHO_API int fpho_batch_last_tile_ms(fpho_batch *b, float *ms);
+FPHO_API int fpho_batch_free(fpho_batch *b);
+
 /* ---- evaluation without allocation (no counterpart in the reference) ---- */
 
 /* Size of the device array that holds all scratch of
