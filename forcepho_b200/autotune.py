@@ -21,7 +21,7 @@ CACHE = os.environ.get("FPHO_AUTOTUNE_CACHE",
                        os.path.join(os.path.expanduser("~"), ".cache", "forcepho_b200",
                                     "autotune.json"))
 DEFAULT = {"variant": 0, "live_cap": 512}
-LIVE_CAPS = (256, 512, 1024)
+LIVE_CAPS = (128, 256, 512)
 
 
 def signature(patch):
@@ -88,8 +88,7 @@ def tune(patch, proposal=None, candidates=None):
         candidates = []
         for v, (nt, k) in enumerate(_lib.variants()):
             for lc in LIVE_CAPS:
-                if lc >= nt:
-                    candidates.append((v, lc))
+                candidates.append((v, lc))
     res = {}
     for v, lc in candidates:
         try:

@@ -29,7 +29,7 @@ class PatchBatch:
     live_cap : image-Gaussian records per shared-memory stage
     """
 
-    def __init__(self, patches, live_cap=256, stream=None):
+    def __init__(self, patches, live_cap=128, stream=None):
         self.patches = list(patches)
         handles = (ctypes.c_void_p * len(self.patches))(
             *[p.device_patch.handle for p in self.patches])

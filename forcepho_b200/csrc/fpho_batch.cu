@@ -28,8 +28,16 @@
 namespace fpho {
 namespace {
 
-constexpr int BT_THREADS = 128;
-constexpr int BT_K = 4;
+constexpr int BT_THREADS = 64;  // the batched tile shape: 64 threads x 8 pixels
+constexpr int BT_K = 8;
+
+// index of the batched tile shape among the compiled variants
+int batched_variant() {
+    for (int v = 0; v < variant_count(); ++v)
+        if (variant_threads(v) == BT_THREADS && variant_tile_pixels(v) == BT_THREADS * BT_K)
+            return v;
+    return -1;
+}
 
 struct BatchPatch {
     PatchView pv;
@@ -178,14 +186,14 @@ extern "C" int fpho_batch_create(fpho_patch *const *patches, int n, int live_cap
     clear_error();
     if (!patches || !out || n < 1) return set_error(FPHO_ERR_INVALID, "bad batch arguments");
     *out = nullptr;
-    if (live_cap < BT_THREADS || live_cap > 4096)
-        return set_error(FPHO_ERR_INVALID, "live_cap %d outside [%d, 4096]", live_cap, BT_THREADS);
-    // the batched tile kernel is compiled for variant 0 (128 threads x 4 pixels)
+    if (live_cap < 32 || live_cap > 4096)
+        return set_error(FPHO_ERR_INVALID, "live_cap %d outside [32, 4096]", live_cap);
+    // the batched tile kernel is compiled for one tile shape (64 threads x 8 pixels)
     for (int i = 0; i < n; ++i) {
         if (!patches[i]) return set_error(FPHO_ERR_INVALID, "patch %d is NULL", i);
-        if (variant_threads(0) != BT_THREADS || variant_tile_pixels(0) != BT_THREADS * BT_K)
-            return set_error(FPHO_ERR_STATE, "variant 0 is not the batched tile shape");
-        int rc = fpho_patch_set_config(patches[i], 0, live_cap, stream);
+        if (batched_variant() < 0)
+            return set_error(FPHO_ERR_STATE, "the batched tile shape is not compiled");
+        int rc = fpho_patch_set_config(patches[i], batched_variant(), live_cap, stream);
         if (rc) return rc;
     }
     fpho_batch *b = new (std::nothrow) fpho_batch();
@@ -224,6 +232,7 @@ extern "C" int fpho_batch_create(fpho_patch *const *patches, int n, int live_cap
         A.pgrad_stride = 7 * p->n_sources;
         A.want_residual = 0;
         A.live_cap = live_cap;
+        A.idx_cap = std::max(p->max_g, 1);
         A.err = b->d_err;
         A.pairs = nullptr;
         b->h_args.push_back(A);
@@ -281,7 +290,8 @@ extern "C" int fpho_batch_create(fpho_patch *const *patches, int n, int live_cap
     if (!rc && cudaMemsetAsync(b->d_counter, 0, sizeof(int), s) != cudaSuccess)
         rc = set_error(FPHO_ERR_CUDA, "cudaMemsetAsync failed");
     if (!rc) {
-        b->smem = tile_smem_bytes(0, live_cap, b->max_stride);
+        b->smem = tile_smem_bytes(batched_variant(), live_cap, std::max(b->max_g, 1),
+                                  b->max_stride);
         if (b->smem > 227 * 1024)
             rc = set_error(FPHO_ERR_LIMIT, "shared memory %zu exceeds 227 KB", b->smem);
     }

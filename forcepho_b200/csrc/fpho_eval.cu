@@ -90,6 +90,7 @@ static const Variant kVariants[] = {
     {64, 4, (const void *)tile_kernel<64, 4>},
     {256, 4, (const void *)tile_kernel<256, 4>},
     {128, 8, (const void *)tile_kernel<128, 8>},
+    {64, 8, (const void *)tile_kernel<64, 8>},
 };
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
@@ -103,7 +104,7 @@ static size_t g_attr_set[64][kNumVariants];  // per device, per variant
 int launch_tile_kernel(int variant, const TileArgs &A, int n_tiles, cudaStream_t stream) {
     if (n_tiles <= 0) return FPHO_OK;
     const Variant &V = kVariants[variant];
-    const size_t smem = tile_smem_bytes(variant, A.live_cap, A.pgrad_stride);
+    const size_t smem = tile_smem_bytes(variant, A.live_cap, A.idx_cap, A.pgrad_stride);
     int dev = 0;
     CUDA_TRY(cudaGetDevice(&dev));
     {
@@ -119,9 +120,8 @@ int launch_tile_kernel(int variant, const TileArgs &A, int n_tiles, cudaStream_t
     return FPHO_OK;
 }
 
-size_t tile_smem_bytes(int variant, int live_cap, int stride) {
-    return (size_t)live_cap * GREC * 4 + (size_t)live_cap * 8 +
-           (size_t)(kVariants[variant].nt / 32) * stride * 4;
+size_t tile_smem_bytes(int variant, int live_cap, int idx_cap, int stride) {
+    return tile_smem_layout_bytes(kVariants[variant].nt / 32, live_cap, idx_cap, stride);
 }
 
 }  // namespace fpho
@@ -253,6 +253,15 @@ int upload_meta(fpho_patch *p, const fpho_patch_struct *h, cudaStream_t s,
                                  "psfgauss[%d].sersic_radius_bin=%d outside [0, n_radii=%d)",
                                  pstart[e] + q, k, nrad);
         }
+    {
+        int mg = 0;
+        for (int e = 0; e < ne; ++e) mg = std::max(mg, gstart[e + 1] - gstart[e]);
+        const size_t need = tile_smem_bytes(p->variant, p->live_cap, std::max(mg, 1), 7 * nsrc);
+        if (need > 227 * 1024)
+            return set_error(FPHO_ERR_LIMIT,
+                             "%d image Gaussians per exposure and %d sources need %zu bytes of "
+                             "shared memory (max 227 KB)", mg, nsrc, need);
+    }
     if (validate_only) return FPHO_OK;
     free_meta(p);
     p->n_sources = nsrc;
@@ -262,6 +271,8 @@ int upload_meta(fpho_patch *p, const fpho_patch_struct *h, cudaStream_t s,
     p->exp_npsf = exp_npsf;
     p->gauss_start = gstart;
     p->n_gauss = (int)ng;
+    p->max_g = 0;
+    for (int e = 0; e < ne; ++e) p->max_g = std::max(p->max_g, gstart[e + 1] - gstart[e]);
     p->n_psfrows = nrows;
     const size_t es = (size_t)ne * nsrc;
     int rc;
@@ -491,9 +502,10 @@ extern "C" int fpho_patch_set_config(fpho_patch *p, int variant, int live_cap, v
     if (variant < 0 || variant >= variant_count())
         return set_error(FPHO_ERR_INVALID, "variant %d not in [0, %d)", variant, variant_count());
     const int nt = variant_threads(variant);
-    if (live_cap < nt || live_cap > 4096)
-        return set_error(FPHO_ERR_INVALID, "live_cap %d outside [%d, 4096]", live_cap, nt);
-    if (tile_smem_bytes(variant, live_cap, 7 * p->n_sources) > 227 * 1024)
+    (void)nt;
+    if (live_cap < 32 || live_cap > 4096)
+        return set_error(FPHO_ERR_INVALID, "live_cap %d outside [32, 4096]", live_cap);
+    if (tile_smem_bytes(variant, live_cap, p->max_g, 7 * p->n_sources) > 227 * 1024)
         return set_error(FPHO_ERR_LIMIT, "shared memory for live_cap %d exceeds 227 KB",
                          live_cap);
     const bool replan = variant_tile_pixels(variant) != variant_tile_pixels(p->variant);
@@ -535,9 +547,7 @@ int enqueue_evaluate(fpho_patch *p, const fpho_source *d_prop, double *d_chi2, f
     CUDA_TRY(cudaMemsetAsync(p->d_err, 0, sizeof(int), s));
     if (p->count_pairs) CUDA_TRY(cudaMemsetAsync(p->d_pairs, 0, sizeof(long long), s));
     const PatchView pv = make_view(p);
-    int max_g = 0;
-    for (int e = 0; e < p->n_exp; ++e)
-        max_g = std::max(max_g, p->gauss_start[e + 1] - p->gauss_start[e]);
+    const int max_g = p->max_g;
     if (max_g > 0) {
         dim3 grid((max_g + 127) / 128, p->n_exp);
         build_image_gaussians<<<grid, 128, 0, s>>>(pv, d_prop, p->d_gtab, p->d_gbox);
@@ -555,6 +565,7 @@ int enqueue_evaluate(fpho_patch *p, const fpho_source *d_prop, double *d_chi2, f
     A.pgrad_stride = 7 * p->n_sources;
     A.want_residual = want_residual ? 1 : 0;
     A.live_cap = p->live_cap;
+    A.idx_cap = std::max(p->max_g, 1);
     A.err = p->d_err;
     A.pairs = p->count_pairs ? p->d_pairs : nullptr;
     if (p->ev_tile0) CUDA_TRY(cudaEventRecord(p->ev_tile0, s));

@@ -17,6 +17,7 @@ struct fpho_patch {
     std::vector<int> exposure_start, exposure_N, n_psf_per_source, psfgauss_start;
     std::vector<int> exp_band, exp_npsf, gauss_start;
     int n_gauss = 0;
+    int max_g = 0;  // most image Gaussians of any exposure
     int64_t n_psfrows = 0;
     bool has_residual = false;
     // device pixel + index arrays

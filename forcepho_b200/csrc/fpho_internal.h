@@ -21,7 +21,7 @@ void clear_error();
 int variant_count();
 int variant_tile_pixels(int v);
 int variant_threads(int v);
-size_t tile_smem_bytes(int variant, int live_cap, int stride);
+size_t tile_smem_bytes(int variant, int live_cap, int idx_cap, int stride);
 int launch_tile_kernel(int variant, const TileArgs &A, int n_tiles, cudaStream_t stream);
 
 PatchView make_view(const fpho_patch *p);

@@ -253,8 +253,11 @@ extern "C" int fpho_evaluate_proposal_noalloc(const fpho_patch_struct *patch, in
                          "the no-allocation entry point has %u",
                          L.total, n_tiles_max, n_gauss_max, (unsigned)FPHO_NOALLOC_SCRATCH_BYTES);
     const int stride = 7 * nsrc;
-    const size_t smem = (size_t)NA_LIVE_CAP * GREC * 4 + (size_t)NA_LIVE_CAP * 8 +
-                        (size_t)(NA_THREADS / 32) * stride * 4;
+    const int idx_cap = nsrc * max_psf_per_source;
+    const size_t smem = tile_smem_layout_bytes(NA_THREADS / 32, NA_LIVE_CAP, idx_cap, stride);
+    if (smem > 227 * 1024)
+        return set_error(FPHO_ERR_LIMIT, "shared memory %zu for %d image Gaussians per exposure "
+                         "exceeds 227 KB", smem, idx_cap);
 
     // once per device (the device current for this call): the array's device
     // address and the tile kernel's dynamic shared-memory limit
@@ -324,6 +327,7 @@ extern "C" int fpho_evaluate_proposal_noalloc(const fpho_patch_struct *patch, in
     A.pgrad_stride = stride;
     A.want_residual = h.residual != nullptr;
     A.live_cap = NA_LIVE_CAP;
+    A.idx_cap = idx_cap;
     A.err = &hdr->err;
     A.pairs = nullptr;
     noalloc_tiles<<<(unsigned)n_tiles_max, NA_THREADS, smem, s>>>(A, hdr);

@@ -37,7 +37,8 @@ struct TileArgs {
     float *pgrad;             // [n_tiles][pgrad_stride] gradient partial per tile
     int pgrad_stride;         // 7 * n_sources
     int want_residual;
-    int live_cap;             // records that fit in the shared-memory stage (>= NT)
+    int live_cap;             // records that fit in the shared-memory stage (>= 1)
+    int idx_cap;              // most image Gaussians of any exposure (kept-list capacity)
     int *err;                 // error word (bit 0: bulk-copy wait gave up)
     long long *pairs;         // optional: evaluated (pixel, Gaussian) pairs, or nullptr
 };
@@ -131,15 +132,50 @@ __device__ __forceinline__ int reduce7_index(int lane) {
 }
 
 // ------------------------------------------------------------ shared layout
-template <int NT>
-struct TileSmem {
-    static constexpr int NW = NT / 32;
-    // dynamic shared memory: [recs live_cap*128 B][live_idx live_cap*4][live_flag live_cap*4]
-    //                        [wacc NW*stride*4]
-    static __host__ __device__ size_t bytes(int live_cap, int stride) {
-        return (size_t)live_cap * GREC * 4 + (size_t)live_cap * 8 + (size_t)NW * stride * 4;
+// Dynamic shared memory of the tile kernel:
+//   [records live_cap x 128 B][kept indices idx_cap x 4 B][kept flags idx_cap x 4 B]
+//   [per-warp source sums NW x stride x 4 B]
+__host__ __device__ inline size_t tile_smem_layout_bytes(int nw, int live_cap, int idx_cap,
+                                                         int stride) {
+    return (size_t)live_cap * GREC * 4 + (size_t)idx_cap * 8 + (size_t)nw * stride * 4;
+}
+
+// ------------------------------------------------------------ culling
+// Minimum over the rectangle [x0,x1] x [y0,y1] of the exp-argument
+// q(p) = (p-c)^T F (p-c): 0 if the centre is inside, else the smallest of the
+// four edge minima (q is convex, so its minimum over the rectangle lies on the
+// boundary; on an edge it is a clamped 1-D quadratic minimum).
+__device__ __forceinline__ float rect_min_q(float4 bb, float xc, float yc, float fxx, float fxy,
+                                            float fyy) {
+    if (xc >= bb.x && xc <= bb.y && yc >= bb.z && yc <= bb.w) return 0.0f;
+    float best = INFINITY;
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+        const float dx = (e ? bb.y : bb.x) - xc;
+        const float dy = fminf(fmaxf(-fxy * dx / fyy, bb.z - yc), bb.w - yc);
+        best = fminf(best, dx * (fxx * dx + fxy * dy) + dy * (fyy * dy + fxy * dx));
     }
-};
+#pragma unroll
+    for (int e = 0; e < 2; ++e) {
+        const float dy = (e ? bb.w : bb.z) - yc;
+        const float dx = fminf(fmaxf(-fxy * dy / fxx, bb.x - xc), bb.y - xc);
+        best = fminf(best, dx * (fxx * dx + fxy * dy) + dy * (fyy * dy + fxy * dx));
+    }
+    return best;
+}
+
+// Is image Gaussian `rec` (in global memory) possibly within exp-argument 36
+// of some point of the tile box?  Conservative: cull only when the exact
+// minimum, less a 2e-3 relative + 2e-3 margin for float rounding, exceeds 36.
+__device__ __forceinline__ bool keeps_tile(const float *rec, float4 bb) {
+    const float4 a = *reinterpret_cast<const float4 *>(rec);      // -xc -xc -yc -yc
+    const float4 b = *reinterpret_cast<const float4 *>(rec + 4);  // fxx fxx fxy fxy
+    const float fyy = rec[R_FYY];
+    const float fxx = b.x, fxy = b.z;
+    if (!(fxx > 0.0f && fyy > 0.0f)) return true;
+    const float q = rect_min_q(bb, -a.x, -a.z, fxx, fxy, fyy);
+    return !(q * (1.0f - 2.0e-3f) - 2.0e-3f > FPHO_MAX_EXP_ARG);
+}
 
 // ------------------------------------------------------------ per-Gaussian helpers
 // Two packed operands from one 16-byte shared-memory load.
@@ -243,8 +279,8 @@ __device__ __forceinline__ void tile_body(const TileArgs &A, int tile, unsigned 
 
     float *recs = reinterpret_cast<float *>(smem);
     int *live_idx = reinterpret_cast<int *>(smem + (size_t)cap * GREC * 4);
-    int *live_flag = live_idx + cap;
-    float *wacc = reinterpret_cast<float *>(live_flag + cap);
+    int *live_flag = live_idx + A.idx_cap;
+    float *wacc = reinterpret_cast<float *>(live_flag + A.idx_cap);
 
     __shared__ int s_cnt[NW];
     __shared__ double s_chi2[NW];
@@ -254,6 +290,7 @@ __device__ __forceinline__ void tile_body(const TileArgs &A, int tile, unsigned 
     const float4 bb = A.want_residual ? A.tbox_all[tile] : A.tbox_w[tile];
     const int g0 = A.pv.gauss_start[td.exposure];
     const int g1 = A.pv.gauss_start[td.exposure + 1];
+    const int npsf = A.pv.exp_npsf[td.exposure];
 
     for (int j = tid; j < NW * stride; j += NT) wacc[j] = 0.0f;
 
@@ -281,103 +318,96 @@ __device__ __forceinline__ void tile_body(const TileArgs &A, int tile, unsigned 
         R[j] = pk(D[2 * j], D[2 * j + 1]);
     }
     if (tid == 0) s_any_weight = 0;
-    __syncthreads();
+
+    // ---- scan once: the ordered list of the exposure's image Gaussians that
+    // can reach the tile (box overlap, then the exact minimum of the
+    // exp-argument over the tile), with a flag when the exp-argument can
+    // exceed 36 inside the tile (its maximum over the box is at a corner).
+    int n_live = 0;
+    for (int base = g0; base < g1; base += NT) {
+        const int idx = base + tid;
+        bool live = false;
+        int flag = 0;
+        if (idx < g1) {
+            const float4 gb = A.gbox[idx];
+            live = !(gb.y < bb.x || gb.x > bb.y || gb.w < bb.z || gb.z > bb.w);
+            if (live) {
+                const float *r = A.gtab + (size_t)idx * GREC;
+                live = keeps_tile(r, bb);
+                const float nxc = r[R_NXC], nyc = r[R_NYC];
+                const float fxx = r[R_FXX], fxy = r[R_FXY], fyy = r[R_FYY];
+                float qmax = 0.0f;
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    const float dx = ((c & 1) ? bb.y : bb.x) + nxc;
+                    const float dy = ((c & 2) ? bb.w : bb.z) + nyc;
+                    qmax = fmaxf(qmax, dx * (fxx * dx + fxy * dy) + dy * (fyy * dy + fxy * dx));
+                }
+                flag = (qmax * (1.0f + CULL_REL) + CULL_ABS >= FPHO_MAX_EXP_ARG) ? FLAG_CUT : 0;
+            }
+        }
+        const unsigned ball = __ballot_sync(0xffffffffu, live);
+        if (lane == 0) s_cnt[warp] = __popc(ball);
+        __syncthreads();
+        int off = 0, tot = 0;
+#pragma unroll
+        for (int w = 0; w < NW; ++w) {
+            off += (w < warp) ? s_cnt[w] : 0;
+            tot += s_cnt[w];
+        }
+        if (live) {
+            const int at = n_live + off + __popc(ball & ((1u << lane) - 1u));
+            live_idx[at] = idx;
+            live_flag[at] = flag;
+        }
+        n_live += tot;
+        __syncthreads();
+    }
+    // last kept Gaussian of each source (sources are contiguous in the list)
+    for (int i = tid; i < n_live; i += NT) {
+        const int src = (live_idx[i] - g0) / npsf;
+        const int nxt = (i + 1 < n_live) ? (live_idx[i + 1] - g0) / npsf : -1;
+        if (nxt != src) live_flag[i] |= FLAG_LAST_SRC;
+    }
     if (any_w) s_any_weight = 1;
     __syncthreads();
     const bool tile_has_weight = s_any_weight != 0;
 
-    const v2 KEXP2 = pk1(KEXP), KEXPLO2 = pk1(KEXP_LO);
-    const v2 CM24 = pk1(-1.0f / 24.0f), C24 = pk1(1.0f / 24.0f);
-    long long npairs = 0;
-
-    // ---- chunked scan + stage: keeps the exposure's Gaussians whose culling
-    // box overlaps the tile, in order, up to `cap` per chunk; `cursor` advances
-    // through [g0, g1).  Returns the number of staged records.
-    auto scan_and_stage = [&](int &cursor) -> int {
-        int n = 0;
-        while (cursor < g1 && n + NT <= cap) {
-            const int idx = cursor + tid;
-            bool live = false;
-            if (idx < g1) {
-                const float4 gb = A.gbox[idx];
-                live = !(gb.y < bb.x || gb.x > bb.y || gb.w < bb.z || gb.z > bb.w);
-            }
-            const unsigned ball = __ballot_sync(0xffffffffu, live);
-            if (lane == 0) s_cnt[warp] = __popc(ball);
-            __syncthreads();
-            int off = 0, tot = 0;
-#pragma unroll
-            for (int w = 0; w < NW; ++w) {
-                off += (w < warp) ? s_cnt[w] : 0;
-                tot += s_cnt[w];
-            }
-            if (live) live_idx[n + off + __popc(ball & ((1u << lane) - 1u))] = idx;
-            n += tot;
-            cursor += NT;
-            __syncthreads();
-        }
-        // stage records with bulk copies issued by warp 0
+    // ---- stage kept records [c0, c0 + n) into shared memory with bulk copies
+    auto stage = [&](int c0, int n) {
         fence_proxy_async_smem();
         if (warp == 0) {
             if (lane == 0) mbar_arrive_expect_tx(mbar, (uint32_t)n * GREC * 4);
             __syncwarp();
             for (int i = lane; i < n; i += 32)
-                bulk_g2s(recs + (size_t)i * GREC, A.gtab + (size_t)live_idx[i] * GREC, GREC * 4,
-                         mbar);
+                bulk_g2s(recs + (size_t)i * GREC, A.gtab + (size_t)live_idx[c0 + i] * GREC,
+                         GREC * 4, mbar);
         }
         mbar_wait_bounded(mbar, phase, A.err);
         phase ^= 1u;
-        // per kept Gaussian: can the exp-argument cross 36 inside the tile (its
-        // maximum over the box is at a corner), and is it its source's last?
-        for (int i = tid; i < n; i += NT) {
-            const float *r = recs + (size_t)i * GREC;
-            const float nxc = r[R_NXC], nyc = r[R_NYC];
-            const float fxx = r[R_FXX], fxy = r[R_FXY], fyy = r[R_FYY];
-            float qmax = 0.0f;
-#pragma unroll
-            for (int c = 0; c < 4; ++c) {
-                const float dx = ((c & 1) ? bb.y : bb.x) + nxc;
-                const float dy = ((c & 2) ? bb.w : bb.z) + nyc;
-                const float q = dx * (fxx * dx + fxy * dy) + dy * (fyy * dy + fxy * dx);
-                qmax = fmaxf(qmax, q);
-            }
-            const int src = __float_as_int(r[R_SRC]);
-            const int nxt = (i + 1 < n) ? __float_as_int(recs[(size_t)(i + 1) * GREC + R_SRC]) : -1;
-            live_flag[i] = ((qmax * (1.0f + CULL_REL) + CULL_ABS >= FPHO_MAX_EXP_ARG) ? FLAG_CUT : 0) |
-                           ((nxt != src) ? FLAG_LAST_SRC : 0);
-        }
-        __syncthreads();
-        return n;
     };
 
+    const v2 KEXP2 = pk1(KEXP), KEXPLO2 = pk1(KEXP_LO);
+    const v2 CM24 = pk1(-1.0f / 24.0f), C24 = pk1(1.0f / 24.0f);
+    const int n_chunks = (n_live + cap - 1) / cap;
+
     // ------------------------------------------------------------ pass 1
-    // npairs counts the records staged over all pass-1 chunks; if that equals
-    // the last chunk's size, the whole kept set is still resident for pass 2.
-    int cursor = g0;
-    int n_last = 0;
-    {
-        bool first = true;
-        while (cursor < g1 || first) {
-            if (!first) __syncthreads();  // previous chunk fully consumed
-            first = false;
-            const int n = scan_and_stage(cursor);
-            n_last = n;
-            npairs += (long long)n;
-            for (int i = 0; i < n; ++i) {
-                const float *r = recs + (size_t)i * GREC;
-                v2 NXC, NYC, FXX, FXY, FYY, AMP, HB, C0;
-                ld2(r + R_NXC, NXC, NYC);
-                ld2(r + R_FXX, FXX, FXY);
-                ld2(r + R_FYY, FYY, AMP);
-                ld2(r + R_HB, HB, C0);
-                const v2 HA = mul2(AMP, CM24);
-                if (live_flag[i] & FLAG_CUT)
-                    residual_pairs<KP, true>(X, Y, R, NXC, NYC, FXX, FXY, FYY, HA, HB, KEXP2,
-                                             KEXPLO2);
-                else
-                    residual_pairs<KP, false>(X, Y, R, NXC, NYC, FXX, FXY, FYY, HA, HB, KEXP2,
-                                              KEXPLO2);
-            }
+    for (int c = 0; c < n_chunks; ++c) {
+        const int c0 = c * cap, n = min(cap, n_live - c0);
+        if (c > 0) __syncthreads();  // previous chunk fully consumed
+        stage(c0, n);
+        for (int i = 0; i < n; ++i) {
+            const float *r = recs + (size_t)i * GREC;
+            v2 NXC, NYC, FXX, FXY, FYY, AMP, HB, C0;
+            ld2(r + R_NXC, NXC, NYC);
+            ld2(r + R_FXX, FXX, FXY);
+            ld2(r + R_FYY, FYY, AMP);
+            ld2(r + R_HB, HB, C0);
+            const v2 HA = mul2(AMP, CM24);
+            if (live_flag[c0 + i] & FLAG_CUT)
+                residual_pairs<KP, true>(X, Y, R, NXC, NYC, FXX, FXY, FYY, HA, HB, KEXP2, KEXPLO2);
+            else
+                residual_pairs<KP, false>(X, Y, R, NXC, NYC, FXX, FXY, FYY, HA, HB, KEXP2, KEXPLO2);
         }
     }
 
@@ -407,22 +437,15 @@ __device__ __forceinline__ void tile_body(const TileArgs &A, int tile, unsigned 
     if (lane == 0) s_chi2[warp] = chi2;
 
     // ------------------------------------------------------------ pass 2
+    // Chunks in reverse order: the last chunk of pass 1 is still staged.
     if (tile_has_weight) {
-        // re-use the staged chunk if the kept set fit in one, otherwise rescan
-        int cursor2 = g0;
-        bool first = true;
-        const bool reuse = (npairs == (long long)n_last);
         float P[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-        while (first || cursor2 < g1) {
-            int n;
-            if (first && reuse) {
-                n = n_last;
-                cursor2 = g1;
-            } else {
+        for (int c = n_chunks - 1; c >= 0; --c) {
+            const int c0 = c * cap, n = min(cap, n_live - c0);
+            if (c != n_chunks - 1) {
                 __syncthreads();
-                n = scan_and_stage(cursor2);
+                stage(c0, n);
             }
-            first = false;
             for (int i = 0; i < n; ++i) {
                 const float *r = recs + (size_t)i * GREC;
                 v2 NXC, NYC, FXX, FXY, FYY, AMP, HB, C0;
@@ -430,7 +453,7 @@ __device__ __forceinline__ void tile_body(const TileArgs &A, int tile, unsigned 
                 ld2(r + R_FXX, FXX, FXY);
                 ld2(r + R_FYY, FYY, AMP);
                 ld2(r + R_HB, HB, C0);
-                const int flag = live_flag[i];
+                const int flag = live_flag[c0 + i];
                 GradSums s;
                 if (flag & FLAG_CUT)
                     gradient_pairs<KP, true>(X, Y, R2, NXC, NYC, FXX, FXY, FYY, C0, C24, KEXP2, s);
@@ -460,7 +483,7 @@ __device__ __forceinline__ void tile_body(const TileArgs &A, int tile, unsigned 
                 P[5] = fmaf(j0.w, gA, P[5]);
                 P[6] = fmaf(j1.x, gA, P[6]);
                 // flush at a source boundary or at the end of the chunk
-                if (flag & FLAG_LAST_SRC) {
+                if ((flag & FLAG_LAST_SRC) || i == n - 1) {
                     const int src = __float_as_int(j3.w);
                     float v[8] = {P[0], P[1], P[2], P[3], P[4], P[5], P[6], 0.0f};
 #pragma unroll
@@ -488,7 +511,7 @@ __device__ __forceinline__ void tile_body(const TileArgs &A, int tile, unsigned 
         A.pgrad[(size_t)tile * stride + j] = v;
     }
     if (A.pairs && tid == 0) atomicAdd(reinterpret_cast<unsigned long long *>(A.pairs),
-                                       (unsigned long long)(npairs * (long long)td.count));
+                                       (unsigned long long)((long long)n_live * td.count));
 }
 
 }  // namespace fpho

@@ -188,7 +188,7 @@ FPHO_API int fpho_EvaluateProposal(fpho_patch *p, const void *dev_patch_struct, 
 /* Build a batch of patches evaluated together by one persistent launch (the
  * reference evaluates one patch per launch, forcepho/proposal.py:133-136, one
  * patch per MPI child, forcepho/dispatcher.py).  Every patch is switched to
- * the batched tile shape (variant 0) with `live_cap`; rebuild the batch after
+ * the batched tile shape (64 threads x 8 pixels) with `live_cap`; rebuild the batch after
  * fpho_patch_replace_meta or fpho_patch_set_config on a member.  The patch
  * handles must outlive the batch. */
 FPHO_API int fpho_batch_create(fpho_patch *const *patches, int n, int live_cap, void *stream,

@@ -100,7 +100,7 @@ def test_residual_matches_oracle():
     assert np.max(np.abs(res - r)) <= 1e-5 * scale
 
 
-@pytest.mark.parametrize("variant", range(6))
+@pytest.mark.parametrize("variant", range(8))
 def test_variants_agree(variant):
     from forcepho_b200 import _lib
     if variant >= len(_lib.variants()):
