@@ -56,6 +56,8 @@ def parse():
     ap.add_argument("--live-cap", type=int, default=None)
     ap.add_argument("--batch-patches", type=int, default=256,
                     help="patches of the batched leg (config 3); 0 skips it")
+    ap.add_argument("--no-differentiable", action="store_true",
+                    help="skip the differentiable-form leg (config 2)")
     return ap.parse_args()
 
 
@@ -261,9 +263,122 @@ def batched_leg(args, torch, lib, steps):
            "timing": "CUDA events per step, L2 flushed between steps; batched step replayed "
                      "from a CUDA graph"}
     del graph
+
+    # the batched differentiable form: device-side proposals (splines) and
+    # bounded transform for all patches, one batched evaluation, gradient
+    # stacking and the leapfrog update, one step per graph replay
+    from forcepho_b200.autograd import BatchPosterior, Leapfrog, default_bounds
+    lows, highs = zip(*[default_bounds(P.params, P.n_bands) for P in patches])
+    bp = BatchPosterior(batch, lows, highs)
+    lf = Leapfrog(bp, eps=1e-3, steps_per_graph=1)
+    z0 = bp.inverse_transform(np.concatenate([P.params.reshape(-1) for P in patches]))
+    p0 = torch.as_tensor(np.random.default_rng(1).standard_normal(bp.ndim), device="cuda")
+    lf.set_state(z0, p0)
+    lf.run(3)
+    ms_leap = timed(lf.graph.replay, steps)
+
+    # the plain drop-in: FastPosterior.lnprob_and_grad per patch (host proposal
+    # from the scipy splines, one GPUProposer call per patch, host I/O)
+    from forcepho_b200.model import FastPosterior
+    from forcepho_b200.proposal import GPUProposer
+    from forcepho_b200.sources import Scene
+    fps = [FastPosterior(GPUProposer(), P, scene=Scene(P.n_sources, P.n_bands, P.table),
+                         lower=lo, upper=hi) for P, lo, hi in zip(patches, lows, highs)]
+    zs = [f.transform.inverse_transform(P.params.reshape(-1)) for f, P in zip(fps, patches)]
+    rng = np.random.default_rng(7)
+
+    def dropin():
+        for f, z in zip(fps, zs):
+            f.lnprob_and_grad(z + 1e-6 * rng.standard_normal(z.shape))
+
+    dropin()
+    reps = 2
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        dropin()
+    ms_dropin = (time.perf_counter() - t0) / reps * 1e3
+    out.update({
+        "batched_leapfrog_ms_per_step": ms_leap,
+        "batched_leapfrog_patch_evals_per_s": n / (ms_leap * 1e-3),
+        "dropin_ms_per_step": ms_dropin,
+        "dropin_patch_evals_per_s": n / (ms_dropin * 1e-3),
+        "speedup_batched_differentiable_vs_dropin": ms_dropin / ms_leap,
+        "dropin": "FastPosterior.lnprob_and_grad per patch: host Scene proposal (scipy "
+                  "splines), GPUProposer.evaluate_proposal with host I/O; host wall clock",
+    })
+    del lf
     batch.free()
     for P in patches:
         P.free()
+    return out
+
+
+def differentiable_leg(args, torch, P, cfg, steps):
+    """Config 2: the config-1 patch through the autograd Function and the
+    device posterior, HMC leapfrog steps of 1e-3 in the unconstrained
+    coordinates replayed from a CUDA graph, against the plain drop-in
+    (FastPosterior.lnprob_and_grad with host proposals and host I/O)."""
+    from forcepho_b200.autograd import DevicePosterior, Leapfrog, default_bounds
+    from forcepho_b200.model import FastPosterior
+    from forcepho_b200.proposal import GPUProposer
+    from forcepho_b200.sources import Scene
+    s = torch.cuda.current_stream()
+    lo, hi = default_bounds(P.params, P.n_bands)
+    post = DevicePosterior(P, lo, hi)
+    z0 = post.inverse_transform(P.params.reshape(-1))
+    p0 = torch.as_tensor(np.random.default_rng(2).standard_normal(post.ndim), device="cuda")
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    # one step per replay, L2 flushed between steps
+    lf = Leapfrog(post, eps=1e-3, steps_per_graph=1, use_autograd=True)
+    lf.set_state(z0, p0)
+    lf.run(3)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(steps)]
+    for e0, e1 in evs:
+        flush.zero_()
+        e0.record(s)
+        lf.graph.replay()
+        e1.record(s)
+    torch.cuda.synchronize()
+    ms_step = float(np.mean([a.elapsed_time(b) for a, b in evs]))
+
+    # the 500-step trajectory back to back (50 steps per graph; L2 stays warm)
+    lf50 = Leapfrog(post, eps=1e-3, steps_per_graph=50, use_autograd=True)
+    lf50.set_state(z0, p0)
+    h0 = float(lf50.hamiltonian())
+    lf50.run(50)
+    lf50.set_state(z0, p0)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(s)
+    lf50.run(500)
+    e1.record(s)
+    torch.cuda.synchronize()
+    ms_traj = e0.elapsed_time(e1)
+    h1 = float(lf50.hamiltonian())
+    err = post.ev.error_word()
+
+    fp = FastPosterior(GPUProposer(), P, scene=Scene(P.n_sources, P.n_bands, P.table),
+                       lower=lo, upper=hi)
+    z = fp.transform.inverse_transform(P.params.reshape(-1))
+    rng = np.random.default_rng(3)
+    fp.lnprob_and_grad(z)
+    n = 20
+    t0 = time.perf_counter()
+    for _ in range(n):
+        fp.lnprob_and_grad(z + 1e-6 * rng.standard_normal(z.shape))
+    ms_dropin = (time.perf_counter() - t0) / n * 1e3
+    out = {"workload": "config2: config-1 patch, 280 parameters, leapfrog eps 1e-3 in "
+                       "unconstrained coordinates",
+           "graph_step_ms": ms_step, "graph_evals_per_s": 1e3 / ms_step,
+           "trajectory_500_ms": ms_traj, "trajectory_evals_per_s": 500 / (ms_traj * 1e-3),
+           "trajectory_dH": h1 - h0, "error_word": err,
+           "dropin_ms_per_eval": ms_dropin, "dropin_evals_per_s": 1e3 / ms_dropin,
+           "speedup_vs_dropin": ms_dropin / ms_step,
+           "timing": "graph step: CUDA events per replay, L2 flushed between steps; "
+                     "trajectory: CUDA events around 10 replays of 50 steps (L2 warm); "
+                     "drop-in: host wall clock per FastPosterior.lnprob_and_grad"}
+    del lf, lf50
     return out
 
 
@@ -382,6 +497,10 @@ def run_ours(args):
     achieved = evaluated_pairs * FLOPS_PER_PAIR / tile_s / 1e12
     sfu = evaluated_pairs * 2 / tile_s / 1e9
 
+    differentiable = None
+    if not args.no_differentiable:
+        differentiable = differentiable_leg(args, torch, P, cfg, steps=max(3, min(args.steps, 50)))
+
     batched = None
     if args.batch_patches > 0:
         batched = batched_leg(args, torch, _lib, steps=max(3, min(args.steps, 50)))
@@ -420,6 +539,7 @@ def run_ours(args):
                          "sfu_gops": sfu, "sfu_peak_gops": ex2_gops, "sfu_frac": sfu / ex2_gops},
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
+            "differentiable": differentiable,
             "batched": batched,
         }
         print(json.dumps(line), flush=True)

@@ -16,6 +16,7 @@ from . import build as _build
 FPHO_OK = 0
 FPHO_IO_HOST = 1
 FPHO_WANT_RESIDUAL = 2
+FPHO_CHI2_ONLY = 4
 
 _ERRNAMES = {1: "INVALID", 2: "CUDA", 3: "NOMEM", 4: "LIMIT", 5: "STATE", 6: "KERNEL"}
 
@@ -73,6 +74,13 @@ _SIGS = {
     "fpho_batch_time_tiles": (c_int, [c_void_p, c_int]),
     "fpho_batch_last_tile_ms": (c_int, [c_void_p, ctypes.POINTER(ctypes.c_float)]),
     "fpho_batch_free": (c_int, [c_void_p]),
+    "fpho_spline_create": (c_int, [c_void_p, c_int, c_void_p, c_int, c_void_p, c_int, c_void_p,
+                                   ctypes.c_double, c_void_p, ctypes.POINTER(c_void_p)]),
+    "fpho_spline_free": (c_int, [c_void_p]),
+    "fpho_build_proposal": (c_int, [c_void_p, c_void_p, c_int, c_int, c_void_p, c_void_p]),
+    "fpho_build_proposal_batch": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p,
+                                          c_void_p, c_void_p]),
+    "fpho_spline_points": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p]),
     "fpho_patch_time_tiles": (c_int, [c_void_p, c_int]),
     "fpho_patch_image_gaussians": (c_int, [c_void_p, c_int, c_void_p, c_int,
                                            ctypes.POINTER(c_int)]),

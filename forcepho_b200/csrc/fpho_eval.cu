@@ -65,7 +65,7 @@ extern "C" int fpho_sizeof(int which) {
 // ======================================================================= kernels
 namespace fpho {
 
-template <int NT, int K>
+template <int NT, int K, bool GRAD>
 __global__ void __launch_bounds__(NT) tile_kernel(TileArgs A) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ uint64_t mbar;
@@ -75,23 +75,21 @@ __global__ void __launch_bounds__(NT) tile_kernel(TileArgs A) {
     }
     __syncthreads();
     uint32_t phase = 0;
-    tile_body<NT, K>(A, blockIdx.x, smem, &mbar, phase);
+    tile_body<NT, K, GRAD>(A, blockIdx.x, smem, &mbar, phase);
 }
 
 // ------------------------------------------------------------ variants
 struct Variant {
     int nt, k;
-    const void *fn;
+    const void *fn[2];  // [0] chi2 only, [1] chi2 + gradient
 };
+#define FPHO_VARIANT(NT, K) \
+    {NT, K, {(const void *)tile_kernel<NT, K, false>, (const void *)tile_kernel<NT, K, true>}}
 static const Variant kVariants[] = {
-    {128, 4, (const void *)tile_kernel<128, 4>},
-    {128, 2, (const void *)tile_kernel<128, 2>},
-    {256, 2, (const void *)tile_kernel<256, 2>},
-    {64, 4, (const void *)tile_kernel<64, 4>},
-    {256, 4, (const void *)tile_kernel<256, 4>},
-    {128, 8, (const void *)tile_kernel<128, 8>},
-    {64, 8, (const void *)tile_kernel<64, 8>},
+    FPHO_VARIANT(128, 4), FPHO_VARIANT(128, 2), FPHO_VARIANT(256, 2), FPHO_VARIANT(64, 4),
+    FPHO_VARIANT(256, 4), FPHO_VARIANT(128, 8), FPHO_VARIANT(64, 8),
 };
+#undef FPHO_VARIANT
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
 int variant_count() { return kNumVariants; }
@@ -99,24 +97,26 @@ int variant_tile_pixels(int v) { return kVariants[v].nt * kVariants[v].k; }
 int variant_threads(int v) { return kVariants[v].nt; }
 
 static std::mutex g_attr_mu;
-static size_t g_attr_set[64][kNumVariants];  // per device, per variant
+static size_t g_attr_set[64][kNumVariants][2];  // per device, variant, gradient flag
 
-int launch_tile_kernel(int variant, const TileArgs &A, int n_tiles, cudaStream_t stream) {
+int launch_tile_kernel(int variant, const TileArgs &A, int n_tiles, cudaStream_t stream,
+                       bool grad) {
     if (n_tiles <= 0) return FPHO_OK;
     const Variant &V = kVariants[variant];
+    const void *fn = V.fn[grad ? 1 : 0];
     const size_t smem = tile_smem_bytes(variant, A.live_cap, A.idx_cap, A.pgrad_stride);
     int dev = 0;
     CUDA_TRY(cudaGetDevice(&dev));
     {
         std::lock_guard<std::mutex> lk(g_attr_mu);
-        if (dev < 64 && g_attr_set[dev][variant] < smem) {
-            CUDA_TRY(cudaFuncSetAttribute(V.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        if (dev < 64 && g_attr_set[dev][variant][grad] < smem) {
+            CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)smem));
-            g_attr_set[dev][variant] = smem;
+            g_attr_set[dev][variant][grad] = smem;
         }
     }
     void *args[] = {(void *)&A};
-    CUDA_TRY(cudaLaunchKernel(V.fn, dim3(n_tiles), dim3(V.nt), args, smem, stream));
+    CUDA_TRY(cudaLaunchKernel(fn, dim3(n_tiles), dim3(V.nt), args, smem, stream));
     return FPHO_OK;
 }
 
@@ -540,7 +540,7 @@ namespace fpho {
 
 // Enqueue one evaluation with device-resident proposal and outputs.
 int enqueue_evaluate(fpho_patch *p, const fpho_source *d_prop, double *d_chi2, float *d_dchi2,
-                     int out_stride, bool want_residual, cudaStream_t s) {
+                     int out_stride, bool want_residual, cudaStream_t s, bool grad) {
     if (want_residual && !p->d_residual)
         return set_error(FPHO_ERR_STATE,
                          "residual requested but the patch was created without one");
@@ -569,12 +569,13 @@ int enqueue_evaluate(fpho_patch *p, const fpho_source *d_prop, double *d_chi2, f
     A.err = p->d_err;
     A.pairs = p->count_pairs ? p->d_pairs : nullptr;
     if (p->ev_tile0) CUDA_TRY(cudaEventRecord(p->ev_tile0, s));
-    int rc = launch_tile_kernel(p->variant, A, p->n_tiles, s);
+    int rc = launch_tile_kernel(p->variant, A, p->n_tiles, s, grad);
     if (rc) return rc;
     if (p->ev_tile1) CUDA_TRY(cudaEventRecord(p->ev_tile1, s));
-    dim3 rg(p->n_bands, (out_stride + 127) / 128);
+    dim3 rg(p->n_bands, grad ? (out_stride + 127) / 128 : 1);
     reduce_bands<<<rg, 128, 0, s>>>(p->d_tile_band_start, p->d_pchi2, p->d_pgrad,
-                                    7 * p->n_sources, d_chi2, d_dchi2, out_stride);
+                                    7 * p->n_sources, d_chi2, grad ? d_dchi2 : nullptr,
+                                    out_stride);
     CUDA_TRY(cudaGetLastError());
     return FPHO_OK;
 }
@@ -585,7 +586,10 @@ extern "C" int fpho_evaluate_proposal(fpho_patch *p, const fpho_source *proposal
                                       double *chi2, float *dchi2, int dchi2_stride,
                                       unsigned flags, void *stream) {
     clear_error();
-    if (!p || !proposal || !chi2 || !dchi2) return set_error(FPHO_ERR_INVALID, "NULL argument");
+    const bool grad = (flags & FPHO_CHI2_ONLY) == 0;
+    if (!p || !proposal || !chi2 || (grad && !dchi2))
+        return set_error(FPHO_ERR_INVALID, "NULL argument");
+    if (!grad) dchi2_stride = 7 * n_sources;
     if (n_sources != p->n_sources)
         return set_error(FPHO_ERR_INVALID, "n_sources=%d but the patch has %d", n_sources,
                          p->n_sources);
@@ -595,7 +599,8 @@ extern "C" int fpho_evaluate_proposal(fpho_patch *p, const fpho_source *proposal
     cudaStream_t s = (cudaStream_t)stream;
     const bool host_io = (flags & FPHO_IO_HOST) != 0;
     const bool want_res = (flags & FPHO_WANT_RESIDUAL) != 0;
-    if (!host_io) return enqueue_evaluate(p, proposal, chi2, dchi2, dchi2_stride, want_res, s);
+    if (!host_io)
+        return enqueue_evaluate(p, proposal, chi2, dchi2, dchi2_stride, want_res, s, grad);
 
     const size_t gbytes = (size_t)p->n_bands * dchi2_stride;
     if (p->d_dchi2_cap < (int)gbytes) {
@@ -607,13 +612,14 @@ extern "C" int fpho_evaluate_proposal(fpho_patch *p, const fpho_source *proposal
     CUDA_TRY(cudaMemcpyAsync(p->d_prop, proposal, sizeof(fpho_source) * n_sources,
                              cudaMemcpyHostToDevice, s));
     int rc = enqueue_evaluate(p, p->d_prop, p->d_chi2_out, p->d_dchi2_out, dchi2_stride,
-                              want_res, s);
+                              want_res, s, grad);
     if (rc) return rc;
     int err = 0;
     CUDA_TRY(cudaMemcpyAsync(chi2, p->d_chi2_out, sizeof(double) * p->n_bands,
                              cudaMemcpyDeviceToHost, s));
-    CUDA_TRY(cudaMemcpyAsync(dchi2, p->d_dchi2_out, sizeof(float) * gbytes,
-                             cudaMemcpyDeviceToHost, s));
+    if (grad)
+        CUDA_TRY(cudaMemcpyAsync(dchi2, p->d_dchi2_out, sizeof(float) * gbytes,
+                                 cudaMemcpyDeviceToHost, s));
     CUDA_TRY(cudaMemcpyAsync(&err, p->d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
     CUDA_TRY(cudaStreamSynchronize(s));
     if (err) return set_error(FPHO_ERR_KERNEL, "tile kernel reported error word 0x%x", err);
@@ -635,7 +641,7 @@ extern "C" int fpho_EvaluateProposal(fpho_patch *p, const void *dev_patch_struct
                          FPHO_MAXSOURCES);
     return enqueue_evaluate(p, (const fpho_source *)dev_proposal, (double *)pchi2,
                             (float *)pdchi2_dp, FPHO_MAXSOURCES * FPHO_NPARAMS,
-                            p->d_residual != nullptr, (cudaStream_t)stream);
+                            p->d_residual != nullptr, (cudaStream_t)stream, true);
 }
 
 extern "C" int fpho_patch_image_gaussians(fpho_patch *p, int exposure, float *host_out,

@@ -22,7 +22,8 @@ int variant_count();
 int variant_tile_pixels(int v);
 int variant_threads(int v);
 size_t tile_smem_bytes(int variant, int live_cap, int idx_cap, int stride);
-int launch_tile_kernel(int variant, const TileArgs &A, int n_tiles, cudaStream_t stream);
+int launch_tile_kernel(int variant, const TileArgs &A, int n_tiles, cudaStream_t stream,
+                       bool grad);
 
 PatchView make_view(const fpho_patch *p);
 

@@ -62,7 +62,7 @@ static __global__ void reduce_bands(const int *tile_band_start, const double *pc
     const int b = blockIdx.x;
     const int t0 = tile_band_start[b], t1 = tile_band_start[b + 1];
     const int j = blockIdx.y * blockDim.x + threadIdx.x;
-    if (j < out_stride) {
+    if (dchi2_out && j < out_stride) {
         double acc = 0.0;
         if (j < stride)
             for (int t = t0; t < t1; ++t) acc += (double)pgrad[(size_t)t * stride + j];

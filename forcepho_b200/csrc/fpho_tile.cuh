@@ -267,7 +267,9 @@ constexpr int FLAG_CUT = 1;        // the exp-argument can exceed 36 inside the 
 constexpr int FLAG_LAST_SRC = 2;   // last kept Gaussian of its source in the chunk
 
 // ------------------------------------------------------------ the tile body
-template <int NT, int K>
+// GRAD = false runs the residual pass and chi2 only (no gradient pass, no
+// gradient partials written).
+template <int NT, int K, bool GRAD = true>
 __device__ __forceinline__ void tile_body(const TileArgs &A, int tile, unsigned char *smem,
                                           uint64_t *mbar, uint32_t &phase) {
     static_assert(K % 2 == 0, "pixels per thread must be even (packed pairs)");
@@ -438,7 +440,7 @@ __device__ __forceinline__ void tile_body(const TileArgs &A, int tile, unsigned 
 
     // ------------------------------------------------------------ pass 2
     // Chunks in reverse order: the last chunk of pass 1 is still staged.
-    if (tile_has_weight) {
+    if (GRAD && tile_has_weight) {
         float P[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         for (int c = n_chunks - 1; c >= 0; --c) {
             const int c0 = c * cap, n = min(cap, n_live - c0);
@@ -504,7 +506,7 @@ __device__ __forceinline__ void tile_body(const TileArgs &A, int tile, unsigned 
         for (int w = 0; w < NW; ++w) c += s_chi2[w];
         A.pchi2[tile] = c;
     }
-    for (int j = tid; j < stride; j += NT) {
+    for (int j = tid; GRAD && j < stride; j += NT) {
         float v = 0.0f;
 #pragma unroll
         for (int w = 0; w < NW; ++w) v += wacc[w * stride + j];

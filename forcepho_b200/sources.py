@@ -23,7 +23,7 @@ from scipy.interpolate import RectBivariateSpline
 from .kernel_limits import MAXRADII
 from .proposal import source_struct_dtype
 
-__all__ = ["SersicTable", "default_table", "proposal_from_params", "SHAPE_COLS"]
+__all__ = ["SersicTable", "Scene", "default_table", "proposal_from_params", "SHAPE_COLS"]
 
 SHAPE_COLS = ["ra", "dec", "q", "pa", "sersic", "rhalf"]
 _DEFAULT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data",
@@ -128,3 +128,30 @@ def proposal_from_params(params, n_bands, table=None):
         out["damplitude_drh"][i, :nr] = table.damplitude_drh(n, rh)
         out["damplitude_dnsersic"][i, :nr] = table.damplitude_dsersic(n, rh)
     return out
+
+
+class Scene:
+    """The map between the flat parameter vector of the active sources and
+    their proposal (forcepho/sources.py:28-97: ``set_all_source_params``,
+    ``get_all_source_params``, ``get_proposal``), for ``n_sources`` Sersic
+    galaxies of ``n_bands`` fluxes each, in Scene order."""
+
+    def __init__(self, n_sources, n_bands, table=None, params=None):
+        self.n_sources, self.n_bands = int(n_sources), int(n_bands)
+        self.table = table or default_table()
+        self.n_params_per_source = self.n_bands + 6
+        self.params = np.zeros((self.n_sources, self.n_params_per_source))
+        if params is not None:
+            self.set_all_source_params(params)
+
+    def __len__(self):
+        return self.n_sources
+
+    def set_all_source_params(self, Theta):
+        self.params[:] = np.asarray(Theta, dtype=np.float64).reshape(self.params.shape)
+
+    def get_all_source_params(self, active=True):
+        return self.params.reshape(-1).copy()
+
+    def get_proposal(self, active=True):
+        return proposal_from_params(self.params, self.n_bands, self.table)

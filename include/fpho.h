@@ -59,6 +59,7 @@ enum fpho_status {
 /* evaluate flags */
 #define FPHO_IO_HOST 1u          /* proposal and outputs are host pointers; the call synchronizes */
 #define FPHO_WANT_RESIDUAL 2u    /* write data - model to the patch's residual array */
+#define FPHO_CHI2_ONLY 4u        /* residual pass and chi2 only; dchi2 is not written (may be NULL) */
 
 /* One PSF Gaussian already matched to a Sersic radius bin:
  * forcepho/src/patch.cc:101-118 (28 bytes). */
@@ -182,6 +183,43 @@ FPHO_API int fpho_evaluate_proposal(fpho_patch *p, const fpho_source *proposal, 
  * fpho_response[n_bands].  Same computation as fpho_evaluate_proposal. */
 FPHO_API int fpho_EvaluateProposal(fpho_patch *p, const void *dev_patch_struct, const void *dev_proposal,
                           void *pchi2, void *pdchi2_dp, void *stream);
+
+/* ---- proposals built on the device -------------------------------------- */
+
+typedef struct fpho_spline fpho_spline;   /* opaque: Sersic amplitude splines on the device */
+
+/* Upload the bicubic B-splines of the Sersic mixture amplitudes: one spline
+ * per mixture radius over (sersic, rh), sharing knots tx[ntx], ty[nty]
+ * (scipy RectBivariateSpline.get_knots()); coeffs[n_radii][ntx-4][nty-4]
+ * (get_coeffs() of each); radii[n_radii] in arcsec; sersic_min = lowest
+ * sersic index of the table.  Replaces Galaxy.initialize_splines
+ * (forcepho/sources.py:623-645). */
+FPHO_API int fpho_spline_create(const double *tx, int ntx, const double *ty, int nty,
+                                const double *coeffs, int n_radii, const double *radii,
+                                double sersic_min, void *stream, fpho_spline **out);
+FPHO_API int fpho_spline_free(fpho_spline *s);
+
+/* Build the device proposal fpho_source[n_sources] from device parameters
+ * theta[n_sources][n_bands + 6] in Scene order (flux_1..flux_B, ra, dec, q,
+ * pa, sersic, rhalf), with mixture amplitudes and their sersic / rh
+ * derivatives from the splines (including the reference's branches for
+ * sersic below the table and rh < 0).  Replaces Scene.get_proposal /
+ * Galaxy.proposal (forcepho/sources.py:80-97, 607-694). */
+FPHO_API int fpho_build_proposal(const fpho_spline *s, const double *theta, int n_sources,
+                                 int n_bands, fpho_source *out, void *stream);
+
+/* The same for the sources of many patches at once: source s has
+ * src_bands[s] bands and its parameters start at theta[src_offset[s]]
+ * (src_bands, src_offset and theta in device memory).  No reference
+ * counterpart: it builds the proposals of a batch (fpho_batch_evaluate). */
+FPHO_API int fpho_build_proposal_batch(const fpho_spline *s, const double *theta, int n_sources,
+                                       const int *src_bands, const long long *src_offset,
+                                       fpho_source *out, void *stream);
+
+/* Spline values and derivatives at m device points (x = sersic, y = rh):
+ * out[m][n_radii][3] = (value, d/dsersic, d/drh). */
+FPHO_API int fpho_spline_points(const fpho_spline *s, const double *x, const double *y, int m,
+                                double *out, void *stream);
 
 /* ---- batched evaluation ------------------------------------------------ */
 

@@ -25,6 +25,7 @@
  * (forcepho/src/patch.cc:23-119, forcepho/src/proposal.cu:13-39) and must stay
  * byte-compatible with it.
  */
+#include <float.h>
 #include <math.h>
 #include <stdint.h>
 #include <stdlib.h>
@@ -405,6 +406,11 @@ typedef struct {
     double jac[7][6];   /* d(A,x,y,fxx,fyy,fxy)/d(flux,ra,dec,q,pa,n,rh) */
 } fpo_imgauss_d;
 
+/* Optional double-precision mixture amplitudes, [n_sources][FPO_MAXRADII],
+ * used instead of the proposal's float ones while set (finite differences
+ * in sersic and rh without the float rounding of the amplitudes). */
+static const double *g_amp_f64 = NULL;
+
 static void convolve_source_f64(int band, int e, int g, int npsf,
                                 const fpo_patch *P, const fpo_source *S,
                                 fpo_imgauss_d *out) {
@@ -434,7 +440,7 @@ static void convolve_source_f64(int band, int e, int g, int npsf,
         fpo_imgauss_d *ig = out + g * npsf + p;
         int k = pg->sersic_radius_bin;
         double r2 = P->rad2[k];
-        double am = gal->mixture_amplitudes[k];
+        double am = g_amp_f64 ? g_amp_f64[g * FPO_MAXRADII + k] : gal->mixture_amplitudes[k];
         /* Sigma = r2 T T^t + Cpsf */
         double s11 = r2 * (T.a * T.a + T.b * T.b) + pg->Cxx;
         double s12 = r2 * (T.a * T.c + T.b * T.d) + pg->Cxy;
@@ -549,15 +555,35 @@ int fpo_evaluate_band_f64(int band, const fpo_patch *P, const fpo_source *S,
     return 0;
 }
 
+/* fpo_evaluate_band_f64 with the mixture amplitudes taken from
+ * amps[n_sources][FPO_MAXRADII] (double) instead of the proposal. */
+int fpo_evaluate_band_f64_amps(int band, const fpo_patch *P, const fpo_source *S,
+                               const double *amps, int use_cutoff, double *chi2_out,
+                               double *dchi2) {
+    g_amp_f64 = amps;
+    int rc = fpo_evaluate_band_f64(band, P, S, use_cutoff, chi2_out, dchi2, NULL);
+    g_amp_f64 = NULL;
+    return rc;
+}
+
 /* Like fpo_evaluate_band_mixed (float image Gaussians, double pixel math),
  * but contracting with the Jacobian per pixel, so that it can also return, per
  * gradient component, the sum over pixels of the absolute value of the
- * per-pixel contribution: the scale against which float rounding of the
- * per-pixel terms is measured (a component much smaller than this scale is
- * ill-conditioned).  dchi2 and dchi2_abs are double[n_sources*7]. */
+ * per-pixel contribution (dchi2_abs) and, if dchi2_abs_terms is not NULL, the
+ * sum over pixels and image Gaussians of the absolute value of each
+ * (pixel, Gaussian) term: the condition scales against which float rounding
+ * is measured (a component much smaller than them is ill-conditioned; the
+ * second also counts cancellation between the Gaussians of a source within a
+ * pixel, e.g. of the mixed-sign d(amplitude)/d(rh) across radii).  If
+ * dchi2_res_scale is not NULL it receives, per component, the sum over pixels
+ * of FLT_EPSILON * (|d| + sum |model terms|) * 2 ie^2 |d model / d theta|:
+ * how far float rounding of the residual alone can move the component.
+ * dchi2, dchi2_abs, dchi2_abs_terms and dchi2_res_scale are
+ * double[n_sources*7]. */
 int fpo_evaluate_band_mixed_abs(int band, const fpo_patch *P, const fpo_source *S,
                                 int use_cutoff, double *chi2_out, double *dchi2,
-                                double *dchi2_abs) {
+                                double *dchi2_abs, double *dchi2_abs_terms,
+                                double *dchi2_res_scale) {
     int nsrc = P->n_sources;
     int npsf = P->n_psf_per_source[band];
     int bN = P->band_N[band], b0 = P->band_start[band];
@@ -566,6 +592,10 @@ int fpo_evaluate_band_mixed_abs(int band, const fpo_patch *P, const fpo_source *
     double *pc = (double *)malloc(sizeof(double) * FPO_NPARAMS * (size_t)(nsrc > 0 ? nsrc : 1));
     if (!ig || !pc) { free(ig); free(pc); return -1; }
     for (int i = 0; i < nsrc * FPO_NPARAMS; i++) dchi2[i] = dchi2_abs[i] = 0.0;
+    if (dchi2_abs_terms)
+        for (int i = 0; i < nsrc * FPO_NPARAMS; i++) dchi2_abs_terms[i] = 0.0;
+    if (dchi2_res_scale)
+        for (int i = 0; i < nsrc * FPO_NPARAMS; i++) dchi2_res_scale[i] = 0.0;
     double chi2 = 0.0;
     for (int ee = 0; ee < bN; ee++) {
         int e = b0 + ee;
@@ -575,7 +605,7 @@ int fpo_evaluate_band_mixed_abs(int band, const fpo_patch *P, const fpo_source *
             int pix = P->exposure_start[e] + p;
             double xp = P->xpix[pix], yp = P->ypix[pix];
             double d = P->data[pix], ie = P->ierr[pix];
-            double r = d;
+            double r = d, mabs = fabs(d);
             for (int i = 0; i < ntot; i++) {
                 const fpo_imgauss *g = ig + i;
                 double dx = xp - g->xcen, dy = yp - g->ycen;
@@ -585,10 +615,16 @@ int fpo_evaluate_band_mixed_abs(int band, const fpo_patch *P, const fpo_source *
                 if (use_cutoff && ea > FPO_MAX_EXP_ARG) continue;
                 double H = 1.0 + (vx * vx + vy * vy - fxx - fyy) / 24.0;
                 r -= (double)g->amp * exp(-0.5 * ea) * H;
+                mabs += fabs((double)g->amp * exp(-0.5 * ea) * H);
             }
             chi2 += (r * ie - d * ie) * (r * ie + d * ie);
             double rie2 = r * ie * ie;
             if (rie2 == 0.0) continue;
+            /* a float evaluation of r carries an error of order
+             * FLT_EPSILON * (|d| + sum |model terms|); through the weight
+             * -2 r ie^2 it moves each component by that error times
+             * 2 ie^2 |d model / d theta| */
+            double rerr_w = 2.0 * (double)FLT_EPSILON * mabs * ie * ie / (-2.0 * rie2);
             memset(pc, 0, sizeof(double) * FPO_NPARAMS * (size_t)nsrc);
             for (int i = 0; i < ntot; i++) {
                 const fpo_imgauss *g = ig + i;
@@ -607,20 +643,26 @@ int fpo_evaluate_band_mixed_abs(int band, const fpo_patch *P, const fpo_source *
                 double gfx = w * (-0.5 * C * dx * dx - c_h * (1.0 - 2.0 * dx * vx) / 24.0);
                 double gfy = w * (-0.5 * C * dy * dy - c_h * (1.0 - 2.0 * dy * vy) / 24.0);
                 double gfxy = w * (-C * dx * dy + c_h * (dy * vx + dx * vy) / 12.0);
+                double t[FPO_NPARAMS];
+                t[0] = g->dA_dFlux * gA;
+                t[1] = g->dx_dAlpha * gx + (double)g->dy_dAlpha * gy;
+                t[2] = g->dx_dDelta * gx + (double)g->dy_dDelta * gy;
+                t[3] = g->dA_dQ * gA + (double)g->dFxx_dQ * gfx + (double)g->dFyy_dQ * gfy +
+                       (double)g->dFxy_dQ * gfxy;
+                t[4] = g->dA_dPA * gA + (double)g->dFxx_dPA * gfx + (double)g->dFyy_dPA * gfy +
+                       (double)g->dFxy_dPA * gfxy;
+                t[5] = g->dA_dSersic * gA;
+                t[6] = g->dA_drh * gA;
                 double *q = pc + (i / npsf) * FPO_NPARAMS;
-                q[0] += g->dA_dFlux * gA;
-                q[1] += g->dx_dAlpha * gx + (double)g->dy_dAlpha * gy;
-                q[2] += g->dx_dDelta * gx + (double)g->dy_dDelta * gy;
-                q[3] += g->dA_dQ * gA + (double)g->dFxx_dQ * gfx + (double)g->dFyy_dQ * gfy +
-                        (double)g->dFxy_dQ * gfxy;
-                q[4] += g->dA_dPA * gA + (double)g->dFxx_dPA * gfx + (double)g->dFyy_dPA * gfy +
-                        (double)g->dFxy_dPA * gfxy;
-                q[5] += g->dA_dSersic * gA;
-                q[6] += g->dA_drh * gA;
+                for (int k = 0; k < FPO_NPARAMS; k++) {
+                    q[k] += t[k];
+                    if (dchi2_abs_terms) dchi2_abs_terms[(i / npsf) * FPO_NPARAMS + k] += fabs(t[k]);
+                }
             }
             for (int k = 0; k < nsrc * FPO_NPARAMS; k++) {
                 dchi2[k] += pc[k];
                 dchi2_abs[k] += fabs(pc[k]);
+                if (dchi2_res_scale) dchi2_res_scale[k] += fabs(pc[k] * rerr_w);
             }
         }
     }

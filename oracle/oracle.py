@@ -97,14 +97,16 @@ def oracle_evaluate(patch, proposal, precision="f32", cutoff=True, residual=Fals
     return chi2, dchi2
 
 
-def oracle_mixed_abs(patch, proposal):
+def oracle_mixed_abs(patch, proposal, terms=False):
     """Mixed-precision evaluation (the reference's float image Gaussians,
     double pixel math) returning chi2, dchi2 (n_bands, n_src, 7) and, per
-    component, the sum over pixels of |per-pixel contribution|."""
+    component, the sum over pixels of |per-pixel contribution|; with
+    ``terms``, also the sum over pixels and Gaussians of |each term| and the
+    residual-rounding scale (see fpo_evaluate_band_mixed_abs)."""
     L = lib()
     if not hasattr(L, "_mixed_abs_bound"):
         vp, ip = ctypes.c_void_p, ctypes.c_int
-        L.fpo_evaluate_band_mixed_abs.argtypes = [ip, vp, vp, ip, vp, vp, vp]
+        L.fpo_evaluate_band_mixed_abs.argtypes = [ip, vp, vp, ip, vp, vp, vp, vp, vp]
         L.fpo_evaluate_band_mixed_abs.restype = ip
         L._mixed_abs_bound = True
     st = patch.host_struct()
@@ -113,14 +115,22 @@ def oracle_mixed_abs(patch, proposal):
     chi2 = np.zeros(nb)
     dchi2 = np.zeros((nb, ns, 7))
     dabs = np.zeros((nb, ns, 7))
+    dterm = np.zeros((nb, ns, 7))
+    dres = np.zeros((nb, ns, 7))
     for b in range(nb):
         c = ctypes.c_double(0.0)
         g = np.zeros(ns * 7)
         a = np.zeros(ns * 7)
+        t = np.zeros(ns * 7)
+        rs = np.zeros(ns * 7)
         if L.fpo_evaluate_band_mixed_abs(b, st.ctypes.data, prop.ctypes.data, 1, ctypes.byref(c),
-                                         g.ctypes.data, a.ctypes.data) != 0:
+                                         g.ctypes.data, a.ctypes.data, t.ctypes.data,
+                                         rs.ctypes.data) != 0:
             raise MemoryError("oracle allocation failed")
         chi2[b], dchi2[b], dabs[b] = c.value, g.reshape(ns, 7), a.reshape(ns, 7)
+        dterm[b], dres[b] = t.reshape(ns, 7), rs.reshape(ns, 7)
+    if terms:
+        return chi2, dchi2, dabs, dterm, dres
     return chi2, dchi2, dabs
 
 
@@ -258,3 +268,84 @@ def ref_evaluate(patch, proposal, bands=None, pool=None):
         chi2[b] = c
         dchi2[b] = g
     return chi2, dchi2
+
+
+# ---------------------------------------------------------------- oracle workers
+def _oracle_init(root):
+    if root not in sys.path:
+        sys.path.insert(0, root)
+    lib()
+
+
+def _worker_mixed_abs(payload, proposal, band):
+    """(band, chi2, dchi2, dabs, dterm, dres), each (n_src, 7) after chi2, of
+    the mixed oracle for one band, in a worker process."""
+    L = lib()
+    if not hasattr(L, "_mixed_abs_bound"):
+        vp, ip = ctypes.c_void_p, ctypes.c_int
+        L.fpo_evaluate_band_mixed_abs.argtypes = [ip, vp, vp, ip, vp, vp, vp, vp, vp]
+        L.fpo_evaluate_band_mixed_abs.restype = ip
+        L._mixed_abs_bound = True
+    arrays, ns, nr = payload
+    st = _struct_from_arrays(arrays, ns, nr)
+    prop = np.ascontiguousarray(proposal)
+    c = ctypes.c_double(0.0)
+    g = np.zeros(ns * 7)
+    a = np.zeros(ns * 7)
+    t = np.zeros(ns * 7)
+    rs = np.zeros(ns * 7)
+    if L.fpo_evaluate_band_mixed_abs(band, st.ctypes.data, prop.ctypes.data, 1, ctypes.byref(c),
+                                     g.ctypes.data, a.ctypes.data, t.ctypes.data,
+                                     rs.ctypes.data) != 0:
+        raise MemoryError("oracle allocation failed")
+    return (band, c.value, g.reshape(ns, 7), a.reshape(ns, 7), t.reshape(ns, 7),
+            rs.reshape(ns, 7))
+
+
+def oracle_pool(processes):
+    """A spawn pool of workers with the C oracle loaded."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    return ctx.Pool(processes, initializer=_oracle_init, initargs=(os.path.dirname(HERE),))
+
+
+def mixed_abs_many(patch, jobs, pool):
+    """Mixed-oracle (chi2, dchi2, dabs) for a list of (proposal, band) jobs,
+    spread over `pool` (see oracle_pool)."""
+    payload = _patch_payload(patch)
+    return pool.starmap(_worker_mixed_abs, [(payload, np.ascontiguousarray(p), b)
+                                            for p, b in jobs])
+
+
+def _worker_f64(payload, proposal, band, amps=None):
+    """(band, chi2) of the all-FP64 oracle for one band, in a worker process;
+    `amps` (n_sources, 10) float64 replaces the proposal's float amplitudes."""
+    L = lib()
+    arrays, ns, nr = payload
+    st = _struct_from_arrays(arrays, ns, nr)
+    prop = np.ascontiguousarray(proposal)
+    c = ctypes.c_double(0.0)
+    g = np.zeros(ns * 7)
+    if amps is None:
+        rc = L.fpo_evaluate_band_f64(band, st.ctypes.data, prop.ctypes.data, 1,
+                                     ctypes.byref(c), g.ctypes.data, None)
+    else:
+        a = np.ascontiguousarray(amps, dtype=np.float64)
+        fn = L.fpo_evaluate_band_f64_amps
+        fn.argtypes = [ctypes.c_int] + [ctypes.c_void_p] * 3 + [ctypes.c_int] + \
+            [ctypes.c_void_p] * 2
+        fn.restype = ctypes.c_int
+        rc = fn(band, st.ctypes.data, prop.ctypes.data, a.ctypes.data, 1, ctypes.byref(c),
+                g.ctypes.data)
+    if rc != 0:
+        raise MemoryError("oracle allocation failed")
+    return band, c.value
+
+
+def f64_chi2_many(patch, jobs, pool):
+    """All-FP64 chi2 for a list of (proposal, band[, amps]) jobs, spread over
+    `pool`."""
+    payload = _patch_payload(patch)
+    args = [(payload, np.ascontiguousarray(j[0]), j[1], j[2] if len(j) > 2 else None)
+            for j in jobs]
+    return [c for _, c in pool.starmap(_worker_f64, args)]
