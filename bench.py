@@ -54,6 +54,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--variant", type=int, default=None)
     ap.add_argument("--live-cap", type=int, default=None)
+    ap.add_argument("--schedule", type=int, default=None, choices=[0, 1],
+                    help="0: one CTA per tile; 1: persistent CTAs, costliest tiles first")
     ap.add_argument("--batch-patches", type=int, default=256,
                     help="patches of the batched leg (config 3); 0 skips it")
     ap.add_argument("--no-differentiable", action="store_true",
@@ -397,15 +399,15 @@ def run_ours(args):
 
     from forcepho_b200 import _lib
     from forcepho_b200.proposal import GPUProposer
-    from forcepho_b200.autotune import choose_config
+    from forcepho_b200.autotune import apply_config, choose_config
 
     P = make_workload(args.seed, device_render=True)
     prop = P.proposal()
     P.return_residual = False
     P.send_to_device()
     dp = P.device_patch
-    cfg = choose_config(P, variant=args.variant, live_cap=args.live_cap)
-    dp.set_config(cfg["variant"], cfg["live_cap"])
+    cfg = choose_config(P, variant=args.variant, live_cap=args.live_cap, schedule=args.schedule)
+    apply_config(P, cfg)
     stream = torch.cuda.current_stream()
     sp = stream.cuda_stream
 
@@ -524,13 +526,14 @@ def run_ours(args):
             "config": {"workload": WORKLOAD, "pairs_per_eval": P.pairs_per_eval,
                        "evaluated_pairs": evaluated_pairs, "l2": "flushed between steps",
                        "tile_variant": list(_lib.variants()[cfg["variant"]]),
-                       "live_cap": cfg["live_cap"], "parallelism": f"patch-parallel x{world}"},
+                       "live_cap": cfg["live_cap"], "schedule": cfg.get("schedule", 0),
+                       "parallelism": f"patch-parallel x{world}"},
             "pix_gauss_per_s": P.pairs_per_eval * value,
             "evaluated_pix_gauss_per_s": evaluated_pairs * value,
             "e2e": {"value": e2e_value, "unit": "evals/s",
                     "h2d_bytes_per_step": int(prop.nbytes),
                     "d2h_bytes_per_step": int(nb * 8 + nb * ns * 7 * 4 + 4)},
-            "gpu_launches": 3 * args.steps,
+            "gpu_launches": (4 if cfg.get("schedule", 0) == 1 else 3) * args.steps,
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_tflops,
                          "unit": "TFLOP/s", "frac": achieved / fp32_tflops,
                          "traffic": None,

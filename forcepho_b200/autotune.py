@@ -1,12 +1,14 @@
 """Launch-configuration autotuner for the pixel-tile kernel.
 
 The tile kernel is compiled in several variants (threads per CTA x pixels per
-thread, see ``fpho_variant_info``) and takes a shared-memory stage size
-(``live_cap``: image-Gaussian records per staged chunk).  The best choice
-depends on the patch (sources, PSF components, pixels per exposure, source
-density).  :func:`choose_config` times every candidate on the patch itself
-with CUDA events and caches the winner in a JSON file keyed by a coarse
-signature of the patch, guarded by a lock for concurrent processes.
+thread, see ``fpho_variant_info``), takes a shared-memory stage size
+(``live_cap``: image-Gaussian records per staged chunk) and runs either one
+CTA per tile or as persistent CTAs taking the costliest tiles first
+(``schedule``, ``fpho_patch_set_schedule``).  The best choice depends on the
+patch (sources, PSF components, pixels per exposure, source density).
+:func:`choose_config` times every candidate on the patch itself with CUDA
+events and caches the winner in a JSON file keyed by a coarse signature of the
+patch, guarded by a lock for concurrent processes.
 """
 
 import fcntl
@@ -20,8 +22,9 @@ from . import _lib
 CACHE = os.environ.get("FPHO_AUTOTUNE_CACHE",
                        os.path.join(os.path.expanduser("~"), ".cache", "forcepho_b200",
                                     "autotune.json"))
-DEFAULT = {"variant": 0, "live_cap": 512}
-LIVE_CAPS = (128, 256, 512)
+DEFAULT = {"variant": 3, "live_cap": 192, "schedule": 1}   # 64 threads x 4 pixels
+LIVE_CAPS = (96, 128, 192, 256, 384)
+SCHEDULES = (0, 1)
 
 
 def signature(patch):
@@ -50,11 +53,12 @@ def _store(key, value):
         os.replace(tmp, CACHE)
 
 
-def time_config(patch, proposal_dev, outs, variant, live_cap, reps=3):
+def time_config(patch, proposal_dev, outs, variant, live_cap, schedule=0, reps=5):
     """Median milliseconds of one evaluation with the given configuration."""
     import torch
     dp = patch.device_patch
     dp.set_config(variant, live_cap)
+    dp.set_schedule(schedule)
     chi2, dchi2 = outs
     s = torch.cuda.current_stream()
     ns = patch.n_sources
@@ -64,6 +68,7 @@ def time_config(patch, proposal_dev, outs, variant, live_cap, reps=3):
                   chi2.data_ptr(), dchi2.data_ptr(), 7 * ns, 0, s.cuda_stream)
 
     ev()
+    ev()  # the persistent schedule orders tiles by the previous evaluation's costs
     ts = []
     for _ in range(reps):
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -76,8 +81,8 @@ def time_config(patch, proposal_dev, outs, variant, live_cap, reps=3):
 
 
 def tune(patch, proposal=None, candidates=None):
-    """Time every (variant, live_cap) on `patch` (already on the device);
-    returns (best config, {config: ms})."""
+    """Time every (variant, live_cap, schedule) on `patch` (already on the
+    device); returns (best config, {config: ms})."""
     import torch
     proposal = patch.proposal() if proposal is None else proposal
     dprop = torch.from_numpy(np.ascontiguousarray(proposal).view(np.uint8).copy()).cuda()
@@ -88,26 +93,30 @@ def tune(patch, proposal=None, candidates=None):
         candidates = []
         for v, (nt, k) in enumerate(_lib.variants()):
             for lc in LIVE_CAPS:
-                candidates.append((v, lc))
+                for sc in SCHEDULES:
+                    candidates.append((v, lc, sc))
     res = {}
-    for v, lc in candidates:
+    for cand in candidates:
+        v, lc = cand[0], cand[1]
+        sc = cand[2] if len(cand) > 2 else 0
         try:
-            res[(v, lc)] = time_config(patch, dprop, outs, v, lc)
+            res[(v, lc, sc)] = time_config(patch, dprop, outs, v, lc, sc)
         except _lib.FphoError:
             continue
     best = min(res, key=res.get)
-    return {"variant": best[0], "live_cap": best[1]}, res
+    return {"variant": best[0], "live_cap": best[1], "schedule": best[2]}, res
 
 
-def choose_config(patch, variant=None, live_cap=None, retune=False):
+def choose_config(patch, variant=None, live_cap=None, schedule=None, retune=False):
     """Configuration for `patch`: explicit arguments win, else the cached
     winner for its signature, else tune now (patch must be on the device)."""
     if variant is not None:
-        return {"variant": int(variant), "live_cap": int(live_cap or DEFAULT["live_cap"])}
+        return {"variant": int(variant), "live_cap": int(live_cap or DEFAULT["live_cap"]),
+                "schedule": int(DEFAULT["schedule"] if schedule is None else schedule)}
     key = signature(patch)
     if not retune:
         c = _load().get(key)
-        if c and c.get("variant", 99) < len(_lib.variants()):
+        if c and c.get("variant", 99) < len(_lib.variants()) and "schedule" in c:
             return c
     try:
         best, _ = tune(patch)
@@ -118,3 +127,9 @@ def choose_config(patch, variant=None, live_cap=None, retune=False):
     except OSError:
         pass
     return best
+
+
+def apply_config(patch, cfg):
+    """Set a configuration from :func:`choose_config` on the patch's handle."""
+    patch.device_patch.set_config(cfg["variant"], cfg["live_cap"])
+    patch.device_patch.set_schedule(cfg.get("schedule", 0))

@@ -78,13 +78,41 @@ __global__ void __launch_bounds__(NT) tile_kernel(TileArgs A) {
     tile_body<NT, K, GRAD>(A, blockIdx.x, smem, &mbar, phase);
 }
 
+// Persistent form: each CTA takes tiles from `order` through an atomic counter
+// (reset by order_tiles) until the list is exhausted, so the most expensive
+// tiles start first and the cheap ones fill the gaps at the end.  The counter
+// only hands out indices; no CTA waits on another.
+template <int NT, int K, bool GRAD>
+__global__ void __launch_bounds__(NT) tile_kernel_dyn(TileArgs A, const int *order, int n_tiles,
+                                                      int *counter) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ uint64_t mbar;
+    __shared__ int s_item;
+    if (threadIdx.x == 0) {
+        mbar_init(&mbar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    uint32_t phase = 0;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+        __syncthreads();
+        const int item = s_item;
+        if (item >= n_tiles) break;
+        tile_body<NT, K, GRAD>(A, order[item], smem, &mbar, phase);
+        __syncthreads();
+    }
+}
+
 // ------------------------------------------------------------ variants
 struct Variant {
     int nt, k;
-    const void *fn[2];  // [0] chi2 only, [1] chi2 + gradient
+    const void *fn[2];   // [0] chi2 only, [1] chi2 + gradient
+    const void *dyn[2];  // persistent forms of the same
 };
-#define FPHO_VARIANT(NT, K) \
-    {NT, K, {(const void *)tile_kernel<NT, K, false>, (const void *)tile_kernel<NT, K, true>}}
+#define FPHO_VARIANT(NT, K)                                                                      \
+    {NT, K, {(const void *)tile_kernel<NT, K, false>, (const void *)tile_kernel<NT, K, true>},  \
+     {(const void *)tile_kernel_dyn<NT, K, false>, (const void *)tile_kernel_dyn<NT, K, true>}}
 static const Variant kVariants[] = {
     FPHO_VARIANT(128, 4), FPHO_VARIANT(128, 2), FPHO_VARIANT(256, 2), FPHO_VARIANT(64, 4),
     FPHO_VARIANT(256, 4), FPHO_VARIANT(128, 8), FPHO_VARIANT(64, 8),
@@ -97,26 +125,66 @@ int variant_tile_pixels(int v) { return kVariants[v].nt * kVariants[v].k; }
 int variant_threads(int v) { return kVariants[v].nt; }
 
 static std::mutex g_attr_mu;
-static size_t g_attr_set[64][kNumVariants][2];  // per device, variant, gradient flag
+// per device, variant, gradient flag, form: the dynamic shared memory the
+// attribute allows, and for the persistent form the resident CTAs per SM and
+// the SM count at that size
+static size_t g_attr_set[64][kNumVariants][2][2];
+static int g_occ[64][kNumVariants][2], g_sms[64];
+static size_t g_occ_smem[64][kNumVariants][2];
+
+static int prepare_fn(const void *fn, int dev, int variant, int grad, int form, size_t smem) {
+    std::lock_guard<std::mutex> lk(g_attr_mu);
+    if (dev < 64 && g_attr_set[dev][variant][grad][form] < smem) {
+        CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+        g_attr_set[dev][variant][grad][form] = smem;
+    }
+    return FPHO_OK;
+}
+
+int device_sms() {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+    std::lock_guard<std::mutex> lk(g_attr_mu);
+    if (!g_sms[dev] &&
+        cudaDeviceGetAttribute(&g_sms[dev], cudaDevAttrMultiProcessorCount, dev) != cudaSuccess)
+        return 148;
+    return g_sms[dev];
+}
 
 int launch_tile_kernel(int variant, const TileArgs &A, int n_tiles, cudaStream_t stream,
-                       bool grad) {
+                       bool grad, const int *order, int *counter) {
     if (n_tiles <= 0) return FPHO_OK;
     const Variant &V = kVariants[variant];
-    const void *fn = V.fn[grad ? 1 : 0];
+    const bool dyn = order && counter;
+    const void *fn = dyn ? V.dyn[grad ? 1 : 0] : V.fn[grad ? 1 : 0];
     const size_t smem = tile_smem_bytes(variant, A.live_cap, A.idx_cap, A.pgrad_stride);
     int dev = 0;
     CUDA_TRY(cudaGetDevice(&dev));
+    if (dev >= 64) return set_error(FPHO_ERR_LIMIT, "device ordinal %d >= 64", dev);
+    int rc = prepare_fn(fn, dev, variant, grad, dyn ? 1 : 0, smem);
+    if (rc) return rc;
+    if (!dyn) {
+        void *args[] = {(void *)&A};
+        CUDA_TRY(cudaLaunchKernel(fn, dim3(n_tiles), dim3(V.nt), args, smem, stream));
+        return FPHO_OK;
+    }
+    int occ = 0, sms = 0;
     {
         std::lock_guard<std::mutex> lk(g_attr_mu);
-        if (dev < 64 && g_attr_set[dev][variant][grad] < smem) {
-            CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)smem));
-            g_attr_set[dev][variant][grad] = smem;
+        if (g_occ_smem[dev][variant][grad] != smem || g_occ[dev][variant][grad] == 0) {
+            CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_occ[dev][variant][grad], fn,
+                                                                   V.nt, smem));
+            g_occ_smem[dev][variant][grad] = smem;
+            if (!g_sms[dev])
+                CUDA_TRY(cudaDeviceGetAttribute(&g_sms[dev], cudaDevAttrMultiProcessorCount, dev));
         }
+        occ = g_occ[dev][variant][grad];
+        sms = g_sms[dev];
     }
-    void *args[] = {(void *)&A};
-    CUDA_TRY(cudaLaunchKernel(fn, dim3(n_tiles), dim3(V.nt), args, smem, stream));
+    if (occ < 1) return set_error(FPHO_ERR_LIMIT, "tile kernel cannot be resident (smem %zu)", smem);
+    const int grid = std::min(n_tiles, occ * sms);
+    void *args[] = {(void *)&A, (void *)&order, (void *)&n_tiles, (void *)&counter};
+    CUDA_TRY(cudaLaunchKernel(fn, dim3(grid), dim3(V.nt), args, smem, stream));
     return FPHO_OK;
 }
 
@@ -167,6 +235,7 @@ void free_meta(fpho_patch *p) {
 void free_plan(fpho_patch *p) {
     dfree(p->d_tiles); dfree(p->d_tbox_all); dfree(p->d_tbox_w); dfree(p->d_tile_band_start);
     dfree(p->d_pchi2); dfree(p->d_pgrad);
+    dfree(p->d_tile_cost); dfree(p->d_tile_order); dfree(p->d_tile_counter);
 }
 
 // Validate the index arrays of a host patch description and fill host copies.
@@ -364,6 +433,10 @@ int build_plan(fpho_patch *p, cudaStream_t s) {
     if ((rc = dalloc(&p->d_tbox_w, tiles.size()))) return rc;
     if ((rc = dalloc(&p->d_pchi2, tiles.size()))) return rc;
     if ((rc = dalloc(&p->d_pgrad, tiles.size() * (size_t)7 * p->n_sources))) return rc;
+    if ((rc = dalloc(&p->d_tile_cost, tiles.size()))) return rc;
+    if ((rc = dalloc(&p->d_tile_order, tiles.size()))) return rc;
+    if ((rc = dalloc(&p->d_tile_counter, 1))) return rc;
+    CUDA_TRY(cudaMemsetAsync(p->d_tile_cost, 0, sizeof(int) * std::max<size_t>(tiles.size(), 1), s));
     if (p->n_tiles > 0) {
         tile_bboxes<<<p->n_tiles, 128, 0, s>>>(make_view(p), p->d_tiles, p->d_tbox_all,
                                               p->d_tbox_w, nullptr);
@@ -515,6 +588,15 @@ extern "C" int fpho_patch_set_config(fpho_patch *p, int variant, int live_cap, v
     return FPHO_OK;
 }
 
+extern "C" int fpho_patch_set_schedule(fpho_patch *p, int schedule) {
+    clear_error();
+    if (!p) return set_error(FPHO_ERR_INVALID, "NULL patch");
+    if (schedule != 0 && schedule != 1)
+        return set_error(FPHO_ERR_INVALID, "schedule %d is neither 0 nor 1", schedule);
+    p->schedule = schedule;
+    return FPHO_OK;
+}
+
 extern "C" int fpho_variant_info(int variant, int out[2]) {
     clear_error();
     if (variant < 0 || variant >= variant_count() || !out)
@@ -569,7 +651,18 @@ int enqueue_evaluate(fpho_patch *p, const fpho_source *d_prop, double *d_chi2, f
     A.err = p->d_err;
     A.pairs = p->count_pairs ? p->d_pairs : nullptr;
     if (p->ev_tile0) CUDA_TRY(cudaEventRecord(p->ev_tile0, s));
-    int rc = launch_tile_kernel(p->variant, A, p->n_tiles, s, grad);
+    int rc;
+    // the order only matters when the tiles outnumber what runs at once
+    if (p->schedule == 1 && p->n_tiles > 4 * device_sms()) {
+        A.tile_cost = p->d_tile_cost;
+        order_tiles<<<1, 1024, 0, s>>>(p->d_tile_cost, p->n_tiles, p->d_tile_order,
+                                       p->d_tile_counter);
+        CUDA_TRY(cudaGetLastError());
+        rc = launch_tile_kernel(p->variant, A, p->n_tiles, s, grad, p->d_tile_order,
+                                p->d_tile_counter);
+    } else {
+        rc = launch_tile_kernel(p->variant, A, p->n_tiles, s, grad);
+    }
     if (rc) return rc;
     if (p->ev_tile1) CUDA_TRY(cudaEventRecord(p->ev_tile1, s));
     dim3 rg(p->n_bands, grad ? (out_stride + 127) / 128 : 1);

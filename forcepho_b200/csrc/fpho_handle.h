@@ -32,13 +32,20 @@ struct fpho_patch {
     fpho_psfgauss *d_psfgauss = nullptr;
     int *d_exp_band = nullptr, *d_exp_npsf = nullptr, *d_gauss_start = nullptr;
     fpho_patch_struct *d_struct = nullptr;
-    // tile plan (host copy of the tile list kept for batching)
-    int variant = 0, live_cap = 512, n_tiles = 0;
+    // tile plan (host copy of the tile list kept for batching); the default
+    // configuration is variant 3 (64 threads x 4 pixels), 192 records per
+    // shared-memory stage, persistent schedule -- the fastest measured on the
+    // 20-source, 8-band x 4-exposure, 128x128 px patch
+    int variant = 3, live_cap = 192, n_tiles = 0;
     std::vector<fpho::TileDesc> h_tiles;
     std::vector<int> tile_band_start;
     fpho::TileDesc *d_tiles = nullptr;
     float4 *d_tbox_all = nullptr, *d_tbox_w = nullptr;
     int *d_tile_band_start = nullptr;
+    // tile scheduling: 0 = one CTA per tile (hardware order), 1 = persistent
+    // CTAs taking tiles by decreasing cost of the previous evaluation
+    int schedule = 1;
+    int *d_tile_cost = nullptr, *d_tile_order = nullptr, *d_tile_counter = nullptr;
     // workspace
     float *d_gtab = nullptr;
     float4 *d_gbox = nullptr;

@@ -22,8 +22,11 @@ int variant_count();
 int variant_tile_pixels(int v);
 int variant_threads(int v);
 size_t tile_smem_bytes(int variant, int live_cap, int idx_cap, int stride);
+int device_sms();  // SMs of the current device (cached)
+// One CTA per tile; or, with `order` and `counter` (both device pointers), the
+// persistent form taking tiles in that order (see order_tiles).
 int launch_tile_kernel(int variant, const TileArgs &A, int n_tiles, cudaStream_t stream,
-                       bool grad);
+                       bool grad, const int *order = nullptr, int *counter = nullptr);
 
 PatchView make_view(const fpho_patch *p);
 

@@ -55,6 +55,47 @@ static __global__ void tile_bboxes(PatchView pv, const TileDesc *tiles, float4 *
     }
 }
 
+// Work order for the persistent tile kernel: tiles by decreasing cost in the
+// previous evaluation (kept image Gaussians x pixels, written by the tile
+// body), approximately -- a counting sort into 64 equal-width buckets of
+// [0, max cost]; within a bucket the order is whatever the shared-memory
+// atomics give.  The result does not depend on the order, since every tile
+// writes its own partials and reduce_bands sums them in tile-index order.
+// One CTA of 1024 threads.  Also resets the work counter.
+static __global__ void __launch_bounds__(1024) order_tiles(const int *cost, int n_tiles, int *order,
+                                                           int *counter) {
+    constexpr int NB = 64;
+    __shared__ int hist[NB];
+    __shared__ int smax;
+    const int tid = threadIdx.x;
+    if (tid < NB) hist[tid] = 0;
+    if (tid == 0) {
+        smax = 0;
+        *counter = 0;
+    }
+    __syncthreads();
+    int m = 0;
+    for (int i = tid; i < n_tiles; i += blockDim.x) m = max(m, cost[i]);
+    for (int o = 16; o > 0; o >>= 1) m = max(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((tid & 31) == 0) atomicMax(&smax, m);
+    __syncthreads();
+    const long long span = (long long)smax + 1;
+    for (int i = tid; i < n_tiles; i += blockDim.x)
+        atomicAdd(&hist[NB - 1 - (int)((long long)cost[i] * NB / span)], 1);
+    __syncthreads();
+    if (tid == 0) {
+        int acc = 0;
+        for (int b = 0; b < NB; ++b) {
+            const int h = hist[b];
+            hist[b] = acc;
+            acc += h;
+        }
+    }
+    __syncthreads();
+    for (int i = tid; i < n_tiles; i += blockDim.x)
+        order[atomicAdd(&hist[NB - 1 - (int)((long long)cost[i] * NB / span)], 1)] = i;
+}
+
 // Sum tile partials per band in double.  grid (n_bands, ceil(out_stride/128)).
 static __global__ void reduce_bands(const int *tile_band_start, const double *pchi2,
                                     const float *pgrad, int stride, double *chi2_out,

@@ -41,6 +41,7 @@ struct TileArgs {
     int idx_cap;              // most image Gaussians of any exposure (kept-list capacity)
     int *err;                 // error word (bit 0: bulk-copy wait gave up)
     long long *pairs;         // optional: evaluated (pixel, Gaussian) pairs, or nullptr
+    int *tile_cost = nullptr; // optional: [n_tiles] kept Gaussians x pixels, written per tile
 };
 
 // ------------------------------------------------------------ mbarrier + bulk copy
@@ -512,6 +513,7 @@ __device__ __forceinline__ void tile_body(const TileArgs &A, int tile, unsigned 
         for (int w = 0; w < NW; ++w) v += wacc[w * stride + j];
         A.pgrad[(size_t)tile * stride + j] = v;
     }
+    if (A.tile_cost && tid == 0) A.tile_cost[tile] = n_live * td.count;
     if (A.pairs && tid == 0) atomicAdd(reinterpret_cast<unsigned long long *>(A.pairs),
                                        (unsigned long long)((long long)n_live * td.count));
 }

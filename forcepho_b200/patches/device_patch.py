@@ -50,6 +50,10 @@ class DevicePatch:
     def set_config(self, variant, live_cap, stream=None):
         _lib.call("fpho_patch_set_config", self.handle, int(variant), int(live_cap), stream)
 
+    def set_schedule(self, schedule):
+        """0: one CTA per tile; 1: persistent CTAs, costliest tiles first."""
+        _lib.call("fpho_patch_set_schedule", self.handle, int(schedule))
+
     def free(self):
         if getattr(self, "handle", None):
             _lib.lib.fpho_patch_free(self.handle)

@@ -299,8 +299,16 @@ FPHO_API int fpho_variant_info(int variant, int out[2]);
 
 /* Select the tile-kernel variant and the shared-memory stage size (image
  * Gaussians per chunk) used by this patch; re-plans the tiles if the tile
- * size changes. */
+ * size changes.  Default: variant 3 (64 threads x 4 pixels), live_cap 192. */
 FPHO_API int fpho_patch_set_config(fpho_patch *p, int variant, int live_cap, void *stream);
+
+/* Tile scheduling of this patch: 0 = one CTA per tile; 1 (default) = as many
+ * persistent CTAs as fit on the GPU, taking tiles in decreasing order of
+ * their cost in the previous evaluation (kept image Gaussians x pixels);
+ * patches of at most 4 tiles per SM always run one CTA per tile.
+ * Results are identical either way.  No reference counterpart (the
+ * reference launches one block per band). */
+FPHO_API int fpho_patch_set_schedule(fpho_patch *p, int schedule);
 
 /* Enable counting of evaluated (pixel, image Gaussian) pairs, i.e. pairs that
  * survive the per-tile culling; *last_count receives the count of the last

@@ -241,3 +241,40 @@ def test_image_gaussians_bitexact(name):
             n_total += got.size
     P.free()
     assert n_exact == n_total
+
+
+@pytest.mark.parametrize("variant", [3, 6, 0])
+def test_persistent_schedule_identical(variant):
+    """The persistent schedule (tiles taken by decreasing cost of the previous
+    evaluation, through an atomic counter) gives bit-identical chi2 and
+    gradients to one CTA per tile -- on the first evaluation (no costs yet)
+    and on later ones, with the proposal changing in between."""
+    import torch
+    from forcepho_b200 import _lib, synth
+    P = synth.make_config(1, seed=5)
+    P.send_to_device()
+    h = P.device_patch.handle
+    nb, ns = P.n_bands, P.n_sources
+    props = [P.proposal(), P.truth_proposal(), P.proposal()]
+    c = torch.zeros(nb, dtype=torch.float64, device="cuda")
+    g = torch.zeros(nb * ns * 7, dtype=torch.float32, device="cuda")
+    s = torch.cuda.current_stream().cuda_stream
+    out = {}
+    for sched in (0, 1):
+        P.device_patch.set_config(variant, 192)
+        P.device_patch.set_schedule(sched)
+        res = []
+        for q in props:
+            dq = torch.from_numpy(q.view(np.uint8).copy()).cuda()
+            _lib.call("fpho_evaluate_proposal", h, dq.data_ptr(), ns, c.data_ptr(), g.data_ptr(),
+                      7 * ns, 0, s)
+            torch.cuda.synchronize()
+            res.append((c.clone(), g.clone()))
+        out[sched] = res
+    for (c0, g0), (c1, g1) in zip(out[0], out[1]):
+        assert torch.equal(c0, c1)
+        assert torch.equal(g0, g1)
+    w = ctypes.c_int()
+    _lib.call("fpho_patch_error_word", h, ctypes.byref(w))
+    assert w.value == 0
+    P.free()
