@@ -40,6 +40,10 @@ sys.path.insert(0, ROOT)
 METRIC = "chi2+grad evals/s & pix·gauss/s: batched vs plain, 1 B200, rel err ≤1e-6"
 FLOPS_PER_PAIR = 105          # 18 (model) + 87 (gradient) FP32 flops, FMA = 2
 WORKLOAD = "config1: 20 src, 8 bands x 4 exp x 128x128 px, 5-gauss PSF, 9 radii"
+# DRAM bytes (read + write) of one tile-kernel launch on this workload, from an
+# ncu capture (profiles/tile_kernel_dyn_64x4_config1.md): the 16 B per pixel
+# of the pixel arrays plus the image-Gaussian table, each read once.
+TILE_TRAFFIC_BYTES = 12658688
 
 
 def parse():
@@ -235,6 +239,14 @@ def batched_leg(args, torch, lib, steps):
     for _ in range(3):
         graph.replay()
     ms_batched = timed(graph.replay, steps)
+    batch.time_tiles(True)
+    tile_ms = []
+    for _ in range(min(steps, 10)):
+        flush.zero_()
+        batch.evaluate_device(dprop, chi2, dchi2)
+        tile_ms.append(batch.last_tile_ms())
+    batch.time_tiles(False)
+    tile_ms = float(np.median(tile_ms))
 
     # plain: one launch sequence per patch, device buffers per patch
     bufs = []
@@ -262,6 +274,9 @@ def batched_leg(args, torch, lib, steps):
            "plain_patch_evals_per_s": n / (ms_plain * 1e-3),
            "batched_pix_gauss_per_s": nominal / (ms_batched * 1e-3),
            "speedup_batched_vs_plain": ms_plain / ms_batched,
+           "roofline": {"kernel": "batch_tiles", "kernel_ms": tile_ms, "bound": "fp32",
+                        "achieved": evaluated * FLOPS_PER_PAIR / (tile_ms * 1e-3) / 1e12,
+                        "unit": "TFLOP/s"},
            "timing": "CUDA events per step, L2 flushed between steps; batched step replayed "
                      "from a CUDA graph"}
     del graph
@@ -506,6 +521,9 @@ def run_ours(args):
     batched = None
     if args.batch_patches > 0:
         batched = batched_leg(args, torch, _lib, steps=max(3, min(args.steps, 50)))
+        rb = batched["roofline"]
+        rb.update({"peak": fp32_tflops, "frac": rb["achieved"] / fp32_tflops,
+                   "peak_source": "measured live: packed FP32 FMA probe kernel"})
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -536,7 +554,9 @@ def run_ours(args):
             "gpu_launches": (4 if cfg.get("schedule", 0) == 1 else 3) * args.steps,
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_tflops,
                          "unit": "TFLOP/s", "frac": achieved / fp32_tflops,
-                         "traffic": None,
+                         "traffic": TILE_TRAFFIC_BYTES,
+                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum "
+                                           "of one launch, profiles/tile_kernel_dyn_64x4_config1.md",
                          "peak_source": "measured live: packed FP32 FMA probe kernel",
                          "kernel": "tile_kernel", "kernel_ms": tile_s * 1e3,
                          "sfu_gops": sfu, "sfu_peak_gops": ex2_gops, "sfu_frac": sfu / ex2_gops},

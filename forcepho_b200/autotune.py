@@ -22,8 +22,8 @@ from . import _lib
 CACHE = os.environ.get("FPHO_AUTOTUNE_CACHE",
                        os.path.join(os.path.expanduser("~"), ".cache", "forcepho_b200",
                                     "autotune.json"))
-DEFAULT = {"variant": 3, "live_cap": 192, "schedule": 1}   # 64 threads x 4 pixels
-LIVE_CAPS = (96, 128, 192, 256, 384)
+DEFAULT = {"variant": 3, "live_cap": 160, "schedule": 1}   # 64 threads x 4 pixels
+LIVE_CAPS = (96, 128, 160, 192, 256, 384)
 SCHEDULES = (0, 1)
 
 

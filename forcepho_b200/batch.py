@@ -104,6 +104,16 @@ class PatchBatch:
             self.evaluate_device(dprop, chi2, dchi2)
         return g
 
+    def time_tiles(self, enable=True):
+        """Record CUDA events around the persistent tile launch."""
+        _lib.call("fpho_batch_time_tiles", self.handle, int(enable))
+
+    def last_tile_ms(self):
+        """Milliseconds of the last timed tile launch (synchronizes on it)."""
+        t = ctypes.c_float()
+        _lib.call("fpho_batch_last_tile_ms", self.handle, ctypes.byref(t))
+        return float(t.value)
+
     def count_pairs(self, enable=True):
         c = ctypes.c_longlong()
         _lib.call("fpho_batch_count_pairs", self.handle, int(enable), ctypes.byref(c))

@@ -136,9 +136,15 @@ __device__ __forceinline__ int reduce7_index(int lane) {
 // Dynamic shared memory of the tile kernel:
 //   [records live_cap x 128 B][kept indices idx_cap x 4 B][kept flags idx_cap x 4 B]
 //   [per-warp source sums NW x stride x 4 B]
+// Shared memory of one tile CTA: `live_cap` staged image-Gaussian records of
+// GSTAGE floats, the kept list (one int per Gaussian of the exposure: local
+// index << 2 | flags) and per-warp gradient sums.  (Reading the Jacobian half
+// of the records from global memory instead halves the stage, but the
+// exposure's records then miss L1 in the gradient epilogue; measured slower.)
+constexpr int GSTAGE = GREC;
 __host__ __device__ inline size_t tile_smem_layout_bytes(int nw, int live_cap, int idx_cap,
                                                          int stride) {
-    return (size_t)live_cap * GREC * 4 + (size_t)idx_cap * 8 + (size_t)nw * stride * 4;
+    return (size_t)live_cap * GSTAGE * 4 + (size_t)idx_cap * 4 + (size_t)nw * stride * 4;
 }
 
 // ------------------------------------------------------------ culling
@@ -263,7 +269,7 @@ __device__ __forceinline__ float lanesum(v2 v) {
     return a + b;
 }
 
-// live_flag bits
+// kept-list flag bits (the low two bits of each entry)
 constexpr int FLAG_CUT = 1;        // the exp-argument can exceed 36 inside the tile
 constexpr int FLAG_LAST_SRC = 2;   // last kept Gaussian of its source in the chunk
 
@@ -281,9 +287,9 @@ __device__ __forceinline__ void tile_body(const TileArgs &A, int tile, unsigned 
     const int stride = A.pgrad_stride;
 
     float *recs = reinterpret_cast<float *>(smem);
-    int *live_idx = reinterpret_cast<int *>(smem + (size_t)cap * GREC * 4);
-    int *live_flag = live_idx + A.idx_cap;
-    float *wacc = reinterpret_cast<float *>(live_flag + A.idx_cap);
+    // kept list: exposure-local Gaussian index << 2 | FLAG_* bits
+    int *kept = reinterpret_cast<int *>(smem + (size_t)cap * GSTAGE * 4);
+    float *wacc = reinterpret_cast<float *>(kept + A.idx_cap);
 
     __shared__ int s_cnt[NW];
     __shared__ double s_chi2[NW];
@@ -360,17 +366,16 @@ __device__ __forceinline__ void tile_body(const TileArgs &A, int tile, unsigned 
         }
         if (live) {
             const int at = n_live + off + __popc(ball & ((1u << lane) - 1u));
-            live_idx[at] = idx;
-            live_flag[at] = flag;
+            kept[at] = ((idx - g0) << 2) | flag;
         }
         n_live += tot;
         __syncthreads();
     }
     // last kept Gaussian of each source (sources are contiguous in the list)
     for (int i = tid; i < n_live; i += NT) {
-        const int src = (live_idx[i] - g0) / npsf;
-        const int nxt = (i + 1 < n_live) ? (live_idx[i + 1] - g0) / npsf : -1;
-        if (nxt != src) live_flag[i] |= FLAG_LAST_SRC;
+        const int src = (kept[i] >> 2) / npsf;
+        const int nxt = (i + 1 < n_live) ? (kept[i + 1] >> 2) / npsf : -1;
+        if (nxt != src) kept[i] |= FLAG_LAST_SRC;
     }
     if (any_w) s_any_weight = 1;
     __syncthreads();
@@ -380,11 +385,11 @@ __device__ __forceinline__ void tile_body(const TileArgs &A, int tile, unsigned 
     auto stage = [&](int c0, int n) {
         fence_proxy_async_smem();
         if (warp == 0) {
-            if (lane == 0) mbar_arrive_expect_tx(mbar, (uint32_t)n * GREC * 4);
+            if (lane == 0) mbar_arrive_expect_tx(mbar, (uint32_t)n * GSTAGE * 4);
             __syncwarp();
             for (int i = lane; i < n; i += 32)
-                bulk_g2s(recs + (size_t)i * GREC, A.gtab + (size_t)live_idx[c0 + i] * GREC,
-                         GREC * 4, mbar);
+                bulk_g2s(recs + (size_t)i * GSTAGE,
+                         A.gtab + (size_t)(g0 + (kept[c0 + i] >> 2)) * GREC, GSTAGE * 4, mbar);
         }
         mbar_wait_bounded(mbar, phase, A.err);
         phase ^= 1u;
@@ -400,14 +405,14 @@ __device__ __forceinline__ void tile_body(const TileArgs &A, int tile, unsigned 
         if (c > 0) __syncthreads();  // previous chunk fully consumed
         stage(c0, n);
         for (int i = 0; i < n; ++i) {
-            const float *r = recs + (size_t)i * GREC;
+            const float *r = recs + (size_t)i * GSTAGE;
             v2 NXC, NYC, FXX, FXY, FYY, AMP, HB, C0;
             ld2(r + R_NXC, NXC, NYC);
             ld2(r + R_FXX, FXX, FXY);
             ld2(r + R_FYY, FYY, AMP);
             ld2(r + R_HB, HB, C0);
             const v2 HA = mul2(AMP, CM24);
-            if (live_flag[c0 + i] & FLAG_CUT)
+            if (kept[c0 + i] & FLAG_CUT)
                 residual_pairs<KP, true>(X, Y, R, NXC, NYC, FXX, FXY, FYY, HA, HB, KEXP2, KEXPLO2);
             else
                 residual_pairs<KP, false>(X, Y, R, NXC, NYC, FXX, FXY, FYY, HA, HB, KEXP2, KEXPLO2);
@@ -450,13 +455,14 @@ __device__ __forceinline__ void tile_body(const TileArgs &A, int tile, unsigned 
                 stage(c0, n);
             }
             for (int i = 0; i < n; ++i) {
-                const float *r = recs + (size_t)i * GREC;
+                const float *r = recs + (size_t)i * GSTAGE;
                 v2 NXC, NYC, FXX, FXY, FYY, AMP, HB, C0;
                 ld2(r + R_NXC, NXC, NYC);
                 ld2(r + R_FXX, FXX, FXY);
                 ld2(r + R_FYY, FYY, AMP);
                 ld2(r + R_HB, HB, C0);
-                const int flag = live_flag[c0 + i];
+                const int flag = kept[c0 + i];
+                const float4 *rj = reinterpret_cast<const float4 *>(r + R_JA_FLUX);
                 GradSums s;
                 if (flag & FLAG_CUT)
                     gradient_pairs<KP, true>(X, Y, R2, NXC, NYC, FXX, FXY, FYY, C0, C24, KEXP2, s);
@@ -474,10 +480,7 @@ __device__ __forceinline__ void tile_body(const TileArgs &A, int tile, unsigned 
                 const float gfyy = lanesum(s.T2) * (1.0f / 12.0f) - 0.5f * lanesum(s.HYY) -
                                    sW * (1.0f / 24.0f);
                 const float gfxy = lanesum(s.T3) * (1.0f / 12.0f) - lanesum(s.HXY);
-                const float4 j0 = *reinterpret_cast<const float4 *>(r + 16);
-                const float4 j1 = *reinterpret_cast<const float4 *>(r + 20);
-                const float4 j2 = *reinterpret_cast<const float4 *>(r + 24);
-                const float4 j3 = *reinterpret_cast<const float4 *>(r + 28);
+                const float4 j0 = rj[0], j1 = rj[1], j2 = rj[2], j3 = rj[3];
                 P[0] = fmaf(j0.x, gA, P[0]);
                 P[1] = fmaf(j1.z, gy, fmaf(j1.y, gx, P[1]));
                 P[2] = fmaf(j2.x, gy, fmaf(j1.w, gx, P[2]));

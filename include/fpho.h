@@ -299,7 +299,7 @@ FPHO_API int fpho_variant_info(int variant, int out[2]);
 
 /* Select the tile-kernel variant and the shared-memory stage size (image
  * Gaussians per chunk) used by this patch; re-plans the tiles if the tile
- * size changes.  Default: variant 3 (64 threads x 4 pixels), live_cap 192. */
+ * size changes.  Default: variant 3 (64 threads x 4 pixels), live_cap 160. */
 FPHO_API int fpho_patch_set_config(fpho_patch *p, int variant, int live_cap, void *stream);
 
 /* Tile scheduling of this patch: 0 = one CTA per tile; 1 (default) = as many
