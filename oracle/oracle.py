@@ -196,6 +196,28 @@ def _patch_payload(patch):
             int(patch.n_sources), int(patch.n_radii))
 
 
+def patch_payload_file(patch, path):
+    """Write the patch arrays to `path` (.npz) once, so that worker jobs can
+    name the file instead of pickling the arrays with every job."""
+    arrays, ns, nr = _patch_payload(patch)
+    np.savez(path, n_sources=ns, n_radii=nr, **arrays)
+    return path
+
+
+_payload_cache = {}
+
+
+def _resolve(payload):
+    if not isinstance(payload, str):
+        return payload
+    if payload not in _payload_cache:
+        d = np.load(payload)
+        arrays = {k: np.ascontiguousarray(d[k]) for k in PATCH_ARRAYS}
+        _payload_cache.clear()
+        _payload_cache[payload] = (arrays, int(d["n_sources"]), int(d["n_radii"]))
+    return _payload_cache[payload]
+
+
 _worker = {}
 
 
@@ -208,7 +230,7 @@ def _worker_init(ms64, root):
 
 def _worker_eval(payload, proposal, band, reps=1):
     import time
-    arrays, ns, nr = payload
+    arrays, ns, nr = _resolve(payload)
     st = _struct_from_arrays(arrays, ns, nr)
     prop = np.ascontiguousarray(proposal)
     maxsrc = 64 if _worker["ms64"] else 30
@@ -286,7 +308,7 @@ def _worker_mixed_abs(payload, proposal, band):
         L.fpo_evaluate_band_mixed_abs.argtypes = [ip, vp, vp, ip, vp, vp, vp, vp, vp]
         L.fpo_evaluate_band_mixed_abs.restype = ip
         L._mixed_abs_bound = True
-    arrays, ns, nr = payload
+    arrays, ns, nr = _resolve(payload)
     st = _struct_from_arrays(arrays, ns, nr)
     prop = np.ascontiguousarray(proposal)
     c = ctypes.c_double(0.0)
@@ -309,19 +331,20 @@ def oracle_pool(processes):
     return ctx.Pool(processes, initializer=_oracle_init, initargs=(os.path.dirname(HERE),))
 
 
-def mixed_abs_many(patch, jobs, pool):
-    """Mixed-oracle (chi2, dchi2, dabs) for a list of (proposal, band) jobs,
-    spread over `pool` (see oracle_pool)."""
-    payload = _patch_payload(patch)
+def mixed_abs_many(patch, jobs, pool, payload=None):
+    """Mixed-oracle (band, chi2, dchi2, dabs, dterm, dres) for a list of
+    (proposal, band) jobs, spread over `pool` (see oracle_pool)."""
+    payload = payload or _patch_payload(patch)
     return pool.starmap(_worker_mixed_abs, [(payload, np.ascontiguousarray(p), b)
                                             for p, b in jobs])
 
 
 def _worker_f64(payload, proposal, band, amps=None):
-    """(band, chi2) of the all-FP64 oracle for one band, in a worker process;
-    `amps` (n_sources, 10) float64 replaces the proposal's float amplitudes."""
+    """(band, chi2, dchi2 (n_src, 7)) of the all-FP64 oracle for one band, in a
+    worker process; `amps` (n_sources, 10) float64 replaces the proposal's
+    float amplitudes."""
     L = lib()
-    arrays, ns, nr = payload
+    arrays, ns, nr = _resolve(payload)
     st = _struct_from_arrays(arrays, ns, nr)
     prop = np.ascontiguousarray(proposal)
     c = ctypes.c_double(0.0)
@@ -339,13 +362,18 @@ def _worker_f64(payload, proposal, band, amps=None):
                 g.ctypes.data)
     if rc != 0:
         raise MemoryError("oracle allocation failed")
-    return band, c.value
+    return band, c.value, g.reshape(ns, 7)
 
 
-def f64_chi2_many(patch, jobs, pool):
+def f64_chi2_many(patch, jobs, pool, payload=None):
     """All-FP64 chi2 for a list of (proposal, band[, amps]) jobs, spread over
-    `pool`."""
-    payload = _patch_payload(patch)
+    `pool` (`payload`: a patch_payload_file path, else the arrays are sent)."""
+    return [c for c, _ in f64_many(patch, jobs, pool, payload)]
+
+
+def f64_many(patch, jobs, pool, payload=None):
+    """All-FP64 (chi2, dchi2) for a list of (proposal, band[, amps]) jobs."""
+    payload = payload or _patch_payload(patch)
     args = [(payload, np.ascontiguousarray(j[0]), j[1], j[2] if len(j) > 2 else None)
             for j in jobs]
-    return [c for _, c in pool.starmap(_worker_f64, args)]
+    return [(c, g) for _, c, g in pool.starmap(_worker_f64, args)]

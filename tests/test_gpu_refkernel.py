@@ -1,0 +1,107 @@
+"""GPU: the reference's own CUDA kernel (oracle/_ref/librefgpu.so, compiled
+from forcepho/src/compute_gaussians_kernel.cu with the reference's options)
+on the device copy of a patch -- the GPU baseline of the benchmark.  Its
+float arithmetic (device expf, warp-shuffle and atomic reduction order)
+differs from the reference CPU kernel's, so it is compared with loose bars:
+chi2 relative error <= 1e-5, gradient components within 1e-3 relative or
+1e-5 of the band's largest component.  Recorded beside it: how far this
+project's kernel and the reference GPU kernel each are from the reference CPU
+kernel."""
+import numpy as np
+import pytest
+
+from conftest import load_golden
+from oracle import oracle as O
+from oracle import refgpu
+
+pytestmark = pytest.mark.gpu
+
+
+def _run_ref_gpu(P, prop):
+    import torch
+    from forcepho_b200 import _lib
+    nb, ns = P.n_bands, P.n_sources
+    P.send_to_device()
+    dstruct = P.device_patch.device_struct
+    dprop = torch.from_numpy(np.ascontiguousarray(prop).view(np.uint8).copy()).cuda()
+    chi2 = torch.zeros(nb, dtype=torch.float64, device="cuda")
+    resp = torch.zeros(nb * _lib.lib.fpho_sizeof(3) // 4, dtype=torch.float32, device="cuda")
+    refgpu.evaluate(dstruct, dprop.data_ptr(), chi2.data_ptr(), resp.data_ptr(), nb, ns,
+                    refgpu.max_gauss_band(P), torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    ms = refgpu.max_sources()
+    d = resp.cpu().numpy().reshape(nb, ms, 7)[:, :ns].astype(np.float64)
+    P.free()
+    return chi2.cpu().numpy(), d
+
+
+@pytest.mark.parametrize("name", ["config0_seed1", "mini_3src_2band"])
+def test_reference_gpu_kernel_runs(name):
+    if not refgpu.available():
+        pytest.skip("reference CUDA kernel not built")
+    P, prop, d = load_golden(name)
+    c_rg, g_rg = _run_ref_gpu(P, prop)
+    from test_gpu_parity import gpu_eval
+    c_us, g_us = gpu_eval(P, prop)
+    c_ref, g_ref = d["ref_chi2"], d["ref_dchi2"].astype(np.float64)
+    np.testing.assert_allclose(c_rg, c_ref, rtol=1e-5)
+    tol = np.maximum(1e-3 * np.abs(g_ref), 1e-5 * np.abs(g_ref).max(axis=(1, 2), keepdims=True))
+    assert np.all(np.abs(g_rg - g_ref) <= tol)
+    rel = lambda a, b: float(np.max(np.abs(a - b) / np.maximum(np.abs(b), 1e-300)))
+    print(f"{name}: vs reference CPU kernel -- chi2: reference GPU {rel(c_rg, c_ref):.2e}, "
+          f"ours {rel(c_us, c_ref):.2e}; gradient: reference GPU {rel(g_rg, g_ref):.2e}, "
+          f"ours {rel(g_us, g_ref):.2e}")
+
+
+def test_reference_gpu_kernel_timing_config1():
+    """Times the reference CUDA kernel against this project's kernel on the
+    20-source, 8-band x 4-exposure, 128x128 px patch (device-resident inputs,
+    CUDA events, L2 flushed between evaluations) and checks that the two agree
+    (chi2 within 1e-5)."""
+    if not refgpu.available():
+        pytest.skip("reference CUDA kernel not built")
+    import torch
+    from forcepho_b200 import _lib, synth
+    P = synth.make_config(1, seed=0, render=synth.render_model_gpu)
+    prop = P.proposal()
+    nb, ns = P.n_bands, P.n_sources
+    P.send_to_device()
+    dstruct = P.device_patch.device_struct
+    dprop = torch.from_numpy(prop.view(np.uint8).copy()).cuda()
+    c_rg = torch.zeros(nb, dtype=torch.float64, device="cuda")
+    resp = torch.zeros(nb * 210, dtype=torch.float32, device="cuda")
+    c_us = torch.zeros(nb, dtype=torch.float64, device="cuda")
+    g_us = torch.zeros(nb * ns * 7, dtype=torch.float32, device="cuda")
+    s = torch.cuda.current_stream()
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    mg = refgpu.max_gauss_band(P)
+
+    def ref_gpu():
+        refgpu.evaluate(dstruct, dprop.data_ptr(), c_rg.data_ptr(), resp.data_ptr(), nb, ns, mg,
+                        s.cuda_stream)
+
+    def ours():
+        _lib.call("fpho_evaluate_proposal", P.device_patch.handle, dprop.data_ptr(), ns,
+                  c_us.data_ptr(), g_us.data_ptr(), 7 * ns, 0, s.cuda_stream)
+
+    def timed(fn, n):
+        fn()
+        fn()
+        ts = []
+        for _ in range(n):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            fn()
+            e1.record(s)
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return float(np.median(ts))
+
+    t_ref = timed(ref_gpu, 5)
+    t_us = timed(ours, 20)
+    np.testing.assert_allclose(c_rg.cpu().numpy(), c_us.cpu().numpy(), rtol=1e-5)
+    print(f"config 1: reference CUDA kernel {t_ref:.3f} ms per evaluation "
+          f"({1e3 / t_ref:.1f} evals/s), this project's {t_us:.3f} ms ({1e3 / t_us:.1f} evals/s): "
+          f"{t_ref / t_us:.1f}x")
+    P.free()
