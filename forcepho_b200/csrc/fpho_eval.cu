@@ -104,15 +104,31 @@ __global__ void __launch_bounds__(NT) tile_kernel_dyn(TileArgs A, const int *ord
     }
 }
 
+// Unit-flux model rows of the design matrix, one CTA per tile.
+template <int NT, int K>
+__global__ void __launch_bounds__(NT) design_kernel(TileArgs A, float *X, long long npix) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ uint64_t mbar;
+    if (threadIdx.x == 0) {
+        mbar_init(&mbar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    uint32_t phase = 0;
+    design_body<NT, K>(A, blockIdx.x, smem, &mbar, phase, X, npix);
+}
+
 // ------------------------------------------------------------ variants
 struct Variant {
     int nt, k;
     const void *fn[2];   // [0] chi2 only, [1] chi2 + gradient
     const void *dyn[2];  // persistent forms of the same
+    const void *design;  // design-matrix rows with the same tile shape
 };
 #define FPHO_VARIANT(NT, K)                                                                      \
     {NT, K, {(const void *)tile_kernel<NT, K, false>, (const void *)tile_kernel<NT, K, true>},  \
-     {(const void *)tile_kernel_dyn<NT, K, false>, (const void *)tile_kernel_dyn<NT, K, true>}}
+     {(const void *)tile_kernel_dyn<NT, K, false>, (const void *)tile_kernel_dyn<NT, K, true>}, \
+     (const void *)design_kernel<NT, K>}
 static const Variant kVariants[] = {
     FPHO_VARIANT(128, 4), FPHO_VARIANT(128, 2), FPHO_VARIANT(256, 2), FPHO_VARIANT(64, 4),
     FPHO_VARIANT(256, 4), FPHO_VARIANT(128, 8), FPHO_VARIANT(64, 8),
@@ -185,6 +201,30 @@ int launch_tile_kernel(int variant, const TileArgs &A, int n_tiles, cudaStream_t
     const int grid = std::min(n_tiles, occ * sms);
     void *args[] = {(void *)&A, (void *)&order, (void *)&n_tiles, (void *)&counter};
     CUDA_TRY(cudaLaunchKernel(fn, dim3(grid), dim3(V.nt), args, smem, stream));
+    return FPHO_OK;
+}
+
+static std::mutex g_design_mu;
+static size_t g_design_set[64][kNumVariants];
+
+int launch_design_kernel(int variant, const TileArgs &A, int n_tiles, float *X, long long npix,
+                         cudaStream_t stream) {
+    if (n_tiles <= 0) return FPHO_OK;
+    const Variant &V = kVariants[variant];
+    const size_t smem = tile_smem_bytes(variant, A.live_cap, A.idx_cap, A.pgrad_stride);
+    int dev = 0;
+    CUDA_TRY(cudaGetDevice(&dev));
+    if (dev >= 64) return set_error(FPHO_ERR_LIMIT, "device ordinal %d >= 64", dev);
+    {
+        std::lock_guard<std::mutex> lk(g_design_mu);
+        if (g_design_set[dev][variant] < smem) {
+            CUDA_TRY(cudaFuncSetAttribute(V.design, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)smem));
+            g_design_set[dev][variant] = smem;
+        }
+    }
+    void *args[] = {(void *)&A, (void *)&X, (void *)&npix};
+    CUDA_TRY(cudaLaunchKernel(V.design, dim3(n_tiles), dim3(V.nt), args, smem, stream));
     return FPHO_OK;
 }
 
@@ -735,6 +775,41 @@ extern "C" int fpho_EvaluateProposal(fpho_patch *p, const void *dev_patch_struct
     return enqueue_evaluate(p, (const fpho_source *)dev_proposal, (double *)pchi2,
                             (float *)pdchi2_dp, FPHO_MAXSOURCES * FPHO_NPARAMS,
                             p->d_residual != nullptr, (cudaStream_t)stream, true);
+}
+
+extern "C" int fpho_patch_design_matrix(fpho_patch *p, const void *dev_proposal,
+                                        int n_sources, float *dev_X, void *stream) {
+    clear_error();
+    if (!p || !dev_proposal || !dev_X) return set_error(FPHO_ERR_INVALID, "NULL argument");
+    if (n_sources != p->n_sources)
+        return set_error(FPHO_ERR_INVALID, "n_sources=%d but the patch has %d", n_sources,
+                         p->n_sources);
+    cudaStream_t s = (cudaStream_t)stream;
+    CUDA_TRY(cudaMemsetAsync(dev_X, 0, sizeof(float) * (size_t)n_sources * p->npix, s));
+    CUDA_TRY(cudaMemsetAsync(p->d_err, 0, sizeof(int), s));
+    const PatchView pv = make_view(p);
+    if (p->max_g > 0) {
+        dim3 grid((p->max_g + 127) / 128, p->n_exp);
+        build_image_gaussians<<<grid, 128, 0, s>>>(
+            pv, static_cast<const fpho_source *>(dev_proposal), p->d_gtab, p->d_gbox);
+        CUDA_TRY(cudaGetLastError());
+    }
+    TileArgs A;
+    A.pv = pv;
+    A.tiles = p->d_tiles;
+    A.tbox_all = p->d_tbox_all;
+    A.tbox_w = p->d_tbox_w;
+    A.gtab = p->d_gtab;
+    A.gbox = p->d_gbox;
+    A.pchi2 = p->d_pchi2;
+    A.pgrad = p->d_pgrad;
+    A.pgrad_stride = 7 * p->n_sources;
+    A.want_residual = 1;
+    A.live_cap = p->live_cap;
+    A.idx_cap = std::max(p->max_g, 1);
+    A.err = p->d_err;
+    A.pairs = nullptr;
+    return launch_design_kernel(p->variant, A, p->n_tiles, dev_X, (long long)p->npix, s);
 }
 
 extern "C" int fpho_patch_image_gaussians(fpho_patch *p, int exposure, float *host_out,

@@ -273,6 +273,68 @@ __device__ __forceinline__ float lanesum(v2 v) {
 constexpr int FLAG_CUT = 1;        // the exp-argument can exceed 36 inside the tile
 constexpr int FLAG_LAST_SRC = 2;   // last kept Gaussian of its source in the chunk
 
+// ------------------------------------------------------------ tile scan
+// One scan of the exposure's image Gaussians [g0, g1): the ordered list of
+// those that can reach the tile (box overlap, then the exact minimum of the
+// exp-argument over the tile box `bb`), each entry (local index << 2 | flags)
+// with FLAG_CUT when the exp-argument can exceed 36 inside the tile (its
+// maximum over the box is at a corner) and FLAG_LAST_SRC on the last kept
+// Gaussian of each source.  Returns the number kept; ends with the list
+// visible to the whole CTA.
+template <int NT>
+__device__ __forceinline__ int scan_tile(const TileArgs &A, float4 bb, int g0, int g1, int npsf,
+                                         int *kept, int *s_cnt) {
+    constexpr int NW = NT / 32;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    int n_live = 0;
+    for (int base = g0; base < g1; base += NT) {
+        const int idx = base + tid;
+        bool live = false;
+        int flag = 0;
+        if (idx < g1) {
+            const float4 gb = A.gbox[idx];
+            live = !(gb.y < bb.x || gb.x > bb.y || gb.w < bb.z || gb.z > bb.w);
+            if (live) {
+                const float *r = A.gtab + (size_t)idx * GREC;
+                live = keeps_tile(r, bb);
+                const float nxc = r[R_NXC], nyc = r[R_NYC];
+                const float fxx = r[R_FXX], fxy = r[R_FXY], fyy = r[R_FYY];
+                float qmax = 0.0f;
+#pragma unroll
+                for (int c = 0; c < 4; ++c) {
+                    const float dx = ((c & 1) ? bb.y : bb.x) + nxc;
+                    const float dy = ((c & 2) ? bb.w : bb.z) + nyc;
+                    qmax = fmaxf(qmax, dx * (fxx * dx + fxy * dy) + dy * (fyy * dy + fxy * dx));
+                }
+                flag = (qmax * (1.0f + CULL_REL) + CULL_ABS >= FPHO_MAX_EXP_ARG) ? FLAG_CUT : 0;
+            }
+        }
+        const unsigned ball = __ballot_sync(0xffffffffu, live);
+        if (lane == 0) s_cnt[warp] = __popc(ball);
+        __syncthreads();
+        int off = 0, tot = 0;
+#pragma unroll
+        for (int w = 0; w < NW; ++w) {
+            off += (w < warp) ? s_cnt[w] : 0;
+            tot += s_cnt[w];
+        }
+        if (live) {
+            const int at = n_live + off + __popc(ball & ((1u << lane) - 1u));
+            kept[at] = ((idx - g0) << 2) | flag;
+        }
+        n_live += tot;
+        __syncthreads();
+    }
+    // last kept Gaussian of each source (sources are contiguous in the list)
+    for (int i = tid; i < n_live; i += NT) {
+        const int src = (kept[i] >> 2) / npsf;
+        const int nxt = (i + 1 < n_live) ? (kept[i + 1] >> 2) / npsf : -1;
+        if (nxt != src) kept[i] |= FLAG_LAST_SRC;
+    }
+    __syncthreads();
+    return n_live;
+}
+
 // ------------------------------------------------------------ the tile body
 // GRAD = false runs the residual pass and chi2 only (no gradient pass, no
 // gradient partials written).
@@ -328,55 +390,8 @@ __device__ __forceinline__ void tile_body(const TileArgs &A, int tile, unsigned 
     }
     if (tid == 0) s_any_weight = 0;
 
-    // ---- scan once: the ordered list of the exposure's image Gaussians that
-    // can reach the tile (box overlap, then the exact minimum of the
-    // exp-argument over the tile), with a flag when the exp-argument can
-    // exceed 36 inside the tile (its maximum over the box is at a corner).
-    int n_live = 0;
-    for (int base = g0; base < g1; base += NT) {
-        const int idx = base + tid;
-        bool live = false;
-        int flag = 0;
-        if (idx < g1) {
-            const float4 gb = A.gbox[idx];
-            live = !(gb.y < bb.x || gb.x > bb.y || gb.w < bb.z || gb.z > bb.w);
-            if (live) {
-                const float *r = A.gtab + (size_t)idx * GREC;
-                live = keeps_tile(r, bb);
-                const float nxc = r[R_NXC], nyc = r[R_NYC];
-                const float fxx = r[R_FXX], fxy = r[R_FXY], fyy = r[R_FYY];
-                float qmax = 0.0f;
-#pragma unroll
-                for (int c = 0; c < 4; ++c) {
-                    const float dx = ((c & 1) ? bb.y : bb.x) + nxc;
-                    const float dy = ((c & 2) ? bb.w : bb.z) + nyc;
-                    qmax = fmaxf(qmax, dx * (fxx * dx + fxy * dy) + dy * (fyy * dy + fxy * dx));
-                }
-                flag = (qmax * (1.0f + CULL_REL) + CULL_ABS >= FPHO_MAX_EXP_ARG) ? FLAG_CUT : 0;
-            }
-        }
-        const unsigned ball = __ballot_sync(0xffffffffu, live);
-        if (lane == 0) s_cnt[warp] = __popc(ball);
-        __syncthreads();
-        int off = 0, tot = 0;
-#pragma unroll
-        for (int w = 0; w < NW; ++w) {
-            off += (w < warp) ? s_cnt[w] : 0;
-            tot += s_cnt[w];
-        }
-        if (live) {
-            const int at = n_live + off + __popc(ball & ((1u << lane) - 1u));
-            kept[at] = ((idx - g0) << 2) | flag;
-        }
-        n_live += tot;
-        __syncthreads();
-    }
-    // last kept Gaussian of each source (sources are contiguous in the list)
-    for (int i = tid; i < n_live; i += NT) {
-        const int src = (kept[i] >> 2) / npsf;
-        const int nxt = (i + 1 < n_live) ? (kept[i + 1] >> 2) / npsf : -1;
-        if (nxt != src) kept[i] |= FLAG_LAST_SRC;
-    }
+    // ---- the ordered list of kept image Gaussians
+    const int n_live = scan_tile<NT>(A, bb, g0, g1, npsf, kept, s_cnt);
     if (any_w) s_any_weight = 1;
     __syncthreads();
     const bool tile_has_weight = s_any_weight != 0;
@@ -519,6 +534,96 @@ __device__ __forceinline__ void tile_body(const TileArgs &A, int tile, unsigned 
     if (A.tile_cost && tid == 0) A.tile_cost[tile] = n_live * td.count;
     if (A.pairs && tid == 0) atomicAdd(reinterpret_cast<unsigned long long *>(A.pairs),
                                        (unsigned long long)((long long)n_live * td.count));
+}
+
+// ------------------------------------------------------------ design rows
+// The unit-flux model of every source at every pixel of the tile:
+// X[src][pix] = sum over the source's image Gaussians of dA/dflux * G * H
+// (dA/dflux = the record's R_JA_FLUX; with the source's flux this is its model
+// divided by the flux, as the reference's design matrix,
+// forcepho/patches/device_patch.py:198-238).  Same scan, staging and
+// exponential as the residual pass; X must be zero on entry, and every
+// (src, pixel) is written by one thread only.
+template <int NT, int K>
+__device__ __forceinline__ void design_body(const TileArgs &A, int tile, unsigned char *smem,
+                                            uint64_t *mbar, uint32_t &phase, float *X,
+                                            long long npix) {
+    static_assert(K % 2 == 0, "pixels per thread must be even (packed pairs)");
+    constexpr int NW = NT / 32;
+    constexpr int KP = K / 2;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int cap = A.live_cap;
+    float *recs = reinterpret_cast<float *>(smem);
+    int *kept = reinterpret_cast<int *>(smem + (size_t)cap * GSTAGE * 4);
+    __shared__ int s_cnt[NW];
+
+    const TileDesc td = A.tiles[tile];
+    const float4 bb = A.tbox_all[tile];
+    const int g0 = A.pv.gauss_start[td.exposure];
+    const int g1 = A.pv.gauss_start[td.exposure + 1];
+    const int npsf = A.pv.exp_npsf[td.exposure];
+    const float xmid = 0.5f * (bb.x + bb.y), ymid = 0.5f * (bb.z + bb.w);
+    v2 Xp[KP], Yp[KP], M[KP];
+#pragma unroll
+    for (int j = 0; j < KP; ++j) {
+        float xs[2], ys[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int li = tid + (2 * j + h) * NT;
+            const bool ok = li < td.count;
+            const int pix = td.pix_begin + (ok ? li : 0);
+            xs[h] = ok ? A.pv.xpix[pix] : xmid;
+            ys[h] = ok ? A.pv.ypix[pix] : ymid;
+        }
+        Xp[j] = pk(xs[0], xs[1]);
+        Yp[j] = pk(ys[0], ys[1]);
+        M[j] = 0ull;
+    }
+    const int n_live = scan_tile<NT>(A, bb, g0, g1, npsf, kept, s_cnt);
+    const v2 KEXP2 = pk1(KEXP), KEXPLO2 = pk1(KEXP_LO), CM24 = pk1(-1.0f / 24.0f);
+    for (int c0 = 0; c0 < n_live; c0 += cap) {
+        const int n = min(cap, n_live - c0);
+        if (c0 > 0) __syncthreads();
+        fence_proxy_async_smem();
+        if (warp == 0) {
+            if (lane == 0) mbar_arrive_expect_tx(mbar, (uint32_t)n * GSTAGE * 4);
+            __syncwarp();
+            for (int i = lane; i < n; i += 32)
+                bulk_g2s(recs + (size_t)i * GSTAGE,
+                         A.gtab + (size_t)(g0 + (kept[c0 + i] >> 2)) * GREC, GSTAGE * 4, mbar);
+        }
+        mbar_wait_bounded(mbar, phase, A.err);
+        phase ^= 1u;
+        for (int i = 0; i < n; ++i) {
+            const float *r = recs + (size_t)i * GSTAGE;
+            v2 NXC, NYC, FXX, FXY, FYY, AMP, HB, C0;
+            ld2(r + R_NXC, NXC, NYC);
+            ld2(r + R_FXX, FXX, FXY);
+            ld2(r + R_FYY, FYY, AMP);
+            ld2(r + R_HB, HB, C0);
+            const v2 UA = pk1(r[R_JA_FLUX]);  // dA/dflux in place of amp
+            const v2 HA = mul2(UA, CM24);
+            const v2 UB = mul2(pk1(-1.0f), mul2(UA, C0));
+            const int flag = kept[c0 + i];
+            if (flag & FLAG_CUT)
+                residual_pairs<KP, true>(Xp, Yp, M, NXC, NYC, FXX, FXY, FYY, HA, UB, KEXP2, KEXPLO2);
+            else
+                residual_pairs<KP, false>(Xp, Yp, M, NXC, NYC, FXX, FXY, FYY, HA, UB, KEXP2, KEXPLO2);
+            if ((flag & FLAG_LAST_SRC) || i == n - 1) {
+                const int src = __float_as_int(r[R_SRC]);
+                float *row = X + (size_t)src * npix + td.pix_begin;
+#pragma unroll
+                for (int j = 0; j < KP; ++j) {
+                    float m0, m1;
+                    unpk(M[j], m0, m1);  // accumulated -model
+                    const int l0 = tid + 2 * j * NT, l1 = l0 + NT;
+                    if (l0 < td.count) row[l0] -= m0;
+                    if (l1 < td.count) row[l1] -= m1;
+                    M[j] = 0ull;
+                }
+            }
+        }
+    }
 }
 
 }  // namespace fpho

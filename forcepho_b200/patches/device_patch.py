@@ -67,13 +67,82 @@ class DevicePatch:
 
 
 class DevicePatchMixin:
-    """Methods shared by device mixins (forcepho/patches/device_patch.py:23-257)."""
+    """Methods shared by device mixins (forcepho/patches/device_patch.py:23-257).
+
+    ``subtract_fixed`` and ``design_matrix`` need the patch class to provide
+    ``set_scene(catalog)`` and ``pack_meta(scene)`` (the reference's
+    JadesPatch does; :class:`forcepho_b200.synth.SyntheticPatch` does for its
+    own sources)."""
 
     def get_proposer(self):
         raise NotImplementedError
 
     def send_to_device(self):
         raise NotImplementedError
+
+    def subtract_fixed(self, fixed, active=None, big=None, maxactive=15, swap_local=False,
+                       big_scene_kwargs={}, **scene_kwargs):
+        """Subtract fixed (and big) sources from the device data, block by block
+        of at most `maxactive` sources, leaving the residual as the device data
+        and the metadata of `active` (or of the last block) installed; returns
+        (proposer, scene of the installed metadata).  As the reference's
+        ``subtract_fixed`` (device_patch.py:113-191)."""
+        scenes = []
+        if big is not None:
+            inds = np.arange(maxactive, len(big), maxactive)
+            scenes.extend([self.set_scene(b, **big_scene_kwargs)
+                           for b in np.array_split(np.asarray(big), inds)])
+        if fixed is not None:
+            inds = np.arange(maxactive, len(fixed), maxactive)
+            scenes.extend([self.set_scene(b, **scene_kwargs)
+                           for b in np.array_split(np.asarray(fixed), inds)])
+        if active is not None:
+            scenes.append(self.set_scene(active, **scene_kwargs))
+        else:
+            if not swap_local:
+                raise ValueError("without `active` the installed metadata belong to a scene "
+                                 "already subtracted; pass swap_local=True to accept that")
+            scenes.append(scenes[-1])
+        if not scenes:
+            raise ValueError("No scenes to prepare!")
+        proposer = self.get_proposer()
+        self.return_residual = True
+        self.pack_meta(scenes[0])
+        self.free()
+        self.send_to_device()  # the host pixel data, unsubtracted
+        for i, scene in enumerate(scenes[1:]):
+            proposer.evaluate_proposal(scenes[i].get_proposal(), patch=self)
+            self.pack_meta(scene)
+            self.swap_on_device()
+        return proposer, scenes[-1]
+
+    def design_matrix_device(self, proposal, stream=None):
+        """Unit-flux model of every source of `proposal` (the scene whose
+        metadata are installed) at every pixel: a float32 CUDA tensor
+        (n_sources, npix) computed by ``fpho_patch_design_matrix``."""
+        import torch
+        prop = np.ascontiguousarray(proposal)
+        ns = len(prop)
+        dprop = torch.from_numpy(prop.view(np.uint8).copy()).cuda()
+        X = torch.empty((ns, int(self.npix)), dtype=torch.float32, device="cuda")
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        _lib.call("fpho_patch_design_matrix", self.device_patch.handle, dprop.data_ptr(), ns,
+                  X.data_ptr(), s)
+        return X
+
+    def design_matrix(self, active=None, proposer=None, **scene_kwargs):
+        """(Xes, ys): per band the design matrix X (n_source, n_pix_band) with
+        Y[band] = f[band] . X[band] and the target data (the device data, e.g.
+        after :meth:`subtract_fixed`), as the reference's ``design_matrix``
+        (device_patch.py:193-238).  One launch builds every source's row."""
+        scene = active if hasattr(active, "get_proposal") else \
+            self.set_scene(active, **scene_kwargs)
+        self.pack_meta(scene)
+        self.replace_device_meta_ptrs()
+        X = self.design_matrix_device(scene.get_proposal()).cpu().numpy()
+        y = self.retrieve_array("data")
+        cuts = np.cumsum(self.band_N_pix[:-1])
+        return list(np.split(X, cuts, axis=1)), list(np.split(y, cuts))
 
     def render(self, proposal):
         """Model images (one flat array per exposure) of a proposal, as the

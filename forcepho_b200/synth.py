@@ -120,6 +120,36 @@ class SyntheticPatch(PatchBase, GPUPatchMixin):
     def truth_proposal(self):
         return proposal_from_params(self.truth, self.n_bands, self.table)
 
+    # ---- scenes: subsets of the patch's sources with their own metadata
+    def set_scene(self, indices, params=None):
+        """A scene of the sources `indices` (rows of ``truth``), with
+        parameters `params` (len(indices) x (n_bands + 6); default the
+        perturbed ``params`` rows), as the reference's ``set_scene``
+        (forcepho/patches/pixel_patch.py) builds one from catalog rows."""
+        from .sources import Scene
+        idx = np.atleast_1d(np.asarray(indices, dtype=np.int64))
+        p = self.params[idx] if params is None else np.asarray(params, np.float64)
+        sc = Scene(len(idx), self.n_bands, self.table, params=p)
+        sc.source_indices = idx
+        return sc
+
+    def pack_meta(self, scene):
+        """Pack the per-source metadata (astrometry and PSF rows) of `scene`
+        into the patch arrays, as the reference's ``pack_meta``
+        (forcepho/patches/patch.py:242-396); pixel arrays are untouched."""
+        full = self._meta_full
+        idx = scene.source_indices
+        ns, n_exp = len(idx), len(self.exposure_N)
+        self.n_sources = ns
+        self.D = np.ascontiguousarray(full["D"][:, idx])
+        self.CW = np.ascontiguousarray(full["CW"][:, idx])
+        self.crpix = np.ascontiguousarray(full["crpix"][:, idx])
+        self.crval = np.ascontiguousarray(full["crval"][:, idx])
+        npsf = full["npsf"]
+        self.psfgauss = np.concatenate([np.tile(m, ns) for m in full["mix"]]).astype(PSF_DTYPE)
+        self.psfgauss_start = (np.arange(n_exp) * ns * npsf).astype(np.int32)
+        self.coerce_arrays()
+
     @property
     def pairs_per_eval(self):
         """Nominal (pixel, image Gaussian) pairs of one evaluation: every
@@ -309,7 +339,7 @@ def make_patch(spec, seed=0, table=None, render=None, return_residual=False):
     nr = table.n_radii
     npsf = nr * spec.n_psf
     P.n_psf_per_source[:] = npsf
-    rows = []
+    rows, mixes = [], []
     P.psfgauss_start[:] = np.arange(n_exp) * ns * npsf
     for e in range(n_exp):
         sig = rng.uniform(*spec.psf_sigma, size=spec.n_psf)
@@ -323,7 +353,10 @@ def make_patch(spec, seed=0, table=None, render=None, return_residual=False):
         per_source = np.concatenate([mix.copy() for _ in range(nr)])
         per_source["sersic_bin"] = np.repeat(np.arange(nr), spec.n_psf)
         rows.append(np.tile(per_source, ns))
+        mixes.append(per_source)
     P.psfgauss = np.concatenate(rows).astype(PSF_DTYPE)
+    P._meta_full = {"D": P.D.copy(), "CW": P.CW.copy(), "crpix": P.crpix.copy(),
+                    "crval": P.crval.copy(), "mix": mixes, "npsf": npsf}
 
     # --- data: truth + noise; ierr = 1/sigma per exposure; masked pixels
     model = (render or render_model_numpy)(P, truth)

@@ -184,6 +184,17 @@ FPHO_API int fpho_evaluate_proposal(fpho_patch *p, const fpho_source *proposal, 
 FPHO_API int fpho_EvaluateProposal(fpho_patch *p, const void *dev_patch_struct, const void *dev_proposal,
                           void *pchi2, void *pdchi2_dp, void *stream);
 
+/* Design matrix of the proposal's sources: X[n_sources][npix] (device,
+ * float) = the unit-flux model of each source at every pixel of the patch
+ * (sum over its image Gaussians of dA/dflux * G * H, the exp-argument cutoff
+ * applied), in the patch's packed pixel order.  Replaces the loop of
+ * one-source renders of DevicePatchMixin.design_matrix
+ * (forcepho/patches/device_patch.py:198-238), which divides each source's
+ * model by its flux; the flux solve on top is forcepho_b200.fitting.
+ * Stream-ordered, no synchronization; check fpho_patch_error_word after. */
+FPHO_API int fpho_patch_design_matrix(fpho_patch *p, const void *dev_proposal, int n_sources,
+                                      float *dev_X, void *stream);
+
 /* ---- proposals built on the device -------------------------------------- */
 
 typedef struct fpho_spline fpho_spline;   /* opaque: Sersic amplitude splines on the device */
