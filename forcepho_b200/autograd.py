@@ -240,7 +240,30 @@ class BatchPosterior:
             g0 += b_ * s_ * NPARAMS
         cuda = lambda a: torch.as_tensor(np.asarray(a, dtype=np.int64), device="cuda")
         self.flux_dst, self.flux_src = cuda(flux_dst), cuda(flux_src)
-        self.shape_dst, self.shape_src = cuda(shape_dst), cuda(shape_src)
+        # shape gradients: each parameter sums its patch's bands; a padded
+        # gather (index n_dchi2 points at an appended zero) keeps the sum
+        # deterministic, in band order
+        dst = np.asarray(shape_dst, dtype=np.int64)
+        srcs = np.asarray(shape_src, dtype=np.int64)
+        order = np.argsort(dst, kind="stable")
+        dst, srcs = dst[order], srcs[order]
+        uniq, first, counts = np.unique(dst, return_index=True, return_counts=True)
+        pad = np.full((len(uniq), max(1, int(counts.max()) if len(counts) else 1)),
+                      batch.n_dchi2, dtype=np.int64)
+        for r, (f, c) in enumerate(zip(first, counts)):
+            pad[r, :c] = srcs[f:f + c]
+        self.shape_dst, self.shape_src = cuda(uniq), cuda(pad)
+        # per-patch sums (one patch per chain in multi-chain sampling): the
+        # bands and the parameters of each patch, padded
+        self.n_patches = len(nb)
+        band_off = np.concatenate([[0], np.cumsum(nb)])
+        bpad = np.full((len(nb), int(nb.max())), batch.n_bands_total, dtype=np.int64)
+        ppad = np.full((len(nb), int(npar.max())), self.ndim, dtype=np.int64)
+        for k in range(len(nb)):
+            bpad[k, :nb[k]] = np.arange(band_off[k], band_off[k + 1])
+            ppad[k, :npar[k]] = np.arange(par_off[k], par_off[k] + npar[k])
+        self.band_pad, self.par_pad = cuda(bpad), cuda(ppad)
+        self.par_patch = cuda(np.repeat(np.arange(len(nb)), npar))
 
     def transform(self, z):
         return self.tr.transform(z)
@@ -254,12 +277,21 @@ class BatchPosterior:
         jac = self.tr.range * s * (1.0 - s)
         self.table.build_proposal_batch(q, self.src_bands, self.src_off, self.prop)
         self.batch.evaluate_device(self.prop, self.chi2, self.dchi2, _stream())
-        d = self.dchi2.to(torch.float64)
-        gq = torch.zeros(self.ndim, dtype=torch.float64, device="cuda")
-        gq.index_add_(0, self.flux_dst, d[self.flux_src])
-        gq.index_add_(0, self.shape_dst, d[self.shape_src])
+        d = torch.cat([self.dchi2.to(torch.float64), self.chi2.new_zeros(1)])
+        gq = torch.empty(self.ndim, dtype=torch.float64, device="cuda")
+        gq[self.flux_dst] = d[self.flux_src]
+        gq[self.shape_dst] = d[self.shape_src].sum(dim=1)
         lnp = self.chi2.sum() * -0.5 + torch.log(jac).sum()
         return lnp, gq * (-0.5 * jac) + (1.0 - 2.0 * s)
+
+    def lnp_per_patch(self, z):
+        """lnp of each patch at z, from the chi2 of the last evaluation (which
+        must have been at z)."""
+        s = torch.sigmoid(z)
+        lj = torch.log(self.tr.range * s * (1.0 - s))
+        c = torch.cat([self.chi2, self.chi2.new_zeros(1)])
+        lj = torch.cat([lj, lj.new_zeros(1)])
+        return c[self.band_pad].sum(dim=1) * -0.5 + lj[self.par_pad].sum(dim=1)
 
 
 class Leapfrog:
