@@ -62,6 +62,8 @@ def parse():
                     help="0: one CTA per tile; 1: persistent CTAs, costliest tiles first")
     ap.add_argument("--batch-patches", type=int, default=256,
                     help="patches of the batched leg (config 3); 0 skips it")
+    ap.add_argument("--chains", type=int, default=256,
+                    help="HMC chains of the multi-chain leg (single-source patch); 0 skips it")
     ap.add_argument("--no-differentiable", action="store_true",
                     help="skip the differentiable-form leg (config 2)")
     return ap.parse_args()
@@ -330,6 +332,73 @@ def batched_leg(args, torch, lib, steps):
     return out
 
 
+def multichain_leg(args, torch, steps, n_chains=256):
+    """The single-source 64x64 px patch sampled by many HMC chains at once:
+    one leapfrog step of every chain per batched launch sequence (graph
+    replay), against one chain on the device posterior (graph replay) and the
+    plain drop-in FastPosterior.lnprob_and_grad (host proposal, host I/O)."""
+    from forcepho_b200 import synth
+    from forcepho_b200.autograd import DevicePosterior, Leapfrog, default_bounds
+    from forcepho_b200.model import FastPosterior
+    from forcepho_b200.proposal import GPUProposer
+    from forcepho_b200.sampling import chain_posterior
+    from forcepho_b200.sources import Scene
+    P = synth.make_config(0, seed=args.seed, render=synth.render_model_gpu)
+    lo, hi = default_bounds(P.params, P.n_bands)
+    s = torch.cuda.current_stream()
+
+    def per_replay(graph, n):
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(n)]
+        for e0, e1 in evs:
+            e0.record(s)
+            graph.replay()
+            e1.record(s)
+        torch.cuda.synchronize()
+        return float(np.median([a.elapsed_time(b) for a, b in evs]))
+
+    post = chain_posterior(P, n_chains, lo, hi)
+    z0 = post.inverse_transform(np.tile(P.params.reshape(-1), n_chains))
+    rng = np.random.default_rng(4)
+    lf = Leapfrog(post, eps=1e-3, steps_per_graph=1)
+    lf.set_state(z0, torch.as_tensor(rng.standard_normal(post.ndim), device="cuda"))
+    lf.run(3)
+    ms_multi = per_replay(lf.graph, steps)
+    del lf
+    for c in post.copies:
+        c.free()
+
+    P.send_to_device()
+    one = DevicePosterior(P, lo, hi)
+    lf1 = Leapfrog(one, eps=1e-3, steps_per_graph=1)
+    z1 = one.inverse_transform(P.params.reshape(-1))
+    lf1.set_state(z1, torch.as_tensor(rng.standard_normal(one.ndim), device="cuda"))
+    lf1.run(3)
+    ms_one = per_replay(lf1.graph, steps)
+    del lf1
+
+    fp = FastPosterior(GPUProposer(), P, scene=Scene(P.n_sources, P.n_bands, P.table),
+                       lower=lo, upper=hi)
+    z = fp.transform.inverse_transform(P.params.reshape(-1))
+    fp.lnprob_and_grad(z)
+    n = 50
+    t0 = time.perf_counter()
+    for _ in range(n):
+        fp.lnprob_and_grad(z + 1e-6 * rng.standard_normal(z.shape))
+    ms_dropin = (time.perf_counter() - t0) / n * 1e3
+    P.free()
+    return {"workload": "config0: 1 source, 1 band x 1 exposure, 64x64 px (4096 px x 27 "
+                        f"image Gaussians), {n_chains} chains",
+            "chains": n_chains,
+            "multichain_step_ms": ms_multi,
+            "multichain_chain_evals_per_s": n_chains / (ms_multi * 1e-3),
+            "one_chain_step_ms": ms_one, "one_chain_evals_per_s": 1e3 / ms_one,
+            "dropin_ms_per_eval": ms_dropin, "dropin_evals_per_s": 1e3 / ms_dropin,
+            "speedup_multichain_vs_dropin": (n_chains / ms_multi) / (1.0 / ms_dropin),
+            "timing": "CUDA events per graph replay of one leapfrog step (inputs L2-resident: "
+                      "the patch is 64 KB); drop-in: host wall clock"}
+
+
 def differentiable_leg(args, torch, P, cfg, steps):
     """Config 2: the config-1 patch through the autograd Function and the
     device posterior, HMC leapfrog steps of 1e-3 in the unconstrained
@@ -518,6 +587,11 @@ def run_ours(args):
     if not args.no_differentiable:
         differentiable = differentiable_leg(args, torch, P, cfg, steps=max(3, min(args.steps, 50)))
 
+    multichain = None
+    if args.chains > 0:
+        multichain = multichain_leg(args, torch, steps=max(3, min(args.steps, 50)),
+                                    n_chains=args.chains)
+
     batched = None
     if args.batch_patches > 0:
         batched = batched_leg(args, torch, _lib, steps=max(3, min(args.steps, 50)))
@@ -563,6 +637,7 @@ def run_ours(args):
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
             "differentiable": differentiable,
+            "multichain": multichain,
             "batched": batched,
         }
         print(json.dumps(line), flush=True)
