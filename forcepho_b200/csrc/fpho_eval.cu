@@ -131,7 +131,7 @@ struct Variant {
      (const void *)design_kernel<NT, K>}
 static const Variant kVariants[] = {
     FPHO_VARIANT(128, 4), FPHO_VARIANT(128, 2), FPHO_VARIANT(256, 2), FPHO_VARIANT(64, 4),
-    FPHO_VARIANT(256, 4), FPHO_VARIANT(128, 8), FPHO_VARIANT(64, 8),
+    FPHO_VARIANT(256, 4), FPHO_VARIANT(128, 8), FPHO_VARIANT(64, 8), FPHO_VARIANT(32, 8),
 };
 #undef FPHO_VARIANT
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);

@@ -216,6 +216,55 @@ __device__ __forceinline__ void residual_pairs(const v2 (&X)[KP], const v2 (&Y)[
     }
 }
 
+// Pass 1 for two consecutive kept Gaussians a, b at once: their exponentials
+// are independent and interleave, and R is updated with a's term and then
+// b's, exactly as two calls of residual_pairs in order would.  The
+// exp-argument cut is applied to both; for a Gaussian without FLAG_CUT no
+// weighted pixel of the tile reaches 36 (and with a residual output every
+// pixel is in the tile box), so the cut changes nothing there.
+template <int KP>
+__device__ __forceinline__ void residual_pairs2(const v2 (&X)[KP], const v2 (&Y)[KP], v2 (&R)[KP],
+                                                const float *ra, const float *rb, v2 CM24,
+                                                v2 KEXP2, v2 KEXPLO2) {
+    v2 NXa, NYa, FXXa, FXYa, FYYa, AMPa, HBa, C0a;
+    v2 NXb, NYb, FXXb, FXYb, FYYb, AMPb, HBb, C0b;
+    ld2(ra + R_NXC, NXa, NYa);
+    ld2(ra + R_FXX, FXXa, FXYa);
+    ld2(ra + R_FYY, FYYa, AMPa);
+    ld2(ra + R_HB, HBa, C0a);
+    ld2(rb + R_NXC, NXb, NYb);
+    ld2(rb + R_FXX, FXXb, FXYb);
+    ld2(rb + R_FYY, FYYb, AMPb);
+    ld2(rb + R_HB, HBb, C0b);
+    const v2 HAa = mul2(AMPa, CM24), HAb = mul2(AMPb, CM24);
+#pragma unroll
+    for (int j = 0; j < KP; ++j) {
+        const v2 DXa = add2(X[j], NXa), DYa = add2(Y[j], NYa);
+        const v2 DXb = add2(X[j], NXb), DYb = add2(Y[j], NYb);
+        const v2 VXa = fma2(FXYa, DYa, mul2(FXXa, DXa));
+        const v2 VXb = fma2(FXYb, DYb, mul2(FXXb, DXb));
+        const v2 VYa = fma2(FXYa, DXa, mul2(FYYa, DYa));
+        const v2 VYb = fma2(FXYb, DXb, mul2(FYYb, DYb));
+        const v2 Qa = fma2(DYa, VYa, mul2(DXa, VXa));
+        const v2 Qb = fma2(DYb, VYb, mul2(DXb, VXb));
+        v2 Ga = exp2_unbiased(fma2(Qa, KEXP2, mul2(Qa, KEXPLO2)));
+        v2 Gb = exp2_unbiased(fma2(Qb, KEXP2, mul2(Qb, KEXPLO2)));
+        {
+            float g0, g1, q0, q1;
+            unpk(Ga, g0, g1);
+            unpk(Qa, q0, q1);
+            Ga = pk(q0 > FPHO_MAX_EXP_ARG ? 0.0f : g0, q1 > FPHO_MAX_EXP_ARG ? 0.0f : g1);
+            unpk(Gb, g0, g1);
+            unpk(Qb, q0, q1);
+            Gb = pk(q0 > FPHO_MAX_EXP_ARG ? 0.0f : g0, q1 > FPHO_MAX_EXP_ARG ? 0.0f : g1);
+        }
+        const v2 Sa = fma2(VYa, VYa, mul2(VXa, VXa));
+        const v2 Sb = fma2(VYb, VYb, mul2(VXb, VXb));
+        R[j] = fma2(fma2(Sa, HAa, HBa), Ga, R[j]);
+        R[j] = fma2(fma2(Sb, HAb, HBb), Gb, R[j]);
+    }
+}
+
 // Pass 2 for one Gaussian over the thread's KP pixel pairs: the twelve sums
 // from which the model's derivatives w.r.t. (A, x, y, fxx, fyy, fxy) follow.
 struct GradSums {
@@ -260,6 +309,77 @@ __device__ __forceinline__ void gradient_pairs(const v2 (&X)[KP], const v2 (&Y)[
         s.T1 = fma2(W, T1, s.T1);
         s.T2 = fma2(W, mul2(DY, VY), s.T2);
         s.T3 = fma2(W, fma2(DX, VY, mul2(DY, VX)), s.T3);
+    }
+}
+
+// Pass 2 for two consecutive kept Gaussians a, b at once (independent
+// exponentials interleave); each set of sums is formed in the same order as
+// by gradient_pairs, and the cut is applied to both (see residual_pairs2).
+template <int KP>
+__device__ __forceinline__ void gradient_pairs2(const v2 (&X)[KP], const v2 (&Y)[KP],
+                                                const v2 (&R2)[KP], const float *ra,
+                                                const float *rb, v2 C24, v2 KEXP2, GradSums &sa,
+                                                GradSums &sb) {
+    v2 NXa, NYa, FXXa, FXYa, FYYa, AMPa, HBa, C0a;
+    v2 NXb, NYb, FXXb, FXYb, FYYb, AMPb, HBb, C0b;
+    ld2(ra + R_NXC, NXa, NYa);
+    ld2(ra + R_FXX, FXXa, FXYa);
+    ld2(ra + R_FYY, FYYa, AMPa);
+    ld2(ra + R_HB, HBa, C0a);
+    ld2(rb + R_NXC, NXb, NYb);
+    ld2(rb + R_FXX, FXXb, FXYb);
+    ld2(rb + R_FYY, FYYb, AMPb);
+    ld2(rb + R_HB, HBb, C0b);
+    sa = GradSums{0ull, 0ull, 0ull, 0ull, 0ull, 0ull, 0ull, 0ull, 0ull, 0ull, 0ull, 0ull};
+    sb = sa;
+#pragma unroll
+    for (int j = 0; j < KP; ++j) {
+        const v2 DXa = add2(X[j], NXa), DYa = add2(Y[j], NYa);
+        const v2 DXb = add2(X[j], NXb), DYb = add2(Y[j], NYb);
+        const v2 VXa = fma2(FXYa, DYa, mul2(FXXa, DXa));
+        const v2 VXb = fma2(FXYb, DYb, mul2(FXXb, DXb));
+        const v2 VYa = fma2(FXYa, DXa, mul2(FYYa, DYa));
+        const v2 VYb = fma2(FXYb, DXb, mul2(FYYb, DYb));
+        const v2 T1a = mul2(DXa, VXa), T1b = mul2(DXb, VXb);
+        const v2 Qa = fma2(DYa, VYa, T1a), Qb = fma2(DYb, VYb, T1b);
+        float ea0, ea1, eb0, eb1, qa0, qa1, qb0, qb1;
+        unpk(mul2(Qa, KEXP2), ea0, ea1);
+        unpk(mul2(Qb, KEXP2), eb0, eb1);
+        unpk(Qa, qa0, qa1);
+        unpk(Qb, qb0, qb1);
+        const float ga0 = qa0 > FPHO_MAX_EXP_ARG ? 0.0f : ex2f(ea0);
+        const float ga1 = qa1 > FPHO_MAX_EXP_ARG ? 0.0f : ex2f(ea1);
+        const float gb0 = qb0 > FPHO_MAX_EXP_ARG ? 0.0f : ex2f(eb0);
+        const float gb1 = qb1 > FPHO_MAX_EXP_ARG ? 0.0f : ex2f(eb1);
+        const v2 Sa = fma2(VYa, VYa, mul2(VXa, VXa)), Sb = fma2(VYb, VYb, mul2(VXb, VXb));
+        const v2 Ha = fma2(Sa, C24, C0a), Hb = fma2(Sb, C24, C0b);
+        const v2 Wa = mul2(R2[j], pk(ga0, ga1)), Wb = mul2(R2[j], pk(gb0, gb1));
+        const v2 WHa = mul2(Wa, Ha), WHb = mul2(Wb, Hb);
+        sa.A = add2(sa.A, WHa);
+        sb.A = add2(sb.A, WHb);
+        sa.HVx = fma2(WHa, VXa, sa.HVx);
+        sb.HVx = fma2(WHb, VXb, sb.HVx);
+        sa.HVy = fma2(WHa, VYa, sa.HVy);
+        sb.HVy = fma2(WHb, VYb, sb.HVy);
+        sa.Vx = fma2(Wa, VXa, sa.Vx);
+        sb.Vx = fma2(Wb, VXb, sb.Vx);
+        sa.Vy = fma2(Wa, VYa, sa.Vy);
+        sb.Vy = fma2(Wb, VYb, sb.Vy);
+        const v2 HDXa = mul2(WHa, DXa), HDXb = mul2(WHb, DXb);
+        sa.HXX = fma2(HDXa, DXa, sa.HXX);
+        sb.HXX = fma2(HDXb, DXb, sb.HXX);
+        sa.HXY = fma2(HDXa, DYa, sa.HXY);
+        sb.HXY = fma2(HDXb, DYb, sb.HXY);
+        sa.HYY = fma2(mul2(WHa, DYa), DYa, sa.HYY);
+        sb.HYY = fma2(mul2(WHb, DYb), DYb, sb.HYY);
+        sa.W = add2(sa.W, Wa);
+        sb.W = add2(sb.W, Wb);
+        sa.T1 = fma2(Wa, T1a, sa.T1);
+        sb.T1 = fma2(Wb, T1b, sb.T1);
+        sa.T2 = fma2(Wa, mul2(DYa, VYa), sa.T2);
+        sb.T2 = fma2(Wb, mul2(DYb, VYb), sb.T2);
+        sa.T3 = fma2(Wa, fma2(DXa, VYa, mul2(DYa, VXa)), sa.T3);
+        sb.T3 = fma2(Wb, fma2(DXb, VYb, mul2(DYb, VXb)), sb.T3);
     }
 }
 
@@ -419,7 +539,11 @@ __device__ __forceinline__ void tile_body(const TileArgs &A, int tile, unsigned 
         const int c0 = c * cap, n = min(cap, n_live - c0);
         if (c > 0) __syncthreads();  // previous chunk fully consumed
         stage(c0, n);
-        for (int i = 0; i < n; ++i) {
+        int i = 0;
+        for (; i + 1 < n; i += 2)
+            residual_pairs2<KP>(X, Y, R, recs + (size_t)i * GSTAGE, recs + (size_t)(i + 1) * GSTAGE,
+                                CM24, KEXP2, KEXPLO2);
+        for (; i < n; ++i) {
             const float *r = recs + (size_t)i * GSTAGE;
             v2 NXC, NYC, FXX, FXY, FYY, AMP, HB, C0;
             ld2(r + R_NXC, NXC, NYC);
@@ -469,23 +593,12 @@ __device__ __forceinline__ void tile_body(const TileArgs &A, int tile, unsigned 
                 __syncthreads();
                 stage(c0, n);
             }
-            for (int i = 0; i < n; ++i) {
-                const float *r = recs + (size_t)i * GSTAGE;
-                v2 NXC, NYC, FXX, FXY, FYY, AMP, HB, C0;
-                ld2(r + R_NXC, NXC, NYC);
-                ld2(r + R_FXX, FXX, FXY);
-                ld2(r + R_FYY, FYY, AMP);
-                ld2(r + R_HB, HB, C0);
-                const int flag = kept[c0 + i];
+            // the Jacobian epilogue of one Gaussian, in list order
+            auto epilogue = [&](const float *r, int flag, const GradSums &s, bool last) {
                 const float4 *rj = reinterpret_cast<const float4 *>(r + R_JA_FLUX);
-                GradSums s;
-                if (flag & FLAG_CUT)
-                    gradient_pairs<KP, true>(X, Y, R2, NXC, NYC, FXX, FXY, FYY, C0, C24, KEXP2, s);
-                else
-                    gradient_pairs<KP, false>(X, Y, R2, NXC, NYC, FXX, FXY, FYY, C0, C24, KEXP2, s);
                 // image-space gradient of this Gaussian over the thread's pixels
                 // (amp factors are folded into the Jacobian rows), in scalars
-                const float fxx = lo(FXX), fxy = lo(FXY), fyy = lo(FYY);
+                const float fxx = r[R_FXX], fxy = r[R_FXY], fyy = r[R_FYY];
                 const float sVx = lanesum(s.Vx), sVy = lanesum(s.Vy), sW = lanesum(s.W);
                 const float gA = lanesum(s.A);
                 const float gx = lanesum(s.HVx) - (fxx * sVx + fxy * sVy) * (1.0f / 12.0f);
@@ -504,7 +617,7 @@ __device__ __forceinline__ void tile_body(const TileArgs &A, int tile, unsigned 
                 P[5] = fmaf(j0.w, gA, P[5]);
                 P[6] = fmaf(j1.x, gA, P[6]);
                 // flush at a source boundary or at the end of the chunk
-                if ((flag & FLAG_LAST_SRC) || i == n - 1) {
+                if ((flag & FLAG_LAST_SRC) || last) {
                     const int src = __float_as_int(j3.w);
                     float v[8] = {P[0], P[1], P[2], P[3], P[4], P[5], P[6], 0.0f};
 #pragma unroll
@@ -513,6 +626,29 @@ __device__ __forceinline__ void tile_body(const TileArgs &A, int tile, unsigned 
                     const int k = reduce7_index(lane);
                     if ((lane & 3) == 0 && k < 7) wacc[warp * stride + src * 7 + k] += tot;
                 }
+            };
+            int i = 0;
+            for (; i + 1 < n; i += 2) {
+                const float *ra = recs + (size_t)i * GSTAGE, *rb = ra + GSTAGE;
+                GradSums sa, sb;
+                gradient_pairs2<KP>(X, Y, R2, ra, rb, C24, KEXP2, sa, sb);
+                epilogue(ra, kept[c0 + i], sa, false);
+                epilogue(rb, kept[c0 + i + 1], sb, i + 1 == n - 1);
+            }
+            for (; i < n; ++i) {
+                const float *r = recs + (size_t)i * GSTAGE;
+                v2 NXC, NYC, FXX, FXY, FYY, AMP, HB, C0;
+                ld2(r + R_NXC, NXC, NYC);
+                ld2(r + R_FXX, FXX, FXY);
+                ld2(r + R_FYY, FYY, AMP);
+                ld2(r + R_HB, HB, C0);
+                const int flag = kept[c0 + i];
+                GradSums s;
+                if (flag & FLAG_CUT)
+                    gradient_pairs<KP, true>(X, Y, R2, NXC, NYC, FXX, FXY, FYY, C0, C24, KEXP2, s);
+                else
+                    gradient_pairs<KP, false>(X, Y, R2, NXC, NYC, FXX, FXY, FYY, C0, C24, KEXP2, s);
+                epilogue(r, flag, s, i == n - 1);
             }
         }
     }
