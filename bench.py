@@ -43,7 +43,7 @@ WORKLOAD = "config1: 20 src, 8 bands x 4 exp x 128x128 px, 5-gauss PSF, 9 radii"
 # DRAM bytes (read + write) of one tile-kernel launch on this workload, from an
 # ncu capture (profiles/tile_kernel_dyn_64x4_config1.md): the 16 B per pixel
 # of the pixel arrays plus the image-Gaussian table, each read once.
-TILE_TRAFFIC_BYTES = 12658688
+TILE_TRAFFIC_BYTES = 12673536
 
 
 def parse():
@@ -147,6 +147,17 @@ def cpu_reference_time(P, prop, reps, cores):
         pool.close()
         pool.join()
     return times
+
+
+def _cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    return ln.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
 
 
 def make_workload(seed, device_render):
@@ -603,11 +614,15 @@ def run_ours(args):
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cores = len(os.sched_getaffinity(0))
         use = min(cores, nb)
-        times = cpu_reference_time(P, prop, 3, use)
-        cpu = {"value": 1.0 / float(np.mean(times)), "unit": "evals/s", "cores": use,
+        times = cpu_reference_time(P, prop, 5, use)
+        one = cpu_reference_time(P, prop, 1, 1)
+        cpu = {"value": 1.0 / float(np.median(times)), "unit": "evals/s", "cores": use,
                "kind": "reference",
-               "sample": "3 full evaluations of the same patch (8 bands, one band per "
-                         f"process on {use} of {cores} host cores)"}
+               "single_core_evals_per_s": 1.0 / float(one[0]),
+               "cpu_model": _cpu_model(),
+               "sample": "median of 5 full evaluations of the same patch after one warm-up "
+                         f"(8 bands, one band per process on {use} of {cores} host cores); "
+                         "single core: one full evaluation, bands in turn"}
 
     if rank == 0:
         line = {

@@ -75,6 +75,7 @@ _SIGS = {
     "fpho_batch_count_pairs": (c_int, [c_void_p, c_int, ctypes.POINTER(ctypes.c_longlong)]),
     "fpho_batch_time_tiles": (c_int, [c_void_p, c_int]),
     "fpho_batch_last_tile_ms": (c_int, [c_void_p, ctypes.POINTER(ctypes.c_float)]),
+    "fpho_batch_error_word": (c_int, [c_void_p, ctypes.POINTER(c_int)]),
     "fpho_batch_free": (c_int, [c_void_p]),
     "fpho_spline_create": (c_int, [c_void_p, c_int, c_void_p, c_int, c_void_p, c_int, c_void_p,
                                    ctypes.c_double, c_void_p, ctypes.POINTER(c_void_p)]),

@@ -114,6 +114,12 @@ class PatchBatch:
         _lib.call("fpho_batch_last_tile_ms", self.handle, ctypes.byref(t))
         return float(t.value)
 
+    def error_word(self):
+        """The batched kernels' error word of the last evaluation (0 = none)."""
+        w = ctypes.c_int()
+        _lib.call("fpho_batch_error_word", self.handle, ctypes.byref(w))
+        return w.value
+
     def count_pairs(self, enable=True):
         c = ctypes.c_longlong()
         _lib.call("fpho_batch_count_pairs", self.handle, int(enable), ctypes.byref(c))

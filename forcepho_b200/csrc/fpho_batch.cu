@@ -206,6 +206,8 @@ extern "C" int fpho_batch_create(fpho_patch *const *patches, int n, int live_cap
     std::vector<BandJob> jobs;
     int rc = FPHO_OK;
     if (!rc) rc = balloc(&b->d_err, 1);
+    if (!rc && cudaMemsetAsync(b->d_err, 0, sizeof(int), (cudaStream_t)stream) != cudaSuccess)
+        rc = set_error(FPHO_ERR_CUDA, "cudaMemsetAsync failed");
     if (!rc) rc = balloc(&b->d_pairs, 1);
     long long dchi2_off = 0;
     int src_off = 0, band_off = 0;
@@ -426,6 +428,13 @@ extern "C" int fpho_batch_evaluate(fpho_batch *b, const fpho_source *proposals, 
     CUDA_TRY(cudaMemcpyAsync(&err, b->d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
     CUDA_TRY(cudaStreamSynchronize(s));
     if (err) return set_error(FPHO_ERR_KERNEL, "batched tile kernel reported error word 0x%x", err);
+    return FPHO_OK;
+}
+
+extern "C" int fpho_batch_error_word(fpho_batch *b, int *out) {
+    clear_error();
+    if (!b || !out) return set_error(FPHO_ERR_INVALID, "NULL argument");
+    CUDA_TRY(cudaMemcpy(out, b->d_err, sizeof(int), cudaMemcpyDeviceToHost));
     return FPHO_OK;
 }
 

@@ -520,6 +520,8 @@ extern "C" int fpho_patch_create(const fpho_patch_struct *host, int n_bands, int
     if (!rc) rc = upload_meta(p, host, s);
     if (!rc) rc = dalloc(&p->d_chi2_out, (size_t)p->n_bands);
     if (!rc) rc = dalloc(&p->d_err, 1);
+    if (!rc && cudaMemsetAsync(p->d_err, 0, sizeof(int), s) != cudaSuccess)
+        rc = set_error(FPHO_ERR_CUDA, "cudaMemsetAsync failed");
     if (!rc) rc = dalloc(&p->d_pairs, 1);
     if (!rc) rc = build_plan(p, s);
     if (!rc) rc = refresh_struct(p, s);

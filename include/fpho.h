@@ -261,6 +261,10 @@ FPHO_API int fpho_batch_evaluate(fpho_batch *b, const fpho_source *proposals, do
 FPHO_API int fpho_batch_count_pairs(fpho_batch *b, int enable, long long *last_count);
 FPHO_API int fpho_batch_time_tiles(fpho_batch *b, int enable);
 FPHO_API int fpho_batch_last_tile_ms(fpho_batch *b, float *ms);
+/* The batch's error word (0 = no kernel reported an error) of the last
+ * evaluation; device-buffer evaluations (without FPHO_IO_HOST) do not check
+ * it.  Synchronizes the device.  No reference counterpart. */
+FPHO_API int fpho_batch_error_word(fpho_batch *b, int *out);
 FPHO_API int fpho_batch_free(fpho_batch *b);
 
 /* ---- evaluation without allocation (no counterpart in the reference) ---- */

@@ -105,3 +105,80 @@ def test_reference_gpu_kernel_timing_config1():
           f"({1e3 / t_ref:.1f} evals/s), this project's {t_us:.3f} ms ({1e3 / t_us:.1f} evals/s): "
           f"{t_ref / t_us:.1f}x")
     P.free()
+
+
+def test_reference_gpu_kernel_timing_config0_and_batch():
+    """Times the reference CUDA kernel on the single-source 64x64 px patch and
+    on 256 uneven patches (one launch per patch, as GPUProposer launches it),
+    beside this project's plain loop and batched form on the same patches;
+    checks agreement of chi2 (1e-5) on every patch."""
+    if not refgpu.available():
+        pytest.skip("reference CUDA kernel not built")
+    import torch
+    from forcepho_b200 import _lib, synth
+    from forcepho_b200.batch import PatchBatch
+    s = torch.cuda.current_stream()
+
+    def setup(P):
+        nb, ns = P.n_bands, P.n_sources
+        P.send_to_device()
+        dprop = torch.from_numpy(P.proposal().view(np.uint8).copy()).cuda()
+        return dict(P=P, nb=nb, ns=ns, dstruct=P.device_patch.device_struct, dprop=dprop,
+                    mg=refgpu.max_gauss_band(P),
+                    c_rg=torch.zeros(nb, dtype=torch.float64, device="cuda"),
+                    resp=torch.zeros(nb * 210, dtype=torch.float32, device="cuda"),
+                    c_us=torch.zeros(nb, dtype=torch.float64, device="cuda"),
+                    g_us=torch.zeros(nb * ns * 7, dtype=torch.float32, device="cuda"))
+
+    def ref_all(items):
+        for it in items:
+            refgpu.evaluate(it["dstruct"], it["dprop"].data_ptr(), it["c_rg"].data_ptr(),
+                            it["resp"].data_ptr(), it["nb"], it["ns"], it["mg"], s.cuda_stream)
+
+    def ours_all(items):
+        for it in items:
+            _lib.call("fpho_evaluate_proposal", it["P"].device_patch.handle,
+                      it["dprop"].data_ptr(), it["ns"], it["c_us"].data_ptr(),
+                      it["g_us"].data_ptr(), 7 * it["ns"], 0, s.cuda_stream)
+
+    def timed(fn, n=5):
+        fn()
+        torch.cuda.synchronize()
+        ts = []
+        for _ in range(n):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(s)
+            fn()
+            e1.record(s)
+            e1.synchronize()
+            ts.append(e0.elapsed_time(e1))
+        return float(np.median(ts))
+
+    # the single-source patch
+    it0 = [setup(synth.make_config(0, seed=1, render=synth.render_model_gpu))]
+    t_ref0, t_us0 = timed(lambda: ref_all(it0), 20), timed(lambda: ours_all(it0), 20)
+    np.testing.assert_allclose(it0[0]["c_rg"].cpu().numpy(), it0[0]["c_us"].cpu().numpy(),
+                               rtol=1e-5)
+    print(f"single-source patch: reference CUDA kernel {t_ref0 * 1e3:.1f} us, "
+          f"this project's {t_us0 * 1e3:.1f} us per evaluation")
+    it0[0]["P"].free()
+
+    # 256 uneven patches
+    patches = synth.make_config(3, seed=3, render=synth.render_model_gpu, n_patches=256)
+    items = [setup(P) for P in patches]
+    t_ref = timed(lambda: ref_all(items), 3)
+    t_us = timed(lambda: ours_all(items), 3)
+    for it in items:
+        np.testing.assert_allclose(it["c_rg"].cpu().numpy(), it["c_us"].cpu().numpy(),
+                                   rtol=1e-5)
+    batch = PatchBatch(patches)
+    dprop, chi2, dchi2 = batch.device_buffers()
+    t_b = timed(lambda: batch.evaluate_device(dprop, chi2, dchi2), 5)
+    nominal = sum(P.pairs_per_eval for P in patches)
+    print(f"256 uneven patches: reference CUDA kernel {t_ref:.2f} ms "
+          f"({256 / (t_ref * 1e-3):.0f} patch-evals/s, {nominal / (t_ref * 1e-3):.3e} "
+          f"pix-gauss/s); this project's plain loop {t_us:.2f} ms; batched {t_b:.2f} ms "
+          f"({256 / (t_b * 1e-3):.0f} patch-evals/s, {nominal / (t_b * 1e-3):.3e} pix-gauss/s)")
+    batch.free()
+    for P in patches:
+        P.free()

@@ -8,8 +8,8 @@
     single-patch device posterior's at the same z (1e-12 relative) and the
     per-chain lnp sum to the total;
   * a short run on the single-source patch: every chain finite, moved, and
-    accepting more than half of its proposals; the tile kernels' error word
-    stays 0.
+    accepting more than half of its proposals; the batched kernels' error
+    word stays 0.
 """
 import numpy as np
 import pytest
@@ -122,10 +122,7 @@ def test_many_chains_on_single_source_patch():
     assert np.all(np.isfinite(z)) and np.all(np.isfinite(hmc.lnp.cpu().numpy()))
     assert np.all(np.any(z != z0.cpu().numpy().reshape(k, -1), axis=1))
     assert acc.mean() > 0.5
-    import ctypes
-    from forcepho_b200 import _lib
+    assert post.batch.error_word() == 0
+    post.batch.free()
     for c in post.copies:
-        w = ctypes.c_int()
-        _lib.call("fpho_patch_error_word", c.device_patch.handle, ctypes.byref(w))
-        assert w.value == 0
         c.free()
