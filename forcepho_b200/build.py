@@ -55,14 +55,20 @@ def build(force=False, verbose=False, extra_flags=()):
     objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
     nvcc = _nvcc()
-    objs = []
+    jobs = []
     for src in sources():
         obj = os.path.join(objdir, os.path.basename(src) + ".o")
-        cmd = [nvcc, *NVCC_FLAGS, *extra_flags, "-I", INCLUDE, "-I", CSRC, "-dc" if False else "-c", src, "-o", obj]
+        cmd = [nvcc, *NVCC_FLAGS, *extra_flags, "-I", INCLUDE, "-I", CSRC, "-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
-        subprocess.run(cmd, check=True)
-        objs.append(obj)
+        jobs.append((cmd, obj))
+    # translation units compile independently: run them side by side
+    from concurrent.futures import ThreadPoolExecutor
+    with ThreadPoolExecutor(max(1, min(len(jobs), os.cpu_count() or 1))) as ex:
+        for r in ex.map(lambda j: subprocess.run(j[0]), jobs):
+            if r.returncode != 0:
+                raise subprocess.CalledProcessError(r.returncode, r.args)
+    objs = [o for _, o in jobs]
     tmp = LIB + ".tmp"
     cmd = [nvcc, *NVCC_FLAGS, "-shared", *objs, "-o", tmp]
     if verbose:
