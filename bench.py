@@ -6,7 +6,7 @@
 Workload: the realistic plain patch (20 Sersic sources, 8 bands x 4
 exposures of 128x128 px, 5-Gaussian PSFs, 9 mixture radii: 524,288 pixels x
 900 image Gaussians per exposure = 4.72e8 pixel-Gaussian pairs per
-evaluation), synthetic and seeded (forcepho_b200.synth, config 1).  A step is
+evaluation), synthetic and seeded (forcepho_b200.synth, "field20").  A step is
 one chi2 + gradient evaluation of one proposal on that patch.  With N GPUs
 (torchrun) every rank evaluates its own copy of the patch (independent
 patches: weak scaling, no collective on the data path).
@@ -39,9 +39,9 @@ sys.path.insert(0, ROOT)
 
 METRIC = "chi2+grad evals/s & pix·gauss/s: batched vs plain, 1 B200, rel err ≤1e-6"
 FLOPS_PER_PAIR = 105          # 18 (model) + 87 (gradient) FP32 flops, FMA = 2
-WORKLOAD = "config1: 20 src, 8 bands x 4 exp x 128x128 px, 5-gauss PSF, 9 radii"
+WORKLOAD = "field20: 20 src, 8 bands x 4 exp x 128x128 px, 5-gauss PSF, 9 radii"
 # DRAM bytes (read + write) of one tile-kernel launch on this workload, from an
-# ncu capture (profiles/tile_kernel_dyn_64x4_config1.md): the 16 B per pixel
+# ncu capture (profiles/tile_kernel_dyn_64x4_field20.md): the 16 B per pixel
 # of the pixel arrays plus the image-Gaussian table, each read once.
 TILE_TRAFFIC_BYTES = 12673536
 
@@ -61,11 +61,11 @@ def parse():
     ap.add_argument("--schedule", type=int, default=None, choices=[0, 1],
                     help="0: one CTA per tile; 1: persistent CTAs, costliest tiles first")
     ap.add_argument("--batch-patches", type=int, default=256,
-                    help="patches of the batched leg (config 3); 0 skips it")
+                    help="patches of the batched leg (uneven patches); 0 skips it")
     ap.add_argument("--chains", type=int, default=256,
                     help="HMC chains of the multi-chain leg (single-source patch); 0 skips it")
     ap.add_argument("--no-differentiable", action="store_true",
-                    help="skip the differentiable-form leg (config 2)")
+                    help="skip the differentiable-form leg (20-source patch)")
     return ap.parse_args()
 
 
@@ -163,7 +163,7 @@ def _cpu_model():
 def make_workload(seed, device_render):
     from forcepho_b200 import synth
     render = synth.render_model_gpu if device_render else None
-    return synth.make_config(1, seed=seed, render=render)
+    return synth.make_workload("field20", seed=seed, render=render)
 
 
 def run_reference(args):
@@ -217,12 +217,12 @@ def probe_fp32(torch, lib):
 
 
 def batched_leg(args, torch, lib, steps):
-    """Config 3: 256 uneven patches.  Batched evaluation (one persistent launch
+    """256 uneven patches.  Batched evaluation (one persistent launch
     per step, replayed from a CUDA graph) against the plain form (one
     fpho_evaluate_proposal per patch), both on device-resident buffers."""
     from forcepho_b200 import synth
     from forcepho_b200.batch import PatchBatch
-    patches = synth.make_config(3, seed=args.seed + 3, render=synth.render_model_gpu,
+    patches = synth.make_workload("uneven", seed=args.seed + 3, render=synth.render_model_gpu,
                                 n_patches=args.batch_patches)
     for P in patches:
         P.return_residual = False
@@ -278,7 +278,7 @@ def batched_leg(args, torch, lib, steps):
         plain()
     ms_plain = timed(plain, max(3, steps // 4))
     n = len(patches)
-    out = {"workload": f"config3: {n} patches, sources U{{1..30}}, bands U{{1..8}}, "
+    out = {"workload": f"uneven: {n} patches, sources U{{1..30}}, bands U{{1..8}}, "
                        "exposures/band U{1..8}, side U[32,200] px",
            "patches": n, "nominal_pairs_per_step": nominal, "evaluated_pairs_per_step": evaluated,
            "work_items": batch.n_work, "persistent_grid": batch.grid,
@@ -354,7 +354,7 @@ def multichain_leg(args, torch, steps, n_chains=256):
     from forcepho_b200.proposal import GPUProposer
     from forcepho_b200.sampling import chain_posterior
     from forcepho_b200.sources import Scene
-    P = synth.make_config(0, seed=args.seed, render=synth.render_model_gpu)
+    P = synth.make_workload("single", seed=args.seed, render=synth.render_model_gpu)
     lo, hi = default_bounds(P.params, P.n_bands)
     s = torch.cuda.current_stream()
 
@@ -398,7 +398,7 @@ def multichain_leg(args, torch, steps, n_chains=256):
         fp.lnprob_and_grad(z + 1e-6 * rng.standard_normal(z.shape))
     ms_dropin = (time.perf_counter() - t0) / n * 1e3
     P.free()
-    return {"workload": "config0: 1 source, 1 band x 1 exposure, 64x64 px (4096 px x 27 "
+    return {"workload": "single: 1 source, 1 band x 1 exposure, 64x64 px (4096 px x 27 "
                         f"image Gaussians), {n_chains} chains",
             "chains": n_chains,
             "multichain_step_ms": ms_multi,
@@ -411,7 +411,7 @@ def multichain_leg(args, torch, steps, n_chains=256):
 
 
 def differentiable_leg(args, torch, P, cfg, steps):
-    """Config 2: the config-1 patch through the autograd Function and the
+    """The 20-source patch through the autograd Function and the
     device posterior, HMC leapfrog steps of 1e-3 in the unconstrained
     coordinates replayed from a CUDA graph, against the plain drop-in
     (FastPosterior.lnprob_and_grad with host proposals and host I/O)."""
@@ -465,7 +465,7 @@ def differentiable_leg(args, torch, P, cfg, steps):
     for _ in range(n):
         fp.lnprob_and_grad(z + 1e-6 * rng.standard_normal(z.shape))
     ms_dropin = (time.perf_counter() - t0) / n * 1e3
-    out = {"workload": "config2: config-1 patch, 280 parameters, leapfrog eps 1e-3 in "
+    out = {"workload": "field20 differentiable: 20-source patch, 280 parameters, leapfrog eps 1e-3 in "
                        "unconstrained coordinates",
            "graph_step_ms": ms_step, "graph_evals_per_s": 1e3 / ms_step,
            "trajectory_500_ms": ms_traj, "trajectory_evals_per_s": 500 / (ms_traj * 1e-3),
@@ -645,7 +645,7 @@ def run_ours(args):
                          "unit": "TFLOP/s", "frac": achieved / fp32_tflops,
                          "traffic": TILE_TRAFFIC_BYTES,
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum "
-                                           "of one launch, profiles/tile_kernel_dyn_64x4_config1.md",
+                                           "of one launch, profiles/tile_kernel_dyn_64x4_field20.md",
                          "peak_source": "measured live: packed FP32 FMA probe kernel",
                          "kernel": "tile_kernel", "kernel_ms": tile_s * 1e3,
                          "sfu_gops": sfu, "sfu_peak_gops": ex2_gops, "sfu_frac": sfu / ex2_gops},

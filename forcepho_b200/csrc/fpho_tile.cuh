@@ -98,7 +98,7 @@ __device__ __forceinline__ double warp_sum_d(double v) {
 // Reduce 7 per-lane values across the warp; afterwards lane k (k < 7) holds
 // the warp total of value k.  Uses 4+2+1+1+1 shuffles instead of 7*5.
 __device__ __forceinline__ float warp_reduce7(float v[8], int lane) {
-    // round 1: lanes < 16 keep 0..3, lanes >= 16 keep 4..7
+    // exchange 1: lanes < 16 keep 0..3, lanes >= 16 keep 4..7
     {
         const bool up = lane & 16;
 #pragma unroll

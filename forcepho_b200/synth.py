@@ -4,18 +4,17 @@ No public dataset is involved in forcepho's hot path; its inputs are packed
 patches (pixel data, inverse errors and pixel coordinates per exposure,
 per-exposure astrometry, photometric conversion and PSF mixtures) and source
 proposals.  This module draws them from ``numpy.random.default_rng(seed)``
-with the distributions of the five workloads the benchmarks and tests use:
+with the distributions of the workloads the benchmarks and tests use:
 
-  config 0  1 band x 1 exposure of 64x64 px, 1 source, 3-Gaussian PSF
-  config 1  8 bands x 4 exposures of 128x128 px, 20 sources, 5-Gaussian PSFs,
-            per-exposure rotation (+-1 deg), scale (+-2%), flux calibration
-            U[0.8, 1.2], 2% of pixels masked (ierr = 0)
-  config 2  the config-1 patch (driven through the differentiable form)
-  config 3  256 patches: sources U{1..30}, bands U{1..8}, exposures per band
-            U{1..8}, exposure side U[32, 200] px
-  config 4  60 sources (half with sersic in [3.5, 6], rh up to 1 arcsec,
-            fluxes LogNormal(0, 3)), 15 bands x 6 exposures of 256x256 px,
-            6-Gaussian PSFs
+  "single"    1 band x 1 exposure of 64x64 px, 1 source, 3-Gaussian PSF
+  "field20"   8 bands x 4 exposures of 128x128 px, 20 sources, 5-Gaussian
+              PSFs, per-exposure rotation (+-1 deg), scale (+-2%), flux
+              calibration U[0.8, 1.2], 2% of pixels masked (ierr = 0)
+  "uneven"    n patches (256 by default): sources U{1..30}, bands U{1..8},
+              exposures per band U{1..8}, exposure side U[32, 200] px
+  "stress60"  60 sources (half with sersic in [3.5, 6], rh up to 1 arcsec,
+              fluxes LogNormal(0, 3)), 15 bands x 6 exposures of 256x256 px,
+              6-Gaussian PSFs
 
 Pixel scale 0.03 arcsec/px.  D (pixels per arcsec) and CW (pixels per degree,
 CW = D diag(3600 cos dec0, 3600)) follow forcepho/slow/stamp.py:250-254.
@@ -36,7 +35,7 @@ from .patches.patch import PSF_DTYPE, PatchBase
 from .patches.device_patch import GPUPatchMixin
 from .sources import default_table, proposal_from_params
 
-__all__ = ["PatchSpec", "SyntheticPatch", "make_config", "make_patch", "config_spec",
+__all__ = ["PatchSpec", "SyntheticPatch", "make_workload", "make_patch", "workload_spec",
            "render_model_numpy", "PIXEL_SCALE", "DEC0"]
 
 PIXEL_SCALE = 0.03      # arcsec per pixel
@@ -69,17 +68,20 @@ class PatchSpec:
         return len(self.exposures_per_band)
 
 
-def config_spec(k, rng=None):
-    """PatchSpec of config k (0, 1, 2 or 4; config 3 draws one spec per patch
-    from ``rng``, see :func:`make_config`)."""
-    if k == 0:
+WORKLOADS = ("single", "field20", "uneven", "stress60")
+
+
+def workload_spec(name, rng=None):
+    """PatchSpec of a workload ("uneven" draws one spec per patch from
+    ``rng``, see :func:`make_workload`)."""
+    if name == "single":
         return PatchSpec(n_sources=1, exposures_per_band=[1], shapes=[(64, 64)], n_psf=3,
                          psf_sigma=(0.5, 3.0), flux_sigma=1.0, position="centre")
-    if k in (1, 2):
+    if name == "field20":
         return PatchSpec(n_sources=20, exposures_per_band=[4] * 8, shapes=[(128, 128)] * 32,
                          n_psf=5, psf_sigma=(0.5, 4.0), rot_deg=1.0, scale_frac=0.02,
                          g_range=(0.8, 1.2), mask_frac=0.02, flux_sigma=1.5)
-    if k == 3:
+    if name == "uneven":
         rng = rng or np.random.default_rng(0)
         nb = int(rng.integers(1, 9))
         epb = [int(rng.integers(1, 9)) for _ in range(nb)]
@@ -90,12 +92,12 @@ def config_spec(k, rng=None):
         return PatchSpec(n_sources=int(rng.integers(1, 31)), exposures_per_band=epb,
                          shapes=shapes, n_psf=5, psf_sigma=(0.5, 4.0), rot_deg=1.0,
                          scale_frac=0.02, g_range=(0.8, 1.2), mask_frac=0.02, flux_sigma=1.5)
-    if k == 4:
+    if name == "stress60":
         return PatchSpec(n_sources=60, exposures_per_band=[6] * 15, shapes=[(256, 256)] * 90,
                          n_psf=6, psf_sigma=(0.5, 4.0), rot_deg=1.0, scale_frac=0.02,
                          g_range=(0.8, 1.2), mask_frac=0.02, flux_sigma=3.0,
                          bright_fraction=0.5, bright_sersic=(3.5, 6.0), bright_rh=(0.05, 1.0))
-    raise ValueError(f"unknown config {k}")
+    raise ValueError(f"unknown workload {name!r} (one of {WORKLOADS})")
 
 
 class SyntheticPatch(PatchBase, GPUPatchMixin):
@@ -382,14 +384,15 @@ def make_patch(spec, seed=0, table=None, render=None, return_residual=False):
     return P
 
 
-def make_config(k, seed=0, render=None, return_residual=False, n_patches=256):
-    """Patch (or, for config 3, list of ``n_patches`` patches) of config k."""
-    if k == 3:
+def make_workload(name, seed=0, render=None, return_residual=False, n_patches=256):
+    """The patch of a workload (for "uneven", a list of ``n_patches``)."""
+    if name == "uneven":
         rng = np.random.default_rng(seed)
         out = []
         for i in range(n_patches):
-            spec = config_spec(3, rng)
+            spec = workload_spec("uneven", rng)
             out.append(make_patch(spec, seed=int(rng.integers(2 ** 31)), render=render,
                                   return_residual=return_residual))
         return out
-    return make_patch(config_spec(k), seed=seed, render=render, return_residual=return_residual)
+    return make_patch(workload_spec(name), seed=seed, render=render,
+                      return_residual=return_residual)

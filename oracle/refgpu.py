@@ -1,5 +1,5 @@
 """The reference's own CUDA kernel, launched on the device copy of a patch.
-TEST AND BENCHMARK INFRASTRUCTURE ONLY (tests/ and bench.py's baseline leg).
+TEST INFRASTRUCTURE ONLY (tests/; the GPU baseline of the benchmark figures).
 
 oracle/Makefile compiles forcepho/src/compute_gaussians_kernel.cu, unchanged
 and with the reference's nvcc options, together with oracle/refgpu_launch.cu

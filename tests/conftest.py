@@ -31,7 +31,7 @@ def pytest_collection_modifyitems(config, items):
             it.add_marker(skip)
 
 
-GOLDEN_CASES = ["config0_seed1", "config0_seed7", "mini_3src_2band"]
+GOLDEN_CASES = ["single_seed1", "single_seed7", "mini_3src_2band"]
 
 
 def load_golden(name):

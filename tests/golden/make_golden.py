@@ -109,8 +109,8 @@ def slow_evaluate(gm, patch, proposal):
 
 def cases():
     """(name, patch) of the committed fixtures."""
-    out = [("config0_seed1", synth.make_config(0, seed=1)),
-           ("config0_seed7", synth.make_config(0, seed=7))]
+    out = [("single_seed1", synth.make_workload("single", seed=1)),
+           ("single_seed7", synth.make_workload("single", seed=7))]
     spec = synth.PatchSpec(n_sources=3, exposures_per_band=[2, 1], shapes=[(40, 40), (37, 45),
                                                                            (40, 40)],
                            n_psf=2, psf_sigma=(0.5, 4.0), rot_deg=1.0, scale_frac=0.02,

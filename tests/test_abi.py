@@ -58,7 +58,7 @@ def _create(st, n_bands):
 def test_create_rejects_null_and_bad_band_count():
     rc, msg, h = _create(None, 1)
     assert rc == 1 and "NULL" in msg and not h.value
-    P, prop, d = load_golden("config0_seed1")
+    P, prop, d = load_golden("single_seed1")
     rc, msg, h = _create(P.host_struct(), 0)
     assert rc == 4 and "n_bands" in msg
     rc, msg, h = _create(P.host_struct(), 31)
@@ -81,7 +81,7 @@ def test_create_rejects_overlapping_bands():
 
 
 def test_create_rejects_bad_radius_bin():
-    P, prop, d = load_golden("config0_seed1")
+    P, prop, d = load_golden("single_seed1")
     P.psfgauss = P.psfgauss.copy()
     P.psfgauss["sersic_bin"][3] = 99
     rc, msg, h = _create(P.host_struct(), 1)

@@ -77,7 +77,7 @@ def test_build_proposal_matches_host():
     from forcepho_b200 import synth
     from forcepho_b200.device_proposal import DeviceSersicTable, proposal_bytes_to_struct
     from forcepho_b200.sources import proposal_from_params
-    P = synth.make_config(1, seed=2)
+    P = synth.make_workload("field20", seed=2)
     params = P.params.copy()
     params[0, P.n_bands + 4] = 0.5      # sersic below the table: one-hot nearest radius
     params[1, P.n_bands + 5] = -0.01    # rh < 0: one-hot radius 0
@@ -96,7 +96,7 @@ def test_chi2_only_matches_full():
     torch = _torch()
     from forcepho_b200 import synth
     from forcepho_b200.autograd import PatchEvaluator
-    P = synth.make_config(1, seed=0)
+    P = synth.make_workload("field20", seed=0)
     P.send_to_device()
     ev = PatchEvaluator(P)
     theta = torch.as_tensor(P.params, device="cuda")
@@ -196,15 +196,15 @@ def oracle_workers():
 
 
 @pytest.mark.parametrize("mode", ["fused", "recompute"])
-def test_autograd_vs_fd_fp64_config0(mode, oracle_workers):
+def test_autograd_vs_fd_fp64_single(mode, oracle_workers):
     from forcepho_b200 import synth
     from forcepho_b200.autograd import PatchEvaluator
-    P = synth.make_config(0, seed=3)
+    P = synth.make_workload("single", seed=3)
     P.send_to_device()
     ev = PatchEvaluator(P, mode=mode)
     res = fd_check(P, ev, P.params, range(P.n_bands + 6), oracle_workers)
     for i, g, fd in res:
-        print(f"config 0 [{mode}] param {i}: autograd {g:.9g} fd {fd:.9g} "
+        print(f"single-source patch [{mode}] param {i}: autograd {g:.9g} fd {fd:.9g} "
               f"rel {abs(g - fd) / abs(fd):.2e}")
     P.free()
 
@@ -213,7 +213,7 @@ def test_recompute_equals_fused():
     torch = _torch()
     from forcepho_b200 import synth
     from forcepho_b200.autograd import PatchEvaluator
-    P = synth.make_config(1, seed=1)
+    P = synth.make_workload("field20", seed=1)
     P.send_to_device()
     a = PatchEvaluator(P, mode="fused")
     b = PatchEvaluator(P, mode="recompute")
@@ -224,7 +224,7 @@ def test_recompute_equals_fused():
     P.free()
 
 
-def test_autograd_vs_reference_config0_100_proposals():
+def test_autograd_vs_reference_single_100_proposals():
     """d lnlike / d theta from the autograd Function against the reference
     kernel's derivatives, stacked as FastPosterior.stack_grad does, on 100
     random proposals around the truth."""
@@ -234,7 +234,7 @@ def test_autograd_vs_reference_config0_100_proposals():
     from forcepho_b200.sources import proposal_from_params
     if not O.ref_available(1):
         pytest.skip("reference CPU kernel not built")
-    P = synth.make_config(0, seed=11)
+    P = synth.make_workload("single", seed=11)
     P.send_to_device()
     ev = PatchEvaluator(P)
     fp = FastPosterior(None, P, scene=object(), transform=BoundedTransform([0], [1]))
@@ -256,7 +256,7 @@ def test_autograd_vs_reference_config0_100_proposals():
             d_gpu = ev.dchi2.cpu().numpy().reshape(d_ref.shape)
             check_grad(d_gpu, d_ref, P, prop)
         fracs.append(np.mean(ok))
-    print("config 0: fraction of components within 1e-5 of the reference:", np.mean(fracs))
+    print("single-source patch: fraction of components within 1e-5 of the reference:", np.mean(fracs))
     P.free()
 
 
@@ -270,7 +270,7 @@ def _posterior(P, mode="fused"):
 def test_lnprob_and_grad_equals_autograd():
     torch = _torch()
     from forcepho_b200 import synth
-    P = synth.make_config(1, seed=4)
+    P = synth.make_workload("field20", seed=4)
     P.send_to_device()
     post = _posterior(P)
     z = post.inverse_transform(P.params.reshape(-1))
@@ -291,7 +291,7 @@ def test_posterior_matches_fastposterior():
     from forcepho_b200.proposal import GPUProposer
     from forcepho_b200.sources import Scene
     from forcepho_b200.autograd import default_bounds
-    P = synth.make_config(1, seed=4)
+    P = synth.make_workload("field20", seed=4)
     P.send_to_device()
     lo, hi = default_bounds(P.params, P.n_bands)
     post = _posterior(P)
@@ -311,7 +311,7 @@ def test_leapfrog_graph_equals_eager(use_autograd):
     torch = _torch()
     from forcepho_b200 import synth
     from forcepho_b200.autograd import Leapfrog
-    P = synth.make_config(1, seed=6)
+    P = synth.make_workload("field20", seed=6)
     P.send_to_device()
     post = _posterior(P)
     z0 = post.inverse_transform(P.params.reshape(-1))
@@ -331,8 +331,8 @@ def test_leapfrog_graph_equals_eager(use_autograd):
     P.free()
 
 
-def test_leapfrog_config2_500_steps():
-    """The config-1 patch through the autograd Function, 500 leapfrog steps
+def test_leapfrog_field20_500_steps():
+    """The 20-source patch through the autograd Function, 500 leapfrog steps
     of 1e-3 in the unconstrained (unit-scaled) coordinates, graph-captured.
     The leapfrog's energy error is second order in the step when the gradient
     is the derivative of lnp, so halving the step (1000 steps of 5e-4, same
@@ -341,7 +341,7 @@ def test_leapfrog_config2_500_steps():
     torch = _torch()
     from forcepho_b200 import synth
     from forcepho_b200.autograd import Leapfrog
-    P = synth.make_config(2, seed=0)
+    P = synth.make_workload("field20", seed=0)
     P.send_to_device()
     post = _posterior(P)
     z0 = post.inverse_transform(P.params.reshape(-1))
@@ -354,12 +354,12 @@ def test_leapfrog_config2_500_steps():
         lf.run(n)
         torch.cuda.synchronize()
         h1, lnp1 = float(lf.hamiltonian()), float(lf.lnp)
-        print(f"config 2 leapfrog eps={eps:g} x {n}: lnp {lnp0:.6f} -> {lnp1:.6f}, "
+        print(f"20-source patch, leapfrog eps={eps:g} x {n}: lnp {lnp0:.6f} -> {lnp1:.6f}, "
               f"H {h0:.6f} -> {h1:.6f}, dH {h1 - h0:.6g}")
         assert np.isfinite(h1)
         dh.append(abs(h1 - h0))
     ratio = dh[0] / dh[1]
-    print(f"config 2 leapfrog: dH ratio for a halved step {ratio:.3f}")
+    print(f"20-source patch, leapfrog: dH ratio for a halved step {ratio:.3f}")
     assert 3.0 < ratio < 5.0
     assert post.ev.error_word() == 0
     P.free()
@@ -370,7 +370,7 @@ def test_batch_posterior_matches_single_patches():
     from forcepho_b200 import synth
     from forcepho_b200.autograd import BatchPosterior, default_bounds
     from forcepho_b200.batch import PatchBatch
-    patches = synth.make_config(3, seed=9, n_patches=5)
+    patches = synth.make_workload("uneven", seed=9, n_patches=5)
     for p in patches:
         p.send_to_device()
     lows, highs = zip(*[default_bounds(p.params, p.n_bands) for p in patches])

@@ -14,7 +14,7 @@ def small_batch(n=6, seed=3):
     rng = np.random.default_rng(seed)
     out = []
     for i in range(n):
-        spec = synth.config_spec(3, rng)
+        spec = synth.workload_spec("uneven", rng)
         spec.shapes = [(s[0] // 3 + 16, s[1] // 3 + 16) for s in spec.shapes]
         spec.n_sources = min(spec.n_sources, 8)
         out.append(synth.make_patch(spec, seed=int(rng.integers(1 << 30))))

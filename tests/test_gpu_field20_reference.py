@@ -44,26 +44,26 @@ def pools():
             p.join()
 
 
-def test_config2_fd_fp64(pools):
+def test_field20_fd_fp64(pools):
     """Central finite differences (h = 1e-4 relative) of the all-FP64 oracle
-    on the config-2 patch for one flux per band and all six shape parameters
+    on the 20-source patch for one flux per band and all six shape parameters
     of two sources (bar: see fd_check)."""
     from forcepho_b200 import synth
     from forcepho_b200.autograd import PatchEvaluator
     from test_gpu_autograd import fd_check
-    P = synth.make_config(2, seed=0)
+    P = synth.make_workload("field20", seed=0)
     P.send_to_device()
     ev = PatchEvaluator(P)
     nb, npar = P.n_bands, P.n_bands + 6
     comps = [b * npar + b for b in range(nb)]
     comps += [0 * npar + nb + j for j in range(6)] + [7 * npar + nb + j for j in range(6)]
     for i, g, fd in fd_check(P, ev, P.params, comps, pools[1]):
-        print(f"config 2 param {i}: autograd {g:.9g} fd {fd:.9g} "
+        print(f"20-source patch, param {i}: autograd {g:.9g} fd {fd:.9g} "
               f"rel {abs(g - fd) / abs(fd):.2e}")
     P.free()
 
 
-def test_config2_autograd_vs_reference_100_proposals(pools):
+def test_field20_autograd_vs_reference_100_proposals(pools):
     ref_pool, orc_pool = pools
     if ref_pool is None:
         pytest.skip("reference CPU kernel not built")
@@ -71,7 +71,7 @@ def test_config2_autograd_vs_reference_100_proposals(pools):
     from forcepho_b200 import synth
     from forcepho_b200.autograd import LnLike, PatchEvaluator
     from forcepho_b200.sources import proposal_from_params
-    P = synth.make_config(2, seed=0)
+    P = synth.make_workload("field20", seed=0)
     P.send_to_device()
     ev = PatchEvaluator(P)
     nb, ns = P.n_bands, P.n_sources
@@ -122,7 +122,7 @@ def test_config2_autograd_vs_reference_100_proposals(pools):
             bad += 1
             details.append((k, b) + tuple(int(i) for i in idx) +
                            (g[idx], r[idx], gm[idx], scale[idx]))
-    print(f"config 2: {N_PROPOSALS} proposals, fraction of per-band gradient components "
+    print(f"20-source patch: {N_PROPOSALS} proposals, fraction of per-band gradient components "
           f"within 1e-5 of the reference: {plain.mean():.4f}; bands needing the "
           f"condition-scale criterion: {len(need)}; failing components: {bad}; "
           f"largest distance from the exact sum in residual-rounding scales: "

@@ -23,7 +23,7 @@ pytestmark = pytest.mark.gpu
 
 def _patch(seed=0):
     from forcepho_b200 import synth
-    spec = synth.config_spec(1)
+    spec = synth.workload_spec("field20")
     spec.shapes = [(48, 48)] * 32
     P = synth.make_patch(spec, seed=seed, render=synth.render_model_gpu)
     return P

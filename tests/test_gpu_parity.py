@@ -141,7 +141,7 @@ def test_variants_agree(variant):
 def test_multi_chunk_staging():
     """live_cap smaller than the kept Gaussians forces several staged chunks."""
     from forcepho_b200 import synth
-    spec = synth.config_spec(1)
+    spec = synth.workload_spec("field20")
     spec.shapes = [(48, 48)] * 32
     P = synth.make_patch(spec, seed=4)
     prop = P.proposal()
@@ -209,10 +209,10 @@ def test_swap_on_device_invariant():
     P.free()
 
 
-def test_config1_full_size():
-    """Config 1 at full size against FP64 and the reference kernel."""
+def test_field20_full_size():
+    """The 20-source patch at full size against FP64 and the reference kernel."""
     from forcepho_b200 import synth
-    P = synth.make_config(1, seed=0)
+    P = synth.make_workload("field20", seed=0)
     prop = P.proposal()
     chi2, dchi2 = gpu_eval(P, prop)
     c64, g64 = O.oracle_evaluate(P, prop, precision="f64")
@@ -220,9 +220,9 @@ def test_config1_full_size():
     rc, rd = O.ref_evaluate(P, prop)
     np.testing.assert_allclose(chi2, rc, rtol=CHI2_RTOL)
     np.testing.assert_allclose(chi2, c64, rtol=CHI2_RTOL)
-    print("config1", grad_report(dchi2, rd, g64, gm))
+    print("20-source patch", grad_report(dchi2, rd, g64, gm))
     frac = check_grad(dchi2, rd, P, prop)
-    print("config1 fraction within 1e-5 of the reference:", frac)
+    print("20-source patch: fraction within 1e-5 of the reference:", frac)
 
 
 @pytest.mark.parametrize("name", GOLDEN_CASES)
@@ -264,7 +264,7 @@ def test_persistent_schedule_identical(variant):
     and on later ones, with the proposal changing in between."""
     import torch
     from forcepho_b200 import _lib, synth
-    P = synth.make_config(1, seed=5)
+    P = synth.make_workload("field20", seed=5)
     P.send_to_device()
     h = P.device_patch.handle
     nb, ns = P.n_bands, P.n_sources

@@ -35,7 +35,7 @@ def _run_ref_gpu(P, prop):
     return chi2.cpu().numpy(), d
 
 
-@pytest.mark.parametrize("name", ["config0_seed1", "mini_3src_2band"])
+@pytest.mark.parametrize("name", ["single_seed1", "mini_3src_2band"])
 def test_reference_gpu_kernel_runs(name):
     if not refgpu.available():
         pytest.skip("reference CUDA kernel not built")
@@ -53,7 +53,7 @@ def test_reference_gpu_kernel_runs(name):
           f"ours {rel(g_us, g_ref):.2e}")
 
 
-def test_reference_gpu_kernel_timing_config1():
+def test_reference_gpu_kernel_timing_field20():
     """Times the reference CUDA kernel against this project's kernel on the
     20-source, 8-band x 4-exposure, 128x128 px patch (device-resident inputs,
     CUDA events, L2 flushed between evaluations) and checks that the two agree
@@ -62,7 +62,7 @@ def test_reference_gpu_kernel_timing_config1():
         pytest.skip("reference CUDA kernel not built")
     import torch
     from forcepho_b200 import _lib, synth
-    P = synth.make_config(1, seed=0, render=synth.render_model_gpu)
+    P = synth.make_workload("field20", seed=0, render=synth.render_model_gpu)
     prop = P.proposal()
     nb, ns = P.n_bands, P.n_sources
     P.send_to_device()
@@ -101,13 +101,13 @@ def test_reference_gpu_kernel_timing_config1():
     t_ref = timed(ref_gpu, 5)
     t_us = timed(ours, 20)
     np.testing.assert_allclose(c_rg.cpu().numpy(), c_us.cpu().numpy(), rtol=1e-5)
-    print(f"config 1: reference CUDA kernel {t_ref:.3f} ms per evaluation "
+    print(f"20-source patch: reference CUDA kernel {t_ref:.3f} ms per evaluation "
           f"({1e3 / t_ref:.1f} evals/s), this project's {t_us:.3f} ms ({1e3 / t_us:.1f} evals/s): "
           f"{t_ref / t_us:.1f}x")
     P.free()
 
 
-def test_reference_gpu_kernel_timing_config0_and_batch():
+def test_reference_gpu_kernel_timing_single_and_uneven():
     """Times the reference CUDA kernel on the single-source 64x64 px patch and
     on 256 uneven patches (one launch per patch, as GPUProposer launches it),
     beside this project's plain loop and batched form on the same patches;
@@ -155,7 +155,7 @@ def test_reference_gpu_kernel_timing_config0_and_batch():
         return float(np.median(ts))
 
     # the single-source patch
-    it0 = [setup(synth.make_config(0, seed=1, render=synth.render_model_gpu))]
+    it0 = [setup(synth.make_workload("single", seed=1, render=synth.render_model_gpu))]
     t_ref0, t_us0 = timed(lambda: ref_all(it0), 20), timed(lambda: ours_all(it0), 20)
     np.testing.assert_allclose(it0[0]["c_rg"].cpu().numpy(), it0[0]["c_us"].cpu().numpy(),
                                rtol=1e-5)
@@ -164,7 +164,7 @@ def test_reference_gpu_kernel_timing_config0_and_batch():
     it0[0]["P"].free()
 
     # 256 uneven patches
-    patches = synth.make_config(3, seed=3, render=synth.render_model_gpu, n_patches=256)
+    patches = synth.make_workload("uneven", seed=3, render=synth.render_model_gpu, n_patches=256)
     items = [setup(P) for P in patches]
     t_ref = timed(lambda: ref_all(items), 3)
     t_us = timed(lambda: ours_all(items), 3)

@@ -76,7 +76,7 @@ def test_chain_copies_match_single_patch():
     import torch
     from forcepho_b200 import synth
     from forcepho_b200.autograd import DevicePosterior
-    P = synth.make_config(1, seed=3)
+    P = synth.make_workload("field20", seed=3)
     post, lo, hi = _chains(P, 3)
     P.send_to_device()
     # the batch evaluates 64x8 tiles with 128-record stages: same for the single patch
@@ -107,7 +107,7 @@ def test_many_chains_on_single_source_patch():
     import torch
     from forcepho_b200 import synth
     from forcepho_b200.sampling import MultiChainHMC
-    P = synth.make_config(0, seed=2)
+    P = synth.make_workload("single", seed=2)
     k = 32
     post, lo, hi = _chains(P, k)
     z0 = post.inverse_transform(np.tile(P.params.reshape(-1), k))

@@ -28,13 +28,13 @@ def _rel(a, b):
     return np.abs(a - b) / np.maximum(np.abs(b), 1e-300)
 
 
-def test_config4_precision():
+def test_stress60_precision():
     if not O.ref_available(60):
         pytest.skip("reference CPU kernel (64-source build) not built")
     import torch
     from forcepho_b200 import _lib, synth
     from forcepho_b200.proposal import GPUProposer
-    P = synth.make_config(4, seed=0, render=synth.render_model_gpu)
+    P = synth.make_workload("stress60", seed=0, render=synth.render_model_gpu)
     prop = P.proposal()
     nb, ns = P.n_bands, P.n_sources
     P.send_to_device()
@@ -86,17 +86,17 @@ def test_config4_precision():
     ok = grad_ok(dchi2, d_ref, gm, sc, rs)
     plain = _rel(dchi2, d_ref) <= 1e-5
     nz = np.abs(d64) > 0
-    print(f"config 4: {ms:.2f} ms per evaluation on the device "
+    print(f"60-source patch: {ms:.2f} ms per evaluation on the device "
           f"({P.pairs_per_eval / (ms * 1e-3):.3e} nominal pix-gauss/s)")
-    print(f"config 4 chi2 rel. error vs FP64: ours max {_rel(chi2, c64).max():.3e}, "
+    print(f"60-source patch, chi2 rel. error vs FP64: ours max {_rel(chi2, c64).max():.3e}, "
           f"reference max {_rel(c_ref, c64).max():.3e}; ours vs reference max "
           f"{_rel(chi2, c_ref).max():.3e}")
-    print(f"config 4 gradient rel. error vs FP64 (median / 99th pct / max over "
+    print(f"60-source patch, gradient rel. error vs FP64 (median / 99th pct / max over "
           f"{int(nz.sum())} components): ours {np.median(_rel(dchi2, d64)[nz]):.2e} / "
           f"{np.percentile(_rel(dchi2, d64)[nz], 99):.2e} / {_rel(dchi2, d64)[nz].max():.2e}; "
           f"reference {np.median(_rel(d_ref, d64)[nz]):.2e} / "
           f"{np.percentile(_rel(d_ref, d64)[nz], 99):.2e} / {_rel(d_ref, d64)[nz].max():.2e}")
-    print(f"config 4 gradient: {plain.mean():.4f} of components within 1e-5 of the reference; "
+    print(f"60-source patch, gradient: {plain.mean():.4f} of components within 1e-5 of the reference; "
           f"largest distance from the exact sum in residual-rounding scales: ours "
           f"{res_multiple(dchi2, gm, rs):.3g}, reference {res_multiple(d_ref, gm, rs):.3g}")
     assert np.all(ok), f"{int((~ok).sum())} gradient components outside the bar"

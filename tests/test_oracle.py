@@ -61,7 +61,7 @@ def test_cutoff_changes_little():
 
 
 def test_residual_output_matches_model():
-    P, prop, d = load_golden("config0_seed1")
+    P, prop, d = load_golden("single_seed1")
     chi2, dchi2, res = O.oracle_evaluate(P, prop, residual=True)
     # chi2 recomputed from the residual with the kernel's offset form
     rie = res * P.ierr

@@ -38,7 +38,7 @@ def device_struct_for(P, torch):
     return st, keep
 
 
-@pytest.mark.parametrize("name", ["mini_3src_2band", "config0_seed1"])
+@pytest.mark.parametrize("name", ["mini_3src_2band", "single_seed1"])
 def test_noalloc_matches_handle_path_twice(name):
     import torch
     from forcepho_b200 import _lib
@@ -76,7 +76,7 @@ def test_noalloc_rejects_oversize():
     FPHO_ERR_LIMIT and a message, before anything is launched."""
     import torch
     from forcepho_b200 import _lib
-    P, prop, d = load_golden("config0_seed1")
+    P, prop, d = load_golden("single_seed1")
     st, keep = device_struct_for(P, torch)
     out = torch.zeros(8, dtype=torch.float64, device="cuda")
     rc = _lib.lib.fpho_evaluate_proposal_noalloc(st.ctypes.data, 1, 60000, 2 ** 30, 1024,
