@@ -149,6 +149,24 @@ def cpu_reference_time(P, prop, reps, cores):
     return times
 
 
+def max_over_ranks(x, world, device="cuda"):
+    """The largest `x` over the ranks (every rank takes part; NCCL needs a CUDA
+    tensor, gloo a CPU one)."""
+    if world <= 1:
+        return float(x)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(steps, seconds, world):
+    """Evaluations per second of the whole job: every rank evaluates `steps`
+    patches, the job takes the slowest rank's `seconds`."""
+    return world * steps / seconds
+
+
 def _cpu_model():
     try:
         with open("/proc/cpuinfo") as f:
@@ -559,13 +577,9 @@ def run_ours(args):
         tile_ms.append(tms.value)
     _lib.call("fpho_patch_time_tiles", dp.handle, 0)
 
-    total_ms = float(np.sum(step_ms))
-    t = torch.tensor([total_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms = float(t.item())
+    total_ms = max_over_ranks(float(np.sum(step_ms)), world)
     ms_per_step = total_ms / args.steps
-    value = world * args.steps / (total_ms * 1e-3)
+    value = whole_job_rate(args.steps, total_ms * 1e-3, world)
 
     # end-to-end through the public API: pinned host proposal -> results on host
     hprop = torch.from_numpy(prop.view(np.uint8).copy()).pin_memory()
@@ -583,11 +597,8 @@ def run_ours(args):
     t0 = time.perf_counter()
     for _ in range(args.steps):
         e2e_step()
-    e2e_s = time.perf_counter() - t0
-    te = torch.tensor([e2e_s], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * args.steps / float(te.item())
+    e2e_s = max_over_ranks(time.perf_counter() - t0, world)
+    e2e_value = whole_job_rate(args.steps, e2e_s, world)
 
     fp32_tflops, ex2_gops = probe_fp32(torch, _lib)
     tile_s = float(np.mean(tile_ms)) * 1e-3
