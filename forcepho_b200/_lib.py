@@ -58,6 +58,7 @@ _SIGS = {
     "fpho_patch_free": (c_int, [c_void_p]),
     "fpho_patch_set_config": (c_int, [c_void_p, c_int, c_int, c_void_p]),
     "fpho_patch_set_schedule": (c_int, [c_void_p, c_int]),
+    "fpho_patch_set_test_stall": (c_int, [c_void_p, c_int]),
     "fpho_patch_design_matrix": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p]),
     "fpho_variant_info": (c_int, [c_int, ctypes.POINTER(c_int)]),
     "fpho_patch_count_pairs": (c_int, [c_void_p, c_int, ctypes.POINTER(ctypes.c_longlong)]),

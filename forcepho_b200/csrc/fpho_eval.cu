@@ -630,6 +630,21 @@ extern "C" int fpho_patch_set_config(fpho_patch *p, int variant, int live_cap, v
     return FPHO_OK;
 }
 
+extern "C" int fpho_patch_set_test_stall(fpho_patch *p, int on) {
+    clear_error();
+    if (!p) return set_error(FPHO_ERR_INVALID, "NULL patch");
+    // one staging per tile only: after a wait that gave up, a second staging
+    // on the same barrier could run ahead of its copies
+    if (on && p->max_g > p->live_cap)
+        return set_error(FPHO_ERR_STATE,
+                         "the test stall needs every exposure's %d image Gaussians to fit one "
+                         "stage of %d records", p->max_g, p->live_cap);
+    if (on && p->schedule == 1 && p->n_tiles > 4 * device_sms())
+        return set_error(FPHO_ERR_STATE, "the test stall needs one CTA per tile (schedule 0)");
+    p->test_extra_tx = on ? 16 : 0;
+    return FPHO_OK;
+}
+
 extern "C" int fpho_patch_set_schedule(fpho_patch *p, int schedule) {
     clear_error();
     if (!p) return set_error(FPHO_ERR_INVALID, "NULL patch");
@@ -692,6 +707,7 @@ int enqueue_evaluate(fpho_patch *p, const fpho_source *d_prop, double *d_chi2, f
     A.idx_cap = std::max(p->max_g, 1);
     A.err = p->d_err;
     A.pairs = p->count_pairs ? p->d_pairs : nullptr;
+    A.test_extra_tx = p->test_extra_tx;
     if (p->ev_tile0) CUDA_TRY(cudaEventRecord(p->ev_tile0, s));
     int rc;
     // the order only matters when the tiles outnumber what runs at once

@@ -45,6 +45,7 @@ struct fpho_patch {
     // tile scheduling: 0 = one CTA per tile (hardware order), 1 = persistent
     // CTAs taking tiles by decreasing cost of the previous evaluation
     int schedule = 1;
+    int test_extra_tx = 0;  // see fpho_patch_set_test_stall
     int *d_tile_cost = nullptr, *d_tile_order = nullptr, *d_tile_counter = nullptr;
     // workspace
     float *d_gtab = nullptr;

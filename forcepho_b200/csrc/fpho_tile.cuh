@@ -42,6 +42,8 @@ struct TileArgs {
     int *err;                 // error word (bit 0: bulk-copy wait gave up)
     long long *pairs;         // optional: evaluated (pixel, Gaussian) pairs, or nullptr
     int *tile_cost = nullptr; // optional: [n_tiles] kept Gaussians x pixels, written per tile
+    int test_extra_tx = 0;    // test of the error path only: bytes the staging wait
+                              // expects beyond those copied, so that it runs out
 };
 
 // ------------------------------------------------------------ mbarrier + bulk copy
@@ -520,7 +522,8 @@ __device__ __forceinline__ void tile_body(const TileArgs &A, int tile, unsigned 
     auto stage = [&](int c0, int n) {
         fence_proxy_async_smem();
         if (warp == 0) {
-            if (lane == 0) mbar_arrive_expect_tx(mbar, (uint32_t)n * GSTAGE * 4);
+            if (lane == 0)
+                mbar_arrive_expect_tx(mbar, (uint32_t)(n * GSTAGE * 4 + A.test_extra_tx));
             __syncwarp();
             for (int i = lane; i < n; i += 32)
                 bulk_g2s(recs + (size_t)i * GSTAGE,

@@ -325,6 +325,18 @@ FPHO_API int fpho_patch_set_config(fpho_patch *p, int variant, int live_cap, voi
  * reference launches one block per band). */
 FPHO_API int fpho_patch_set_schedule(fpho_patch *p, int schedule);
 
+/* For tests of the error path only (no reference counterpart): with `on`
+ * non-zero, every staging wait of this patch's tile kernel expects 16 bytes
+ * that no copy delivers, so each wait gives up after its bounded spin (about
+ * 2^22 polls), sets the error word and the evaluation returns
+ * FPHO_ERR_KERNEL (host I/O) or leaves the word for fpho_patch_error_word.
+ * Nothing hangs or faults, and the results of such an evaluation are
+ * meaningless.  Switch it off to evaluate normally again.  Refused
+ * (FPHO_ERR_STATE) unless every tile is staged at most once and runs in its
+ * own CTA: more image Gaussians per exposure than the stage holds, or a
+ * persistent schedule over many tiles. */
+FPHO_API int fpho_patch_set_test_stall(fpho_patch *p, int on);
+
 /* Enable counting of evaluated (pixel, image Gaussian) pairs, i.e. pairs that
  * survive the per-tile culling; *last_count receives the count of the last
  * evaluation (synchronizes).  last_count may be NULL. */
