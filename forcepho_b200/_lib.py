@@ -56,6 +56,17 @@ _SIGS = {
     "fpho_patch_device_struct": (c_int, [c_void_p, ctypes.POINTER(c_void_p)]),
     "fpho_patch_info": (c_int, [c_void_p, c_int64_p]),
     "fpho_patch_free": (c_int, [c_void_p]),
+    "fpho_patch_create_device_pixels": (c_int, [c_void_p, c_int, c_int, c_void_p,
+                                                ctypes.POINTER(c_void_p)]),
+    "fpho_store_create": (c_int, [c_int, c_int, c_int, c_int, ctypes.POINTER(c_void_p)]),
+    "fpho_store_add_exposure": (c_int, [c_void_p, c_void_p, c_int, c_void_p,
+                                        ctypes.POINTER(c_int)]),
+    "fpho_store_info": (c_int, [c_void_p, c_int64_p]),
+    "fpho_store_count": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "fpho_store_gather": (c_int, [c_void_p, c_int, c_void_p, c_void_p, c_void_p, ctypes.c_float,
+                                  c_void_p, c_void_p, c_void_p, c_void_p, ctypes.c_int64,
+                                  c_void_p, c_void_p, c_void_p]),
+    "fpho_store_free": (c_int, [c_void_p]),
     "fpho_patch_set_config": (c_int, [c_void_p, c_int, c_int, c_void_p]),
     "fpho_patch_set_schedule": (c_int, [c_void_p, c_int]),
     "fpho_patch_set_test_stall": (c_int, [c_void_p, c_int]),

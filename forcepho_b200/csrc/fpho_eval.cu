@@ -259,10 +259,11 @@ void dfree(T *&p) {
     p = nullptr;
 }
 template <typename T>
-int dupload(T **dst, const T *src, size_t n, cudaStream_t s) {
+int dupload(T **dst, const T *src, size_t n, cudaStream_t s,
+            cudaMemcpyKind kind = cudaMemcpyHostToDevice) {
     int rc = dalloc(dst, n);
     if (rc) return rc;
-    if (n) CUDA_TRY(cudaMemcpyAsync(*dst, src, n * sizeof(T), cudaMemcpyHostToDevice, s));
+    if (n) CUDA_TRY(cudaMemcpyAsync(*dst, src, n * sizeof(T), kind, s));
     return FPHO_OK;
 }
 
@@ -489,8 +490,9 @@ int build_plan(fpho_patch *p, cudaStream_t s) {
 }  // namespace
 
 // ======================================================================= C ABI
-extern "C" int fpho_patch_create(const fpho_patch_struct *host, int n_bands, int return_residual,
-                                 void *stream, fpho_patch **out) {
+// `pixel_kind`: where host->data, ierr, xpix and ypix live (host or device).
+static int create_patch(const fpho_patch_struct *host, int n_bands, int return_residual,
+                        void *stream, fpho_patch **out, cudaMemcpyKind pixel_kind) {
     clear_error();
     if (!out) return set_error(FPHO_ERR_INVALID, "out is NULL");
     *out = nullptr;
@@ -502,10 +504,10 @@ extern "C" int fpho_patch_create(const fpho_patch_struct *host, int n_bands, int
     if (!rc) rc = upload_meta(p, host, s, /*validate_only=*/true);
     if (!rc) {
         const size_t np = (size_t)p->npix;
-        if (!rc) rc = dupload(&p->d_data, host->data, np, s);
-        if (!rc) rc = dupload(&p->d_ierr, host->ierr, np, s);
-        if (!rc) rc = dupload(&p->d_xpix, host->xpix, np, s);
-        if (!rc) rc = dupload(&p->d_ypix, host->ypix, np, s);
+        if (!rc) rc = dupload(&p->d_data, host->data, np, s, pixel_kind);
+        if (!rc) rc = dupload(&p->d_ierr, host->ierr, np, s, pixel_kind);
+        if (!rc) rc = dupload(&p->d_xpix, host->xpix, np, s, pixel_kind);
+        if (!rc) rc = dupload(&p->d_ypix, host->ypix, np, s, pixel_kind);
         if (!rc) rc = dupload(&p->d_exposure_start, p->exposure_start.data(), (size_t)p->n_exp, s);
         if (!rc) rc = dupload(&p->d_exposure_N, p->exposure_N.data(), (size_t)p->n_exp, s);
         if (!rc) rc = dupload(&p->d_band_start, p->band_start.data(), (size_t)p->n_bands, s);
@@ -531,6 +533,17 @@ extern "C" int fpho_patch_create(const fpho_patch_struct *host, int n_bands, int
     }
     *out = p;
     return FPHO_OK;
+}
+
+extern "C" int fpho_patch_create(const fpho_patch_struct *host, int n_bands, int return_residual,
+                                 void *stream, fpho_patch **out) {
+    return create_patch(host, n_bands, return_residual, stream, out, cudaMemcpyHostToDevice);
+}
+
+extern "C" int fpho_patch_create_device_pixels(const fpho_patch_struct *desc, int n_bands,
+                                               int return_residual, void *stream,
+                                               fpho_patch **out) {
+    return create_patch(desc, n_bands, return_residual, stream, out, cudaMemcpyDeviceToDevice);
 }
 
 extern "C" int fpho_patch_replace_meta(fpho_patch *p, const fpho_patch_struct *host, void *stream) {

@@ -25,12 +25,15 @@ _ARRAY_CODE = {"data": 0, "residual": 1, "ierr": 2, "xpix": 3, "ypix": 4}
 class DevicePatch:
     """Owner of one ``fpho_patch`` handle (device copy of a patch + workspace)."""
 
-    def __init__(self, patch, return_residual=False, stream=None):
-        st = patch.host_struct()
+    def __init__(self, patch, return_residual=False, stream=None, device_pixels=None):
+        """`device_pixels`: {"data", "ierr", "xpix", "ypix": device address}
+        to create the patch from pixel arrays already on the device."""
+        st = patch.host_struct(pointers=device_pixels)
         self._keep = st  # host arrays stay referenced by `patch`
         h = ctypes.c_void_p()
-        _lib.call("fpho_patch_create", st.ctypes.data, int(patch.n_bands),
-                  int(bool(return_residual)), stream, ctypes.byref(h))
+        create = "fpho_patch_create_device_pixels" if device_pixels else "fpho_patch_create"
+        _lib.call(create, st.ctypes.data, int(patch.n_bands), int(bool(return_residual)), stream,
+                  ctypes.byref(h))
         self.handle = h.value
         self.return_residual = bool(return_residual)
 

@@ -1,0 +1,236 @@
+"""Exposures held in GPU memory, and patches packed from them on the device.
+
+The reference packs every patch on the host: it reads each overlapping
+exposure's whole super-pixel array from the HDF5 pixel store, tests every
+super-pixel's corners against the region with numpy, and concatenates the
+selected pixels before copying them to the GPU
+(forcepho/patches/pixel_patch.py:124-198, 297-342).  When patches are fit
+one after another that work repeats for every patch.
+
+:class:`DeviceStore` uploads the exposures once (the ``fpho_store`` of the C
+ABI: 32 MiB per 2048x2048 exposure, so a B200 holds thousands) and
+:class:`GPUStorePatch` -- a :class:`~.pixel_patch.StorePatch` with the GPU
+mix-in -- selects super-pixels and packs the patch's pixel arrays with CUDA
+kernels straight into device memory, in the reference's order, so the host
+keeps only the index arrays and the per-scene metadata.
+"""
+
+import ctypes
+
+import numpy as np
+
+from .. import _lib
+from ..region import REGION_CIRCLE, REGION_RECT
+from .device_patch import DevicePatch, GPUPatchMixin
+from .pixel_patch import StorePatch
+
+__all__ = ["DeviceStore", "GPUStorePatch", "REGION_DTYPE", "region_records"]
+
+# fpho_region of include/fpho.h
+REGION_DTYPE = np.dtype([("kind", np.int32), ("reserved", np.int32), ("p", np.float64, 14)])
+
+
+def region_records(region, wcses):
+    """One ``fpho_region`` record per exposure WCS."""
+    out = np.zeros(len(wcses), dtype=REGION_DTYPE)
+    for i, w in enumerate(wcses):
+        kind, p = region.device_params(w)
+        if kind not in (REGION_CIRCLE, REGION_RECT):
+            raise ValueError(f"region kind {kind}")
+        out[i]["kind"] = kind
+        out[i]["p"][:len(p)] = p
+    return out
+
+
+class DeviceStore:
+    """Super-pixel exposures resident in GPU memory.
+
+    Parameters
+    ----------
+    nside : int or (nx, ny), image size in pixels
+    super_pixel_size : int
+    max_exposures : capacity (all device memory is allocated here)
+    """
+
+    def __init__(self, nside, super_pixel_size=8, max_exposures=64):
+        nx, ny = (int(nside), int(nside)) if np.ndim(nside) == 0 else (int(nside[0]),
+                                                                       int(nside[1]))
+        h = ctypes.c_void_p()
+        _lib.call("fpho_store_create", nx, ny, int(super_pixel_size), int(max_exposures),
+                  ctypes.byref(h))
+        self.handle = h.value
+        self.nside = (nx, ny)
+        self.super_pixel_size = int(super_pixel_size)
+        self.names = []
+
+    @classmethod
+    def from_pixelstore(cls, pixelstore, paths=None, max_exposures=None):
+        """Upload exposures (``"band/expID"`` paths; default all) of a
+        :class:`~.storage.PixelStore`."""
+        paths = list(paths) if paths is not None else pixelstore.exposure_paths()
+        st = cls(pixelstore.imsize, pixelstore.super_pixel_size,
+                 max_exposures or max(len(paths), 1))
+        for p in paths:
+            st.add(pixelstore.data[p + "/data"].array(), name=p)
+        return st
+
+    def add(self, superpixels, name=None, stream=None):
+        """Append one exposure: an (nsx, nsy, 2 s^2) float32 array on the host
+        or a CUDA tensor of that shape.  Returns its index."""
+        nsx, nsy = self.nside[0] // self.super_pixel_size, self.nside[1] // self.super_pixel_size
+        shape = (nsx, nsy, 2 * self.super_pixel_size ** 2)
+        idx = ctypes.c_int()
+        if hasattr(superpixels, "is_cuda") and superpixels.is_cuda:
+            import torch
+            t = superpixels.contiguous().to(torch.float32)
+            if tuple(t.shape) != shape:
+                raise ValueError(f"super-pixel array of shape {tuple(t.shape)}, expected {shape}")
+            _lib.call("fpho_store_add_exposure", self.handle, t.data_ptr(), 1, stream,
+                      ctypes.byref(idx))
+            if stream is None:
+                torch.cuda.synchronize()
+        else:
+            a = np.ascontiguousarray(superpixels, dtype=np.float32)
+            if a.shape != shape:
+                raise ValueError(f"super-pixel array of shape {a.shape}, expected {shape}")
+            _lib.call("fpho_store_add_exposure", self.handle, a.ctypes.data, 0, stream,
+                      ctypes.byref(idx))
+        self.names.append(name if name is not None else str(idx.value))
+        return idx.value
+
+    def index(self, name):
+        return self.names.index(name)
+
+    def info(self):
+        out = (ctypes.c_int64 * 6)()
+        _lib.call("fpho_store_info", self.handle, out)
+        return dict(zip(["nsx", "nsy", "super_pixel_size", "n_exposures", "capacity",
+                         "bytes_per_exposure"], list(out)))
+
+    def count(self, indices, regions, stream=None):
+        """Selected super-pixels of each exposure (`regions`: REGION_DTYPE
+        records, one per index)."""
+        idx = np.ascontiguousarray(indices, dtype=np.int32)
+        reg = np.ascontiguousarray(regions, dtype=REGION_DTYPE)
+        out = np.zeros(len(idx), dtype=np.int32)
+        _lib.call("fpho_store_count", self.handle, len(idx), idx.ctypes.data, reg.ctypes.data,
+                  out.ctypes.data, stream)
+        return out
+
+    def gather(self, indices, regions, background=None, max_snr=None, npix=None, stream=None):
+        """Pack the selected pixels: returns (data, ierr, xpix, ypix) float32
+        CUDA tensors and the exposure_start, exposure_N arrays."""
+        import torch
+        idx = np.ascontiguousarray(indices, dtype=np.int32)
+        reg = np.ascontiguousarray(regions, dtype=REGION_DTYPE)
+        if npix is None:
+            npix = int(self.count(idx, reg, stream).astype(np.int64).sum()) \
+                * self.super_pixel_size ** 2
+        bufs = [torch.empty(max(npix, 1), dtype=torch.float32, device="cuda") for _ in range(4)]
+        bg = None if background is None else np.ascontiguousarray(background, dtype=np.float32)
+        start = np.zeros(len(idx), dtype=np.int32)
+        n = np.zeros(len(idx), dtype=np.int32)
+        if stream is None:
+            stream = torch.cuda.current_stream().cuda_stream
+        _lib.call("fpho_store_gather", self.handle, len(idx), idx.ctypes.data, reg.ctypes.data,
+                  None if bg is None else bg.ctypes.data, float(max_snr or 0.0),
+                  *[b.data_ptr() for b in bufs], int(npix), start.ctypes.data, n.ctypes.data,
+                  stream)
+        total = int(n.astype(np.int64).sum())
+        return [b[:total] for b in bufs], start, n
+
+    def free(self):
+        if getattr(self, "handle", None):
+            _lib.lib.fpho_store_free(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class GPUStorePatch(StorePatch, GPUPatchMixin):
+    """A :class:`~.pixel_patch.StorePatch` whose super-pixel selection and
+    pixel packing run on the GPU over a :class:`DeviceStore`.
+
+    The exposures found and the packed arrays are those of the host
+    ``StorePatch`` (bounding-box corner check on the host, then exposures with
+    at least one super-pixel in the region).  The pixel arrays stay on the
+    device (``pixels``: data, ierr, xpix, ypix tensors);
+    :meth:`pixels_to_host` copies them into the usual attributes.
+
+    Parameters are those of ``StorePatch`` plus ``device_store`` (default:
+    upload every exposure of the pixel store).
+    """
+
+    def __init__(self, pixelstore="", metastore="", psfstore="", splinedata="",
+                 spline_smoothing=None, return_residual=False, device_store=None, debug=0):
+        super().__init__(pixelstore=pixelstore, metastore=metastore, psfstore=psfstore,
+                         splinedata=splinedata, spline_smoothing=spline_smoothing,
+                         return_residual=return_residual, debug=debug)
+        self.device_store = device_store or DeviceStore.from_pixelstore(self.pixelstore)
+        self.pixels = None
+        self.device_patch = None
+
+    def find_exposures(self, region, bandlist):
+        imsize = np.zeros(2) + self.pixelstore.nside_full
+        bra, bdec = region.bounding_box
+        cand = []
+        for band in bandlist:
+            if band not in self.metastore.headers:
+                continue
+            for expID in self.metastore.headers[band].keys():
+                wcs = self.metastore.get_wcs(band, expID)
+                bx, by = wcs.world_to_pixel_values(bra, bdec)
+                if np.any((bx > 0) & (bx < imsize[0]) & (by > 0) & (by < imsize[1])):
+                    cand.append((band, expID, wcs))
+        if not cand:
+            return [], [], [], []
+        idx = [self.device_store.index(f"{b}/{e}") for b, e, _ in cand]
+        counts = self.device_store.count(idx, region_records(region, [w for _, _, w in cand]))
+        keep = [c for c, n in zip(cand, counts) if n > 0]
+        return ([self.metastore.headers[b][e] for b, e, _ in keep], [w for _, _, w in keep],
+                [f"{b}/{e}" for b, e, _ in keep], [b for b, _, _ in keep])
+
+    def pack_pix(self, region, dtype=None):
+        idx = [self.device_store.index(p) for p in self.epaths]
+        regs = region_records(region, self.wcses)
+        pix, start, n = self.device_store.gather(idx, regs, background=self.background_offsets,
+                                                 max_snr=getattr(self, "max_snr", None))
+        self.pixels = dict(zip(["data", "ierr", "xpix", "ypix"], pix))
+        for k in ("data", "ierr", "xpix", "ypix"):
+            self.__dict__.pop(k, None)
+        self.exposure_start, self.exposure_N = start, n
+        nb = len(self.uniq_bands)
+        self.band_N = np.zeros(nb, dtype=np.int16)
+        b = 0
+        for e in range(len(self.epaths)):
+            if e > 0 and self.bands[e] != self.bands[e - 1]:
+                b += 1
+            self.band_N[b] += 1
+        self.band_start = np.zeros(nb, dtype=np.int16)
+        self.band_start[1:] = np.cumsum(self.band_N)[:-1]
+
+    @property
+    def npix(self):
+        return int(np.asarray(self.exposure_N, dtype=np.int64).sum())
+
+    def pixels_to_host(self):
+        """Copy the device pixel arrays into ``data``, ``ierr``, ``xpix``,
+        ``ypix`` (numpy), as the host StorePatch holds them."""
+        for k, t in self.pixels.items():
+            setattr(self, k, t.cpu().numpy())
+        return self
+
+    def send_to_device(self):
+        if self.pixels is None:
+            raise RuntimeError("build_patch (or pack_pix) must run before send_to_device")
+        ptrs = {k: t.data_ptr() for k, t in self.pixels.items()}
+        for k in ("data", "ierr", "xpix", "ypix"):   # host_struct coerces these if present
+            self.__dict__.pop(k, None)
+        self.device_patch = DevicePatch(self, return_residual=self.return_residual,
+                                        device_pixels=ptrs)
+        self._dirty_data = False
+        return self.device_patch

@@ -9,7 +9,7 @@ with the ``Patch`` struct of the device ABI (forcepho/src/patch.cc:23-99,
 
 import numpy as np
 
-__all__ = ["PatchBase", "PSF_COLS", "PSF_DTYPE"]
+__all__ = ["PatchBase", "Patch", "PSF_COLS", "PSF_DTYPE"]
 
 # PSF Gaussian columns, as forcepho/patches/storage.py:35-36
 PSF_COLS = ["amp", "xcen", "ycen", "Cxx", "Cyy", "Cxy"]
@@ -143,13 +143,18 @@ class PatchBase:
                 continue
             setattr(self, name, np.ascontiguousarray(a, dtype=dt))
 
-    def host_struct(self, residual=None):
+    def host_struct(self, residual=None, pointers=None):
         """A ``patch_struct_dtype`` record holding HOST pointers to this
-        patch's arrays (the form :func:`fpho_patch_create` reads)."""
+        patch's arrays (the form :func:`fpho_patch_create` reads).
+        `pointers` ({field: address}) overrides fields, e.g. device pixel
+        arrays for ``fpho_patch_create_device_pixels``."""
         self.coerce_arrays()
+        pointers = pointers or {}
         st = np.zeros(1, dtype=self.patch_struct_dtype)
         for name in self.patch_struct_dtype.names:
-            if self.patch_struct_dtype[name] == self.ptr_dtype:
+            if name in pointers:
+                st[name] = pointers[name]
+            elif self.patch_struct_dtype[name] == self.ptr_dtype:
                 if name == "residual":
                     st[name] = 0 if residual is None else residual.ctypes.data
                 else:
@@ -167,3 +172,126 @@ class PatchBase:
         """Split a pixel array into one array per band."""
         arr = getattr(self, attr)
         return np.split(arr, np.cumsum(self.band_N_pix[:-1]))
+
+
+class Patch(PatchBase):
+    """A patch whose per-scene metadata is packed from exposure WCSs, a PSF
+    store and a Sersic spline table (forcepho/patches/patch.py:200-424:
+    ``pack_meta``, ``_pack_source_metadata``, ``_pack_astrometry``,
+    ``_pack_fluxcal``, ``_pack_psf``, ``set_scene``, ``zerocoords``).
+
+    Subclasses fill the pixel arrays and the exposure lists ``wcses``,
+    ``hdrs``, ``bands``, ``bandlist``, ``n_exp_per_band``.
+
+    Parameters
+    ----------
+    psfstore : path of a PSF store (HDF5), or ""
+    splinedata : path of a Sersic spline table (forcepho's ``.h5`` or this
+        package's ``.npz``); "" uses the packaged table
+    spline_smoothing : smoothing of the amplitude splines
+    """
+
+    def __init__(self, psfstore="", splinedata="", spline_smoothing=None,
+                 return_residual=False, meta_dtype=np.float32, pix_dtype=np.float32, debug=0):
+        super().__init__(return_residual=return_residual, meta_dtype=meta_dtype,
+                         pix_dtype=pix_dtype)
+        from .storage import PSFStore
+        self.debug = debug
+        self.psfstore = PSFStore(psfstore) if psfstore else None
+        self.splinedata = splinedata
+        self.spline_smoothing = spline_smoothing
+        self.patch_reference_coordinates = np.zeros(2)
+        self._table = None
+
+    @property
+    def table(self):
+        from ..sources import SersicTable, default_table
+        if self._table is None:
+            self._table = (SersicTable.from_file(self.splinedata, self.spline_smoothing)
+                           if self.splinedata else default_table())
+        return self._table
+
+    def set_scene(self, sourcecat, splinedata=None):
+        """A Scene of the catalog rows: fluxes from the columns named by
+        ``bandlist``, then ra, dec, q, pa, sersic, rhalf."""
+        from ..sources import SHAPE_COLS, Scene, SersicTable
+        table = SersicTable.from_file(splinedata, self.spline_smoothing) if splinedata \
+            else self.table
+        cat = np.atleast_1d(sourcecat)
+        cols = list(self.bandlist) + SHAPE_COLS
+        params = np.stack([np.asarray(cat[c], dtype=np.float64) for c in cols], axis=-1)
+        return Scene(len(cat), len(self.bandlist), table, params=params)
+
+    def zerocoords(self, scene, sky_zero=None):
+        """Subtract the (median, by default) source position from the
+        scene's positions in place and return it (patch.py:425-456)."""
+        nb = scene.n_bands
+        if sky_zero is None:
+            sky_zero = np.array([np.median(scene.params[:, nb]),
+                                 np.median(scene.params[:, nb + 1])])
+        zero = np.array(sky_zero, dtype=np.float64)
+        self.patch_reference_coordinates = zero
+        scene.params[:, nb] -= zero[0]
+        scene.params[:, nb + 1] -= zero[1]
+        return zero
+
+    def unzerocoords(self, scene):
+        nb = scene.n_bands
+        zero = self.patch_reference_coordinates
+        scene.params[:, nb] += zero[0]
+        scene.params[:, nb + 1] += zero[1]
+        return scene
+
+    def pack_meta(self, scene):
+        self.patch_reference_coordinates = self.zerocoords(scene)
+        self.n_sources = len(scene)
+        self._pack_source_metadata(scene)
+        self._pack_astrometry(self.wcses, scene)
+        self._pack_fluxcal(self.hdrs)
+        self._pack_psf(self.bands, self.wcses, scene)
+        self.scene = scene
+
+    def _pack_source_metadata(self, scene, dtype=None):
+        self.n_sources = len(scene)
+        self.n_radii = scene.table.n_radii
+        self.rad2 = (scene.table.radii ** 2).astype(np.float32)
+
+    def _pack_astrometry(self, wcses, scene, dtype=None):
+        from ..wcs import scale_at_sky
+        ns, nb = len(scene), scene.n_bands
+        self.D = np.empty((self.n_exp, ns, 2, 2), dtype=np.float32)
+        self.CW = np.empty((self.n_exp, ns, 2, 2), dtype=np.float32)
+        self.crpix = np.empty((self.n_exp, ns, 2), dtype=np.float32)
+        self.crval = np.empty((self.n_exp, ns, 2), dtype=np.float32)
+        ra0, dec0 = self.patch_reference_coordinates
+        sky = np.stack([scene.params[:, nb] + ra0, scene.params[:, nb + 1] + dec0], axis=-1)
+        for j, wcs in enumerate(wcses):
+            for i in range(ns):
+                CW_mat, D_mat = scale_at_sky(sky[i], wcs)
+                self.D[j, i] = D_mat
+                self.CW[j, i] = CW_mat
+            self.crval[j] = sky - self.patch_reference_coordinates
+            x, y = wcs.world_to_pixel_values(sky[:, 0], sky[:, 1])
+            self.crpix[j] = np.stack([x, y], axis=-1)
+
+    def _pack_fluxcal(self, hdrs, tweakphot=None, dtype=None):
+        self.G = np.ones(self.n_exp, dtype=np.float32)
+        if tweakphot:
+            for j, hdr in enumerate(hdrs):
+                self.G[j] = hdr[tweakphot]
+
+    def _pack_psf(self, bands, wcses, scene, dtype=None, psf_dtype=None):
+        ns = len(scene)
+        npsf = [self.psfstore.n_psf_per_source(b) for b in self.bandlist]
+        self.n_psf_per_source = np.array(npsf, dtype=np.int32)
+        self.psfgauss_start = np.zeros(self.n_exp, dtype=np.int32)
+        n_psfgauss = int((self.n_psf_per_source * np.asarray(self.n_exp_per_band) * ns).sum())
+        self.psfgauss = np.empty(n_psfgauss, dtype=PSF_DTYPE)
+        s = 0
+        for e in range(self.n_exp):
+            self.psfgauss_start[e] = s
+            rows = self.psfstore.lookup(bands[e])
+            for _ in range(ns):
+                self.psfgauss[s:s + len(rows)] = rows
+                s += len(rows)
+        assert s == n_psfgauss

@@ -56,6 +56,25 @@ class SersicTable:
         self.sersic_range = (self.ngrid.min(), self.ngrid.max())
         self.rh_range = (self.rgrid.min(), self.rgrid.max())
 
+    @classmethod
+    def from_file(cls, path, spline_smoothing=None):
+        """A table from forcepho's spline-data HDF5 file (datasets nsersic,
+        rh, amplitudes of shape (n_grid, n_radii), radii; read as
+        forcepho/sources.py:623-645 does) or from this package's ``.npz``
+        form (ngrid, rgrid, amplitudes (n_n, n_r, n_radii), radii)."""
+        if str(path).endswith(".npz"):
+            d = np.load(path)
+            return cls(d["ngrid"], d["rgrid"], d["amplitudes"], d["radii"], spline_smoothing)
+        from . import h5lite
+        with h5lite.File(path) as f:
+            n = np.asarray(f["nsersic"][:], dtype=np.float64)
+            r = np.asarray(f["rh"][:], dtype=np.float64)
+            A = np.asarray(f["amplitudes"][:])
+            radii = np.asarray(f["radii"][:], dtype=np.float64)
+        ngrid, rgrid = np.unique(n), np.unique(r)
+        amps = np.stack([A[:, i].reshape(len(ngrid), len(rgrid)) for i in range(A.shape[1])], -1)
+        return cls(ngrid, rgrid, amps, radii, spline_smoothing)
+
     @property
     def n_radii(self):
         return len(self.radii)

@@ -396,3 +396,116 @@ def make_workload(name, seed=0, render=None, return_residual=False, n_patches=25
         return out
     return make_patch(workload_spec(name), seed=seed, render=render,
                       return_residual=return_residual)
+
+
+# ------------------------------------------------------------------ stores
+STORE_BANDS = ["F090W", "F115W", "F150W", "F200W", "F277W", "F356W", "F410M", "F444W"]
+
+
+def store_header(band, nside, crval, crpix, rot_deg, scale=PIXEL_SCALE, bkg=0.0):
+    """A FITS header dict with a TAN WCS: north up to within `rot_deg`, east
+    to -x (CD1_1 < 0), `scale` arcsec per pixel."""
+    t = np.deg2rad(rot_deg)
+    c = scale / 3600.0
+    cd = np.array([[-c * np.cos(t), c * np.sin(t)], [c * np.sin(t), c * np.cos(t)]])
+    return {"NAXIS": 2, "NAXIS1": int(nside[0]), "NAXIS2": int(nside[1]),
+            "CTYPE1": "RA---TAN", "CTYPE2": "DEC--TAN",
+            "CRPIX1": float(crpix[0]), "CRPIX2": float(crpix[1]),
+            "CRVAL1": float(crval[0]), "CRVAL2": float(crval[1]),
+            "CD1_1": float(cd[0, 0]), "CD1_2": float(cd[0, 1]),
+            "CD2_1": float(cd[1, 0]), "CD2_2": float(cd[1, 1]),
+            "FILTER": band, "BKG": float(bkg)}
+
+
+def make_store(directory, n_bands=3, exposures_per_band=2, nside=256, super_pixel_size=8,
+               seed=0, n_psf=3, n_sources=6, ra0=53.16, dec0=DEC0, rot_deg=20.0,
+               mask_frac=0.02, n_locations=2):
+    """Write a seeded pixel store (HDF5), metadata store (JSON) and PSF store
+    (HDF5) in forcepho's layouts into `directory`, and return
+    ``dict(pixelstore=, metastore=, psfstore=, bands=, catalog=, epaths=)``.
+
+    Exposures of one band are dithered by up to 10% of the image and rotated
+    by up to `rot_deg`; fluxes are a smooth background plus Gaussian noise
+    (ierr = 1/sigma, `mask_frac` of pixels with ierr = 0, a few bright pixels
+    with signal-to-noise above 100); every header carries a ``BKG`` keyword.
+    The catalog holds `n_sources` galaxies near (ra0, dec0)."""
+    import json
+    import os
+    from . import h5lite
+    from .fitsio import Header
+    from .patches.patch import PSF_COLS
+    rng = np.random.default_rng(seed)
+    os.makedirs(directory, exist_ok=True)
+    nx, ny = (nside, nside) if np.ndim(nside) == 0 else tuple(nside)
+    s = super_pixel_size
+    bands = STORE_BANDS[:n_bands]
+    pix, pattrs, headers, epaths = {}, {}, {}, []
+    for b in bands:
+        headers[b] = {}
+        for j in range(exposures_per_band):
+            expID = f"exp{j:02d}"
+            shift = rng.uniform(-0.1, 0.1, 2) * np.array([nx, ny]) * PIXEL_SCALE / 3600.0
+            crval = (ra0 + shift[0] / np.cos(np.deg2rad(dec0)), dec0 + shift[1])
+            crpix = (nx / 2.0 + rng.uniform(-3, 3), ny / 2.0 + rng.uniform(-3, 3))
+            bkg = float(rng.normal(0.0, 0.01))
+            hdr = store_header(b, (nx, ny), crval, crpix, rng.uniform(-rot_deg, rot_deg), bkg=bkg)
+            xx, yy = np.meshgrid(np.arange(nx), np.arange(ny), indexing="ij")
+            sky = 0.02 * np.sin(xx / 37.0) * np.cos(yy / 23.0) + bkg
+            sigma = 0.05
+            im = (sky + rng.normal(0.0, sigma, (nx, ny))).astype(np.float32)
+            ierr = np.full((nx, ny), 1.0 / sigma, dtype=np.float32)
+            ierr[rng.uniform(size=(nx, ny)) < mask_frac] = 0.0
+            hot = rng.uniform(size=(nx, ny)) < 0.001
+            im[hot] = 20.0                                   # S/N 400: capped by max_snr=100
+            sp = np.concatenate(
+                [a.reshape(nx // s, s, ny // s, s).transpose(0, 2, 1, 3).reshape(nx // s, ny // s,
+                                                                                s * s)
+                 for a in (im, ierr)], axis=-1).astype(np.float32)
+            path = f"{b}/{expID}"
+            pix[path + "/data"] = sp
+            pattrs[path + "/data"] = {"counts_to_flux": 1.0, "flux_units": "image"}
+            headers[b][expID] = Header(hdr)
+            epaths.append(path)
+    pattrs["/"] = {"nside_full": np.array([nx, ny]), "super_pixel_size": np.int64(s)}
+    pixelstore = os.path.join(directory, "pixels.h5")
+    h5lite.write(pixelstore, pix, pattrs)
+    metastore = os.path.join(directory, "meta.json")
+    with open(metastore, "w") as f:
+        json.dump({b: {e: h.tostring() for e, h in ex.items()} for b, ex in headers.items()}, f)
+    # PSF store: n_locations mixtures per band, n_psf Gaussians for each of 9 radius bins
+    table = default_table()
+    npsf = n_psf * table.n_radii
+    psf, psfattrs = {}, {}
+    for b in bands:
+        par = np.zeros((n_locations, npsf), dtype=PSF_DTYPE)
+        for loc in range(n_locations):
+            amp = rng.dirichlet(np.ones(n_psf))
+            sig = rng.uniform(0.5, 3.0, n_psf)
+            for k in range(table.n_radii):
+                rows = par[loc, k * n_psf:(k + 1) * n_psf]
+                rows["amp"] = amp
+                rows["xcen"] = rng.normal(0, 0.05, n_psf)
+                rows["ycen"] = rng.normal(0, 0.05, n_psf)
+                rows["Cxx"] = sig ** 2
+                rows["Cyy"] = sig ** 2 * rng.uniform(0.9, 1.1, n_psf)
+                rows["Cxy"] = rng.normal(0, 0.05, n_psf)
+                rows["sersic_bin"] = k
+        psf[f"{b}/parameters"] = par
+        psf[f"{b}/detector_locations"] = rng.uniform(0, nx, (2, n_locations))
+        psfattrs[b] = {"n_psf_per_source": np.int64(npsf)}
+    psfstore = os.path.join(directory, "psf.h5")
+    h5lite.write(psfstore, psf, psfattrs)
+    # catalog near the centre, fluxes in every band column
+    cols = [(c, np.float64) for c in ["ra", "dec", "q", "pa", "sersic", "rhalf"]]
+    cat = np.zeros(n_sources, dtype=cols + [(b, np.float64) for b in bands])
+    cosd = np.cos(np.deg2rad(dec0))
+    cat["ra"] = ra0 + rng.uniform(-1.0, 1.0, n_sources) / 3600.0 / cosd
+    cat["dec"] = dec0 + rng.uniform(-1.0, 1.0, n_sources) / 3600.0
+    cat["q"] = rng.uniform(0.5, 0.95, n_sources)
+    cat["pa"] = rng.uniform(-1.2, 1.2, n_sources)
+    cat["sersic"] = rng.uniform(1.0, 4.0, n_sources)
+    cat["rhalf"] = rng.uniform(0.05, 0.3, n_sources)
+    for b in bands:
+        cat[b] = rng.lognormal(0.0, 0.5, n_sources)
+    return dict(pixelstore=pixelstore, metastore=metastore, psfstore=psfstore, bands=bands,
+                catalog=cat, epaths=epaths)

@@ -131,6 +131,14 @@ FPHO_API int fpho_sizeof(int which);
 FPHO_API int fpho_patch_create(const fpho_patch_struct *host, int n_bands, int return_residual,
                       void *stream, fpho_patch **out);
 
+/* As fpho_patch_create, but desc->data, ierr, xpix and ypix are DEVICE
+ * pointers (copied device to device; the caller keeps ownership), e.g. the
+ * output of fpho_store_gather.  The index arrays and the metadata are host
+ * pointers, as for fpho_patch_create.  No counterpart in the reference, whose
+ * pixel arrays always start on the host (device_patch.py:268-300). */
+FPHO_API int fpho_patch_create_device_pixels(const fpho_patch_struct *desc, int n_bands,
+                                             int return_residual, void *stream, fpho_patch **out);
+
 /* Replace the per-scene metadata (n_sources, rad2, D, crpix, crval, CW, G,
  * n_psf_per_source, psfgauss, psfgauss_start) with new host arrays, keeping
  * the pixel arrays.  Replaces GPUPatchMixin.replace_device_meta_ptrs
@@ -362,6 +370,62 @@ FPHO_API int fpho_patch_last_tile_ms(fpho_patch *p, float *ms);
  * (ops = blocks*threads*iters*8).  dev_out: device float[blocks] scratch. */
 FPHO_API int fpho_probe_launch(int which, int blocks, int threads, int iters, float *dev_out,
                                void *stream);
+
+/* ---- exposure store: super-pixel exposures resident in GPU memory ------ */
+
+/* Replaces the host packing of StorePatch (forcepho/patches/pixel_patch.py:
+ * 124-198 pack_pix, 297-342 find_exposures/find_pixels): the exposures of a
+ * pixel store are uploaded once, in the pixel store's layout -- per exposure
+ * (nside_x/s, nside_y/s, 2 s^2) floats, each super-pixel's s x s fluxes in
+ * row-major order then their inverse errors (forcepho/patches/storage.py:
+ * 62-96, 245-276) -- and a patch's pixels are selected and packed on the
+ * device. */
+typedef struct fpho_store fpho_store;
+
+#define FPHO_REGION_CIRCLE 1
+#define FPHO_REGION_RECT 2
+
+/* The region test of one exposure, in that exposure's pixels.  A super-pixel
+ * is selected if one of its corner pixels -- (0,0), (1,0), (1,1), (0,1) times
+ * (s-1) from its first pixel -- passes:
+ *   FPHO_REGION_CIRCLE  p = {xc, yc, r2}: (xc-x)^2 + (yc-y)^2 < r2 in double
+ *                       (CircularRegion.contains, forcepho/region.py:91-116);
+ *   FPHO_REGION_RECT    p = {ra_min, ra_max, dec_min, dec_max, crpix1, crpix2
+ *                       (1-based), cd11, cd12, cd21, cd22, crval1, crval2,
+ *                       lonpole}: the corner's TAN sky position strictly inside
+ *                       the box (RectangularRegion.contains, region.py:168-192). */
+typedef struct fpho_region {
+    int32_t kind;
+    int32_t reserved;
+    double p[14];
+} fpho_region;
+
+/* A store for up to max_exposures exposures of nside_x x nside_y pixels in
+ * super-pixels of super_pixel_size (all memory is allocated here). */
+FPHO_API int fpho_store_create(int nside_x, int nside_y, int super_pixel_size, int max_exposures,
+                               fpho_store **out);
+/* Append one exposure's super-pixel array (host memory, or device memory if
+ * on_device); *index receives its store index. */
+FPHO_API int fpho_store_add_exposure(fpho_store *st, const float *superpixels, int on_device,
+                                     void *stream, int *index);
+/* out: nsx, nsy, super_pixel_size, exposures, capacity, bytes per exposure. */
+FPHO_API int fpho_store_info(const fpho_store *st, int64_t out[6]);
+/* Selected super-pixels of each listed exposure (host n_superpixels[n_exp]);
+ * synchronizes.  StorePatch.find_exposures keeps exposures with at least one. */
+FPHO_API int fpho_store_count(fpho_store *st, int n_exp, const int32_t *exposures,
+                              const fpho_region *regions, int32_t *n_superpixels, void *stream);
+/* Pack the selected pixels of the listed exposures, in that order, into the
+ * device arrays data, ierr, xpix, ypix (npix_capacity floats each; LIMIT if
+ * the patch is larger).  background (host, n_exp, nullable) is subtracted from
+ * the fluxes in float; max_snr > 0 caps ierr at max_snr / flux where
+ * flux * ierr > max_snr (PixelPatch._cap_snr).  exposure_start/exposure_N
+ * (host, n_exp) receive the pixel index of each exposure.  Synchronizes. */
+FPHO_API int fpho_store_gather(fpho_store *st, int n_exp, const int32_t *exposures,
+                               const fpho_region *regions, const float *background, float max_snr,
+                               float *data, float *ierr, float *xpix, float *ypix,
+                               int64_t npix_capacity, int32_t *exposure_start,
+                               int32_t *exposure_N, void *stream);
+FPHO_API int fpho_store_free(fpho_store *st);
 
 #ifdef __cplusplus
 }

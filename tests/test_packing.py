@@ -1,0 +1,227 @@
+"""CPU: the packing path's host pieces against the reference's own packing code.
+
+tests/golden/packing_store.npz and packing_fits.npz were written by
+tests/golden/make_packing_golden.py, which runs forcepho's StorePatch,
+FITSPatch and Patch.pack_meta from the reference sources.  Checked here:
+
+  * the HDF5 subset reader (on the reference's own data files when present)
+    and writer (round trips: nested groups, B-trees of several levels,
+    compound and array types, attributes);
+  * the FITS reader, the TAN WCS and the region helpers;
+  * the host StorePatch / FITSPatch mirrors, bit for bit against the golden
+    pixel digests, index arrays and metadata;
+  * oracle/packing.py (the checker of the device store) against the same
+    digests.
+"""
+import hashlib
+import os
+
+import numpy as np
+import pytest
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+REF_DATA = "/root/reference/tests/data"
+
+
+def _digest(a):
+    return hashlib.sha256(np.ascontiguousarray(a, dtype=np.float32).tobytes()).hexdigest()
+
+
+def _cases():
+    import sys
+    sys.path.insert(0, GOLDEN)
+    import make_packing_golden as G
+    return G
+
+
+@pytest.fixture(scope="module")
+def store(tmp_path_factory):
+    from forcepho_b200 import synth
+    G = _cases()
+    return synth.make_store(str(tmp_path_factory.mktemp("store")), seed=G.STORE_SEED,
+                            **G.STORE_KW)
+
+
+def _region(kind, args):
+    from forcepho_b200.region import CircularRegion, RectangularRegion
+    return CircularRegion(*args) if kind == "circle" else RectangularRegion(*args)
+
+
+# ------------------------------------------------------------------ HDF5
+def test_h5_roundtrip(tmp_path):
+    from forcepho_b200 import h5lite
+    from forcepho_b200.patches.patch import PSF_DTYPE
+    rng = np.random.default_rng(0)
+    arr = np.dtype([("gauss_params", np.float32, 6), ("sersic_bin", np.int32)])
+    P = np.zeros((3, 9), dtype=arr)
+    P["gauss_params"] = rng.normal(size=(3, 9, 6))
+    P["sersic_bin"] = np.arange(9)
+    Q = np.zeros((2, 4), dtype=PSF_DTYPE)
+    Q["amp"] = rng.random((2, 4))
+    ds = {f"F090W/exp{e:03d}/data": rng.normal(size=(2, 2, 8)).astype(np.float32)
+          for e in range(300)}
+    ds.update({"CLEAR/parameters": P, "CLEAR/q": Q, "x": np.arange(5, dtype=np.int16),
+               "s": np.float64(3.5), "u": np.arange(4, dtype=np.uint64).reshape(2, 2)})
+    attrs = {"/": {"nside_full": np.array([32, 32]), "super_pixel_size": 8, "name": "store"},
+             "CLEAR": {"n_psf_per_source": np.int64(9)},
+             "F090W/exp003/data": {"counts_to_flux": 1.5, "flux_units": "nJy"}}
+    path = str(tmp_path / "t.h5")
+    h5lite.write(path, ds, attrs)
+    data, at = h5lite.read_tree(path)
+    for k, v in ds.items():
+        got = np.asarray(data[k])
+        assert got.dtype == np.asarray(v).dtype and np.array_equal(got, v), k
+    assert at["/"]["super_pixel_size"] == 8 and at["/"]["name"] == "store"
+    assert list(at["/"]["nside_full"]) == [32, 32]
+    assert at["CLEAR"]["n_psf_per_source"] == 9
+    assert at["F090W/exp003/data"] == {"counts_to_flux": 1.5, "flux_units": "nJy"}
+    with h5lite.File(path) as f:
+        assert len(f["F090W"].keys()) == 300
+        assert f["F090W"].keys() == sorted(f["F090W"].keys())
+        assert "F090W/exp299/data" in f and "F090W/exp300/data" not in f
+        assert isinstance(f["F090W/exp007/data"].array(), np.memmap)
+
+
+@pytest.mark.skipif(not os.path.isdir(REF_DATA), reason="reference data files not present")
+def test_h5_reads_reference_files():
+    from forcepho_b200 import h5lite
+    from forcepho_b200.patches.storage import PSFStore
+    with h5lite.File(f"{REF_DATA}/sersic_splinedata_large.h5") as f:
+        assert sorted(f.keys()) == ["amplitudes", "nsersic", "radii", "rh"]
+        assert f["amplitudes"].shape == (5555, 9) and f["radii"].shape == (9,)
+    with h5lite.File(f"{REF_DATA}/sersic_mog_model.smooth=0.0150.h5") as f:
+        assert f.attrs["smoothing"] == 0.015
+        assert f["model"].shape == (50, 6399)
+    psf = PSFStore(f"{REF_DATA}/test_image/sersic1.0_rhalf0.150_snr050_noise1_psf.h5")
+    rows = psf.lookup("CLEAR")
+    assert psf.n_psf_per_source("CLEAR") == 9 and len(rows) == 9
+    assert np.array_equal(rows["sersic_bin"], np.arange(9))
+    assert np.all(rows["Cxx"] == 6.25) and np.all(rows["amp"] == 1.0)
+
+
+# ------------------------------------------------------------------ FITS, WCS, regions
+def test_fits_header_roundtrip_and_wcs():
+    from forcepho_b200 import synth
+    from forcepho_b200.fitsio import Header
+    from forcepho_b200.wcs import TanWCS, scale_at_sky
+    h = Header(synth.store_header("F200W", (2048, 2048), (53.1, -27.8), (1024.3, 1020.7), 17.0))
+    h2 = Header.fromstring(h.tostring())
+    assert h2 == h
+    w = TanWCS(h2)
+    x0, y0 = w.world_to_pixel_values(53.1, -27.8)
+    assert abs(x0 - 1023.3) < 1e-9 and abs(y0 - 1019.7) < 1e-9
+    xy = np.random.default_rng(1).uniform(-3000, 5000, (2, 500))
+    back = np.array(w.world_to_pixel_values(*w.pixel_to_world_values(*xy)))
+    assert np.abs(back - xy).max() < 1e-7
+    CW, D = scale_at_sky((53.1005, -27.8002), w)
+    assert np.allclose(np.linalg.inv(D) / 3600.0, w.cd, rtol=1e-12)
+    # the finite-difference branch also sees the projection's local rotation
+    # (meridian convergence, ~1e-5 of the scale 60 px from the tangent point)
+    w.has_distortion = True
+    CW2, D2 = scale_at_sky((53.1005, -27.8002), w)
+    assert np.abs(CW2 - CW).max() < 1e-5 * np.abs(CW).max()
+    assert np.abs(D2 - D).max() < 1e-5 * np.abs(D).max()
+
+
+def test_regions():
+    from forcepho_b200.region import RectangularRegion, polygon_contains, polygons_overlap
+    a = RectangularRegion(58, 59, 26, 27)
+    assert polygons_overlap(a, RectangularRegion(57, 60, 25, 28))
+    assert not polygons_overlap(a, RectangularRegion(60, 62, 25, 28))
+    assert polygons_overlap(a, RectangularRegion(58.5, 62, 25, 28))
+    pts = np.atleast_2d([[0.5, 0.5], [0.5, 1.1], [-0.1, 0.5]])
+    for poly, want in (([[0, 0], [1., 0], [1, 1], [0, 1]], [True, False, False]),
+                       ([[0, 0], [0., 1], [1, 1], [1, 0]], [True, False, False]),
+                       ([[0, 0], [0, 3.0], [1, 1], [1, 0]], [True, True, False])):
+        assert list(polygon_contains(np.array(poly), pts)) == want
+
+
+@pytest.mark.skipif(not os.path.isdir(REF_DATA), reason="reference data files not present")
+def test_fits_reader_on_reference_image():
+    from forcepho_b200 import fitsio
+    hdus = fitsio.read_hdus(f"{REF_DATA}/test_image/sersic1.0_rhalf0.150_snr050_noise1_data.fits")
+    assert [d.shape for _, d in hdus[:3]] == [(100, 100)] * 3
+    cat = hdus[-1][1]
+    assert cat["ra"][0] == 53.0 and cat["dec"][0] == -27.0 and cat["rhalf"][0] == 0.15
+    assert hdus[0][0]["CTYPE1"] == "RA---TAN" and hdus[0][0]["FILTER"] == "CLEAR"
+
+
+# ------------------------------------------------------------------ packing vs the reference
+def _check_packed(p, gold, name):
+    for k in ("data", "ierr", "xpix", "ypix"):
+        assert _digest(getattr(p, k)) == str(gold[f"{name}/{k}_sha256"]), (name, k)
+    for k in ("exposure_start", "exposure_N", "band_start", "band_N", "D", "CW", "crpix",
+              "crval", "G", "rad2", "n_psf_per_source", "psfgauss_start"):
+        np.testing.assert_array_equal(np.asarray(getattr(p, k)), gold[f"{name}/{k}"],
+                                      err_msg=f"{name}/{k}")
+    ps = np.stack([p.psfgauss[c].astype(np.float64) for c in p.psfgauss.dtype.names], -1)
+    np.testing.assert_array_equal(ps, gold[f"{name}/psfgauss"])
+    assert list(p.epaths) == [str(e) for e in gold[f"{name}/epaths"]]
+
+
+def test_store_patch_matches_reference(store):
+    from forcepho_b200.patches.pixel_patch import StorePatch
+    G = _cases()
+    gold = np.load(os.path.join(GOLDEN, "packing_store.npz"))
+    for name, kind, args, tweak, max_snr in G.STORE_CASES:
+        p = StorePatch(store["pixelstore"], store["metastore"], store["psfstore"])
+        p.max_snr = max_snr
+        p.build_patch(_region(kind, args), store["catalog"], allbands=store["bands"],
+                      tweak_background=tweak)
+        _check_packed(p, gold, name)
+
+
+def test_oracle_packing_matches_reference(store):
+    from oracle import packing as OP
+    from forcepho_b200.patches.storage import MetaStore, PixelStore
+    G = _cases()
+    gold = np.load(os.path.join(GOLDEN, "packing_store.npz"))
+    ps, ms = PixelStore(store["pixelstore"]), MetaStore(store["metastore"])
+    for name, kind, args, tweak, max_snr in G.STORE_CASES:
+        region = _region(kind, args)
+        epaths = [str(e) for e in gold[f"{name}/epaths"]]
+        sps, regs, bg = [], [], []
+        for ep in epaths:
+            band, exp = ep.split("/")
+            w = ms.get_wcs(band, exp)
+            sps.append(np.asarray(ps.data[ep + "/data"].array()))
+            regs.append(region.device_params(w))
+            bg.append(ms.headers[band][exp]["BKG"])
+        out = OP.pack(sps, regs, background=bg if tweak else None, max_snr=max_snr)
+        for k in ("data", "ierr", "xpix", "ypix"):
+            assert _digest(out[k]) == str(gold[f"{name}/{k}_sha256"]), (name, k)
+        np.testing.assert_array_equal(out["exposure_N"], gold[f"{name}/exposure_N"])
+        np.testing.assert_array_equal(out["exposure_start"], gold[f"{name}/exposure_start"])
+
+
+@pytest.mark.skipif(not os.path.isdir(REF_DATA), reason="reference data files not present")
+def test_fits_patch_matches_reference():
+    from forcepho_b200 import fitsio
+    from forcepho_b200.patches.pixel_patch import FITSPatch
+    from forcepho_b200.region import CircularRegion
+    gold = np.load(os.path.join(GOLDEN, "packing_fits.npz"))
+    img = f"{REF_DATA}/test_image/sersic1.0_rhalf0.150_snr050_noise1_data.fits"
+    p = FITSPatch(fitsfiles=[img], psfstore=img.replace("_data.fits", "_psf.h5"),
+                  splinedata=f"{REF_DATA}/sersic_splinedata_large.h5", sci_ext=0, unc_ext=1)
+    p.build_patch(CircularRegion(*gold["region"]), None, allbands=["CLEAR"])
+    p.pack_meta(p.set_scene(fitsio.getdata(img, -1)))
+    for k in ("data", "ierr", "xpix", "ypix", "exposure_start", "exposure_N", "band_start",
+              "band_N", "D", "CW", "crpix", "crval", "G", "rad2", "n_psf_per_source"):
+        np.testing.assert_array_equal(np.asarray(getattr(p, k)), gold[k], err_msg=k)
+
+
+def test_superpixelize_matches_the_loop():
+    """The reshape in PixelStore.superpixelize gives the element order of
+    the reference's double loop (storage.py:245-276), restated here."""
+    from forcepho_b200.patches.storage import PixelStore
+    rng = np.random.default_rng(3)
+    im, ie = rng.normal(size=(24, 40)), rng.normal(size=(24, 40))
+    ps = PixelStore.__new__(PixelStore)
+    ps.super_pixel_size, ps.pix_dtype = 8, np.float32
+    got = ps.superpixelize(im, ie)
+    want = np.empty((3, 5, 128), dtype=np.float32)
+    for ii in range(3):
+        for jj in range(5):
+            want[ii, jj, :64] = im[ii * 8:ii * 8 + 8, jj * 8:jj * 8 + 8].flatten()
+            want[ii, jj, 64:] = ie[ii * 8:ii * 8 + 8, jj * 8:jj * 8 + 8].flatten()
+    np.testing.assert_array_equal(got, want)
