@@ -66,6 +66,8 @@ def parse():
                     help="HMC chains of the multi-chain leg (single-source patch); 0 skips it")
     ap.add_argument("--no-differentiable", action="store_true",
                     help="skip the differentiable-form leg (20-source patch)")
+    ap.add_argument("--packing-patches", type=int, default=16,
+                    help="patches packed from the exposure store in the packing leg; 0 skips it")
     return ap.parse_args()
 
 
@@ -428,6 +430,91 @@ def multichain_leg(args, torch, steps, n_chains=256):
                       "the patch is 64 KB); drop-in: host wall clock"}
 
 
+def measured_hbm_gbs():
+    """HBM copy bandwidth measured on this pool (MEASURED_PEAKS.json beside
+    this file), else the earlier pool measurement of 6650 GB/s."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback: earlier measurement on this pool"
+
+
+def packing_leg(args, torch, n_patches):
+    """Patches packed from an exposure store: 8 bands x 4 exposures of
+    2048x2048 px in the reference's HDF5 super-pixel layout, circular regions
+    of 1.92 arcsec (~128 px across) at random positions.  Device: exposures
+    resident in HBM, selection + gather kernels (GPUStorePatch.build_patch:
+    exposure finding and pixel packing).  Host: the reference's algorithm
+    (StorePatch.build_patch, bit-identical output) on a bounded sample."""
+    import shutil
+    import tempfile
+    from forcepho_b200 import synth
+    from forcepho_b200.patches.device_store import DeviceStore, GPUStorePatch
+    from forcepho_b200.patches.pixel_patch import StorePatch
+    from forcepho_b200.patches.storage import PixelStore
+    from forcepho_b200.region import CircularRegion
+    d = tempfile.mkdtemp(prefix="fpho_store_")
+    try:
+        st = synth.make_store(d, n_bands=8, exposures_per_band=4, nside=2048, seed=args.seed,
+                              n_sources=20)
+        rng = np.random.default_rng(args.seed + 7)
+        cosd = np.cos(np.deg2rad(synth.DEC0))
+        regions = [CircularRegion(53.16 + rng.uniform(-5, 5) / 3600.0 / cosd,
+                                  synth.DEC0 + rng.uniform(-5, 5) / 3600.0, 1.92 / 3600.0)
+                   for _ in range(n_patches + 3)]
+        t0 = time.perf_counter()
+        ds = DeviceStore.from_pixelstore(PixelStore(st["pixelstore"]))
+        torch.cuda.synchronize()
+        upload_s = time.perf_counter() - t0
+        gp = GPUStorePatch(st["pixelstore"], st["metastore"], st["psfstore"], device_store=ds)
+        for r in regions[:3]:
+            gp.build_patch(r, None, allbands=st["bands"])
+        ds.time_gather(True)
+        gather_ms, npix = [], []
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for r in regions[3:]:
+            gp.build_patch(r, None, allbands=st["bands"])
+            gather_ms.append(ds.last_gather_ms())
+            npix.append(gp.npix)
+        torch.cuda.synchronize()
+        dev_s = (time.perf_counter() - t0) / n_patches
+        hp = StorePatch(st["pixelstore"], st["metastore"], st["psfstore"])
+        hp.build_patch(regions[0], None, allbands=st["bands"])          # warm the page cache
+        n_host = min(4, n_patches)
+        t0 = time.perf_counter()
+        for r in regions[3:3 + n_host]:
+            hp.build_patch(r, None, allbands=st["bands"])
+        host_s = (time.perf_counter() - t0) / n_host
+        gp.build_patch(regions[2 + n_host], None, allbands=st["bands"])
+        gp.pixels_to_host()
+        identical = all(np.array_equal(np.asarray(getattr(gp, k)), np.asarray(getattr(hp, k)))
+                        for k in ("data", "ierr", "xpix", "ypix", "exposure_start", "exposure_N",
+                                  "band_start", "band_N"))
+        ds.free()
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+    peak, peak_src = measured_hbm_gbs()
+    g_ms = float(np.median(gather_ms))
+    mean_px = float(np.mean(npix))
+    achieved = mean_px * 24 / (g_ms * 1e-3) / 1e9
+    return {"workload": "store: 8 bands x 4 exposures of 2048x2048 px (8x8 super-pixels, "
+                        "1 GiB in HBM), circular regions of 1.92 arcsec, "
+                        f"{mean_px:.0f} px per patch",
+            "metric": "patches packed/s", "device_patches_per_s": 1.0 / dev_s,
+            "host_patches_per_s": 1.0 / host_s, "speedup": host_s / dev_s,
+            "host_sample": f"{n_host} patches, StorePatch.build_patch on 1 core: the "
+                           "reference's selection and output, HDF5 store in the page cache, "
+                           "reading only the selected super-pixels through a memory map (the "
+                           "reference reads each exposure whole)",
+            "identical_to_host": bool(identical), "store_upload_s": upload_s,
+            "roofline": {"bound": "hbm", "kernel": "store_gather", "kernel_ms": g_ms,
+                         "algorithmic_bytes_per_px": 24, "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_src}}
+
+
 def differentiable_leg(args, torch, P, cfg, steps):
     """The 20-source patch through the autograd Function and the
     device posterior, HMC leapfrog steps of 1e-3 in the unconstrained
@@ -621,6 +708,10 @@ def run_ours(args):
         rb.update({"peak": fp32_tflops, "frac": rb["achieved"] / fp32_tflops,
                    "peak_source": "measured live: packed FP32 FMA probe kernel"})
 
+    packing = None
+    if rank == 0 and world == 1 and args.packing_patches > 0:
+        packing = packing_leg(args, torch, args.packing_patches)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cores = len(os.sched_getaffinity(0))
@@ -665,6 +756,7 @@ def run_ours(args):
             "differentiable": differentiable,
             "multichain": multichain,
             "batched": batched,
+            "packing": packing,
         }
         print(json.dumps(line), flush=True)
     P.free()

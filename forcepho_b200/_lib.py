@@ -67,6 +67,8 @@ _SIGS = {
                                   c_void_p, c_void_p, c_void_p, c_void_p, ctypes.c_int64,
                                   c_void_p, c_void_p, c_void_p]),
     "fpho_store_free": (c_int, [c_void_p]),
+    "fpho_store_time_gather": (c_int, [c_void_p, c_int]),
+    "fpho_store_last_gather_ms": (c_int, [c_void_p, ctypes.POINTER(ctypes.c_float)]),
     "fpho_patch_set_config": (c_int, [c_void_p, c_int, c_int, c_void_p]),
     "fpho_patch_set_schedule": (c_int, [c_void_p, c_int]),
     "fpho_patch_set_test_stall": (c_int, [c_void_p, c_int]),

@@ -8,19 +8,26 @@
 // (forcepho/patches/pixel_patch.py:124-198, 307-342; region tests
 // forcepho/region.py:91-116 and 168-192).  Here the super-pixel arrays of all
 // exposures stay in HBM (one 2048x2048 exposure is 32 MiB, so a B200 holds
-// thousands), and three kernels do the selection and the packing:
+// thousands), and four kernels do the selection and the packing:
 //
-//   store_count   one CTA per (chunk of 1024 super-pixels, exposure): the
-//                 region test of every super-pixel, and the chunk's count;
-//   store_scan    one CTA per exposure: exclusive prefix sum of its chunks'
-//                 counts, and the exposure's total;
-//   store_gather  one CTA per (chunk, exposure): the same test, the rank of
-//                 each selected super-pixel within the chunk, then a copy of
-//                 the chunk's selected super-pixels to their place in the
-//                 patch arrays -- consecutive output addresses across the
-//                 CTA, 256-byte runs of input per super-pixel of 8x8 --
-//                 with the background offset and the signal-to-noise cap of
-//                 forcepho/patches/pixel_patch.py:176-205 applied on the way.
+//   store_count    one CTA per (chunk of 1024 super-pixels, exposure): the
+//                  region test of every super-pixel of the exposure's box
+//                  (the rows and columns a circle can reach, computed on the
+//                  host; the whole image for a rectangle), and the chunk's
+//                  count;
+//   store_scan     one CTA per exposure: exclusive prefix sum of its chunks'
+//                  counts, and the exposure's total (read back by the host,
+//                  which sizes the patch from it);
+//   store_compact  one CTA per (chunk, exposure): the same test and the rank
+//                  of each selected super-pixel, which goes to its place in a
+//                  list of the selected super-pixels in output order;
+//   store_copy     one thread per 4 output pixels of the list (float4 loads
+//                  and stores when the super-pixel side is even and the
+//                  outputs are 16-byte aligned), so every CTA moves data and
+//                  the stores are consecutive across each warp: fluxes minus
+//                  the background offset, inverse errors with the
+//                  signal-to-noise cap of forcepho/patches/pixel_patch.py:
+//                  176-205, and the pixel coordinates.
 //
 // Output order is the reference's: exposures in the order given, super-pixels
 // in row-major (x super-pixel, y super-pixel) order (numpy.where over the
@@ -33,6 +40,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
+#include <cstdint>
 #include <new>
 #include <vector>
 
@@ -59,9 +68,18 @@ struct fpho_store {
     int *d_chunk = nullptr;           // [scratch_exp][n_chunks]
     int *d_total = nullptr;           // [scratch_exp]
     int *d_exps = nullptr;            // [scratch_exp]
-    long long *d_start = nullptr;     // [scratch_exp] first output pixel
+    int *d_spbase = nullptr;          // [scratch_exp] selected super-pixels before exposure e
+    int *d_box = nullptr;             // [scratch_exp][4] super-pixel box of each exposure
+    int grid_chunks = 1;              // chunks per exposure of the last count pass
+    int *d_list_sp = nullptr;         // [list_cap] selected super-pixels in output order
+    int *d_list_exp = nullptr;        // [list_cap] their position in the exposure list
+    size_t list_cap = 0;
     float *d_bg = nullptr;            // [scratch_exp]
     fpho_region *d_regions = nullptr; // [scratch_exp]
+    // optional CUDA-event timing of the gather kernel
+    bool time_gather = false;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    float last_gather_ms = 0.f;
     int n_chunks() const { return (nsx * nsy + kChunk - 1) / kChunk; }
     static constexpr int kChunk = 1024;
 };
@@ -121,18 +139,30 @@ __device__ bool superpixel_selected(const fpho_region &R, int sx, int sy, int s)
     return in;
 }
 
-// Flags of this thread's 4 consecutive super-pixels of the chunk (bit j set
-// if super-pixel chunk*1024 + 4*tid + j is selected).
-__device__ unsigned thread_flags(const fpho_region &R, int chunk, int nsx, int nsy, int s) {
-    const int n = nsx * nsy;
+// The super-pixels a region can select in one exposure: rows x0..x0+nx-1,
+// columns y0..y0+ny-1 (a conservative box computed on the host; the whole
+// image when no box is known).  Visited in row-major order, which is the
+// order of the whole image restricted to the box.
+struct SpBox {
+    int x0, y0, nx, ny;
+};
+
+// Flags of this thread's 4 consecutive super-pixels of the chunk of the box
+// (bit j set if box position chunk*1024 + 4*tid + j is selected).
+__device__ unsigned thread_flags(const fpho_region &R, const SpBox &B, int chunk, int s) {
+    const int n = B.nx * B.ny;
     const int base = chunk * fpho_store::kChunk + threadIdx.x * kPerThread;
     unsigned f = 0;
 #pragma unroll
     for (int j = 0; j < kPerThread; ++j) {
-        const int sp = base + j;
-        if (sp < n && superpixel_selected(R, sp / nsy, sp % nsy, s)) f |= 1u << j;
+        const int b = base + j;
+        if (b < n && superpixel_selected(R, B.x0 + b / B.ny, B.y0 + b % B.ny, s)) f |= 1u << j;
     }
     return f;
+}
+
+__device__ __forceinline__ int box_chunks(const SpBox &B) {
+    return (B.nx * B.ny + fpho_store::kChunk - 1) / fpho_store::kChunk;
 }
 
 // Exclusive prefix sum of `v` over the CTA; *total receives the sum.
@@ -164,9 +194,15 @@ __device__ int block_exclusive_scan(int v, int *total) {
 }
 
 __global__ void __launch_bounds__(kThreads)
-store_count(const fpho_region *regions, int nsx, int nsy, int s, int n_chunks, int *chunk_count) {
+store_count(const fpho_region *regions, const SpBox *boxes, int s, int n_chunks,
+            int *chunk_count) {
     const int e = blockIdx.y, chunk = blockIdx.x;
-    const unsigned f = thread_flags(regions[e], chunk, nsx, nsy, s);
+    const SpBox B = boxes[e];
+    if (chunk >= box_chunks(B)) {
+        if (threadIdx.x == 0) chunk_count[(size_t)e * n_chunks + chunk] = 0;
+        return;
+    }
+    const unsigned f = thread_flags(regions[e], B, chunk, s);
     const int c = __syncthreads_count(f & 1u) + __syncthreads_count(f & 2u) +
                   __syncthreads_count(f & 4u) + __syncthreads_count(f & 8u);
     if (threadIdx.x == 0) chunk_count[(size_t)e * n_chunks + chunk] = c;
@@ -189,38 +225,75 @@ store_scan(int n_chunks, int *chunk_count, int *total) {
 }
 
 __global__ void __launch_bounds__(kThreads)
-store_gather(const float *__restrict__ pix, size_t exp_floats, const int *exps,
-             const fpho_region *regions, const int *chunk_off, const long long *exp_start,
-             const float *bg, float max_snr, int nsx, int nsy, int s, int n_chunks,
-             float *__restrict__ data, float *__restrict__ ierr, float *__restrict__ xpix,
-             float *__restrict__ ypix) {
-    __shared__ int sel[fpho_store::kChunk];
+store_compact(const fpho_region *regions, const SpBox *boxes, const int *chunk_off,
+              const int *spbase, int nsy, int s, int n_chunks, int *list_sp, int *list_exp) {
     const int e = blockIdx.y, chunk = blockIdx.x;
-    const unsigned f = thread_flags(regions[e], chunk, nsx, nsy, s);
+    const SpBox B = boxes[e];
+    if (chunk >= box_chunks(B)) return;
+    const unsigned f = thread_flags(regions[e], B, chunk, s);
     int n_sel;
-    int r = block_exclusive_scan(__popc(f), &n_sel);
+    const int r = block_exclusive_scan(__popc(f), &n_sel);
+    if (n_sel == 0) return;
+    const long long o = (long long)spbase[e] + chunk_off[(size_t)e * n_chunks + chunk] + r;
     const int base = chunk * fpho_store::kChunk + threadIdx.x * kPerThread;
+    int q = 0;
 #pragma unroll
     for (int j = 0; j < kPerThread; ++j)
-        if (f & (1u << j)) sel[r++] = base + j;
-    __syncthreads();
-    if (n_sel == 0) return;
+        if (f & (1u << j)) {
+            const int b = base + j;
+            list_sp[o + q] = (B.x0 + b / B.ny) * nsy + (B.y0 + b % B.ny);
+            list_exp[o + q] = e;
+            ++q;
+        }
+}
+
+__device__ __forceinline__ void pack_pixel(float &d, float &ie, float b, bool has_bg,
+                                           float max_snr) {
+    if (has_bg) d = __fsub_rn(d, b);
+    if (max_snr > 0.f && ie > 0.f && __fmul_rn(d, ie) > max_snr) ie = __fdiv_rn(max_snr, d);
+}
+
+// VEC: 4 consecutive output pixels per thread (s^2 % 4 == 0, outputs 16-byte
+// aligned); otherwise one.  Output pixel p belongs to list entry p / s^2.
+template <bool VEC>
+__global__ void __launch_bounds__(kThreads)
+store_copy(const float *__restrict__ pix, size_t exp_floats, const int *__restrict__ exps,
+           const int *__restrict__ list_sp, const int *__restrict__ list_exp, long long n_items,
+           const float *__restrict__ bg, float max_snr, int nsy, int s,
+           float *__restrict__ data, float *__restrict__ ierr, float *__restrict__ xpix,
+           float *__restrict__ ypix) {
+    const long long g = (long long)blockIdx.x * kThreads + threadIdx.x;
+    if (g >= n_items) return;
     const int s2 = s * s;
-    const long long out0 = exp_start[e] + (long long)chunk_off[(size_t)e * n_chunks + chunk] * s2;
-    const float *src_e = pix + (size_t)exps[e] * exp_floats;
+    const long long p = VEC ? g * 4 : g;
+    const long long j = p / s2;
+    const int k = (int)(p - j * s2);
+    const int e = list_exp[j], sp = list_sp[j];
+    const float *src = pix + (size_t)exps[e] * exp_floats + (size_t)sp * 2 * s2;
     const float b = bg ? bg[e] : 0.f;
-    const int n = n_sel * s2;
-    for (int i = threadIdx.x; i < n; i += kThreads) {
-        const int sp = sel[i / s2], k = i % s2;
-        const float *src = src_e + (size_t)sp * 2 * s2;
+    const int x0 = (sp / nsy) * s, y0 = (sp % nsy) * s;
+    if (VEC) {
+        float4 d = *reinterpret_cast<const float4 *>(src + k);
+        float4 ie = *reinterpret_cast<const float4 *>(src + s2 + k);
+        pack_pixel(d.x, ie.x, b, bg != nullptr, max_snr);
+        pack_pixel(d.y, ie.y, b, bg != nullptr, max_snr);
+        pack_pixel(d.z, ie.z, b, bg != nullptr, max_snr);
+        pack_pixel(d.w, ie.w, b, bg != nullptr, max_snr);
+        *reinterpret_cast<float4 *>(data + p) = d;
+        *reinterpret_cast<float4 *>(ierr + p) = ie;
+        *reinterpret_cast<float4 *>(xpix + p) =
+            make_float4((float)(x0 + k / s), (float)(x0 + (k + 1) / s), (float)(x0 + (k + 2) / s),
+                        (float)(x0 + (k + 3) / s));
+        *reinterpret_cast<float4 *>(ypix + p) =
+            make_float4((float)(y0 + k % s), (float)(y0 + (k + 1) % s), (float)(y0 + (k + 2) % s),
+                        (float)(y0 + (k + 3) % s));
+    } else {
         float d = src[k], ie = src[s2 + k];
-        if (bg) d = __fsub_rn(d, b);
-        if (max_snr > 0.f && ie > 0.f && __fmul_rn(d, ie) > max_snr) ie = __fdiv_rn(max_snr, d);
-        const long long o = out0 + i;
-        data[o] = d;
-        ierr[o] = ie;
-        xpix[o] = (float)((sp / nsy) * s + k / s);
-        ypix[o] = (float)((sp % nsy) * s + k % s);
+        pack_pixel(d, ie, b, bg != nullptr, max_snr);
+        data[p] = d;
+        ierr[p] = ie;
+        xpix[p] = (float)(x0 + k / s);
+        ypix[p] = (float)(y0 + k % s);
     }
 }
 
@@ -243,18 +316,53 @@ void dfree(T *&p) {
 
 int ensure_scratch(fpho_store *st, int n_exp) {
     if (n_exp <= st->scratch_exp) return FPHO_OK;
-    dfree(st->d_chunk); dfree(st->d_total); dfree(st->d_exps); dfree(st->d_start);
-    dfree(st->d_bg); dfree(st->d_regions);
+    dfree(st->d_chunk); dfree(st->d_total); dfree(st->d_exps); dfree(st->d_spbase);
+    dfree(st->d_bg); dfree(st->d_regions); dfree(st->d_box);
     st->scratch_exp = 0;
     int rc;
     if ((rc = dalloc(&st->d_chunk, (size_t)n_exp * st->n_chunks()))) return rc;
     if ((rc = dalloc(&st->d_total, (size_t)n_exp))) return rc;
     if ((rc = dalloc(&st->d_exps, (size_t)n_exp))) return rc;
-    if ((rc = dalloc(&st->d_start, (size_t)n_exp))) return rc;
+    if ((rc = dalloc(&st->d_spbase, (size_t)n_exp))) return rc;
+    if ((rc = dalloc(&st->d_box, (size_t)n_exp * 4))) return rc;
     if ((rc = dalloc(&st->d_bg, (size_t)n_exp))) return rc;
     if ((rc = dalloc(&st->d_regions, (size_t)n_exp))) return rc;
     st->scratch_exp = n_exp;
     return FPHO_OK;
+}
+
+// The super-pixels a region can select (rows x0.., columns y0.., counts nx,
+// ny).  For a circle: super-pixels whose corner pixels all lie at least
+// r + 1 pixel from the centre along x (or along y) cannot pass the test
+// (xc - x)^2 + (yc - y)^2 < r2, whatever the rounding, so the box keeps the
+// rows and columns within that reach.  A circle with r2 <= 0 selects
+// nothing; other regions, and circles with non-finite parameters, get the
+// whole image (the exact test decides).
+void region_box(const fpho_region &R, int nsx, int nsy, int s, int box[4]) {
+    box[0] = 0; box[1] = 0; box[2] = nsx; box[3] = nsy;
+    if (R.kind != FPHO_REGION_CIRCLE) return;
+    const double xc = R.p[0], yc = R.p[1], r2 = R.p[2];
+    if (!std::isfinite(xc) || !std::isfinite(yc) || !std::isfinite(r2)) return;
+    if (!(r2 > 0.0)) {
+        box[2] = box[3] = 0;
+        return;
+    }
+    const double reach = std::sqrt(r2) + 1.0;
+    auto range = [&](double c, int n, int &lo, int &cnt) {
+        // super-pixel i can pass only if [i s, i s + s - 1] meets (c - reach, c + reach)
+        const double a = std::floor((c - reach - (s - 1)) / s), b = std::floor((c + reach) / s);
+        const double a2 = std::max(a, 0.0), b2 = std::min(b, (double)(n - 1));
+        if (a2 > b2) {
+            lo = 0;
+            cnt = 0;
+        } else {
+            lo = (int)a2;
+            cnt = (int)(b2 - a2) + 1;
+        }
+    };
+    range(xc, nsx, box[0], box[2]);
+    range(yc, nsy, box[1], box[3]);
+    if (box[2] == 0 || box[3] == 0) box[2] = box[3] = 0;
 }
 
 // Validate the call's exposure list and regions, upload them, and run the
@@ -276,9 +384,18 @@ int count_pass(fpho_store *st, int n_exp, const int32_t *exposures, const fpho_r
     CUDA_TRY(cudaMemcpyAsync(st->d_exps, exposures, sizeof(int) * n_exp, cudaMemcpyHostToDevice, s));
     CUDA_TRY(cudaMemcpyAsync(st->d_regions, regions, sizeof(fpho_region) * n_exp,
                              cudaMemcpyHostToDevice, s));
-    const int nc = st->n_chunks();
-    store_count<<<dim3(nc, n_exp), kThreads, 0, s>>>(st->d_regions, st->nsx, st->nsy, st->s, nc,
-                                                     st->d_chunk);
+    std::vector<int> boxes(4 * (size_t)n_exp);
+    int nc = 1;
+    for (int e = 0; e < n_exp; ++e) {
+        region_box(regions[e], st->nsx, st->nsy, st->s, &boxes[4 * (size_t)e]);
+        const long long n = (long long)boxes[4 * e + 2] * boxes[4 * e + 3];
+        nc = std::max(nc, (int)((n + fpho_store::kChunk - 1) / fpho_store::kChunk));
+    }
+    st->grid_chunks = nc;
+    CUDA_TRY(cudaMemcpyAsync(st->d_box, boxes.data(), sizeof(int) * boxes.size(),
+                             cudaMemcpyHostToDevice, s));
+    store_count<<<dim3(nc, n_exp), kThreads, 0, s>>>(
+        st->d_regions, reinterpret_cast<const SpBox *>(st->d_box), st->s, nc, st->d_chunk);
     CUDA_TRY(cudaGetLastError());
     store_scan<<<n_exp, kThreads, 0, s>>>(nc, st->d_chunk, st->d_total);
     CUDA_TRY(cudaGetLastError());
@@ -371,13 +488,14 @@ extern "C" int fpho_store_gather(fpho_store *st, int n_exp, const int32_t *expos
     std::vector<int> totals;
     int rc = count_pass(st, n_exp, exposures, regions, totals, s);
     if (rc) return rc;
-    std::vector<long long> start(n_exp);
-    long long npix = 0;
+    std::vector<int> spbase(n_exp);
+    long long npix = 0, nsp = 0;
     for (int e = 0; e < n_exp; ++e) {
-        start[e] = npix;
+        spbase[e] = (int)std::min<long long>(nsp, INT32_MAX);
         exposure_start[e] = (int32_t)std::min<long long>(npix, INT32_MAX);
         exposure_N[e] = totals[e] * st->s2;
         npix += (long long)totals[e] * st->s2;
+        nsp += totals[e];
     }
     if (npix > INT32_MAX) return set_error(FPHO_ERR_LIMIT, "the patch would have %lld pixels", npix);
     if (npix > npix_capacity)
@@ -386,28 +504,76 @@ extern "C" int fpho_store_gather(fpho_store *st, int n_exp, const int32_t *expos
     if (npix == 0) return FPHO_OK;
     if (!data || !ierr || !xpix || !ypix)
         return set_error(FPHO_ERR_INVALID, "an output pixel array is NULL");
-    CUDA_TRY(cudaMemcpyAsync(st->d_start, start.data(), sizeof(long long) * n_exp,
+    if ((size_t)nsp > st->list_cap) {
+        dfree(st->d_list_sp);
+        dfree(st->d_list_exp);
+        st->list_cap = 0;
+        if ((rc = dalloc(&st->d_list_sp, (size_t)nsp))) return rc;
+        if ((rc = dalloc(&st->d_list_exp, (size_t)nsp))) return rc;
+        st->list_cap = (size_t)nsp;
+    }
+    CUDA_TRY(cudaMemcpyAsync(st->d_spbase, spbase.data(), sizeof(int) * n_exp,
                              cudaMemcpyHostToDevice, s));
     if (background)
         CUDA_TRY(cudaMemcpyAsync(st->d_bg, background, sizeof(float) * n_exp,
                                  cudaMemcpyHostToDevice, s));
-    const int nc = st->n_chunks();
-    store_gather<<<dim3(nc, n_exp), kThreads, 0, s>>>(
-        st->d_pix, st->exp_floats, st->d_exps, st->d_regions, st->d_chunk, st->d_start,
-        background ? st->d_bg : nullptr, max_snr, st->nsx, st->nsy, st->s, nc, data, ierr, xpix,
-        ypix);
+    const int nc = st->grid_chunks;
+    const bool vec = (st->s2 % 4 == 0) &&
+                     ((((uintptr_t)data) | ((uintptr_t)ierr) | ((uintptr_t)xpix) |
+                       ((uintptr_t)ypix)) % 16 == 0);
+    const long long n_items = vec ? npix / 4 : npix;
+    const unsigned blocks = (unsigned)((n_items + kThreads - 1) / kThreads);
+    if (st->time_gather) CUDA_TRY(cudaEventRecord(st->ev0, s));
+    store_compact<<<dim3(nc, n_exp), kThreads, 0, s>>>(
+        st->d_regions, reinterpret_cast<const SpBox *>(st->d_box), st->d_chunk, st->d_spbase,
+        st->nsy, st->s, nc, st->d_list_sp, st->d_list_exp);
     CUDA_TRY(cudaGetLastError());
+    const float *bgp = background ? st->d_bg : nullptr;
+    if (vec)
+        store_copy<true><<<blocks, kThreads, 0, s>>>(st->d_pix, st->exp_floats, st->d_exps,
+                                                     st->d_list_sp, st->d_list_exp, n_items, bgp,
+                                                     max_snr, st->nsy, st->s, data, ierr, xpix,
+                                                     ypix);
+    else
+        store_copy<false><<<blocks, kThreads, 0, s>>>(st->d_pix, st->exp_floats, st->d_exps,
+                                                      st->d_list_sp, st->d_list_exp, n_items, bgp,
+                                                      max_snr, st->nsy, st->s, data, ierr, xpix,
+                                                      ypix);
+    CUDA_TRY(cudaGetLastError());
+    if (st->time_gather) CUDA_TRY(cudaEventRecord(st->ev1, s));
     // the host vectors above die on return; the stream must be done with them
     CUDA_TRY(cudaStreamSynchronize(s));
+    if (st->time_gather) CUDA_TRY(cudaEventElapsedTime(&st->last_gather_ms, st->ev0, st->ev1));
+    return FPHO_OK;
+}
+
+extern "C" int fpho_store_time_gather(fpho_store *st, int enable) {
+    clear_error();
+    if (!st) return set_error(FPHO_ERR_INVALID, "NULL store");
+    if (enable && !st->ev0) {
+        CUDA_TRY(cudaEventCreate(&st->ev0));
+        CUDA_TRY(cudaEventCreate(&st->ev1));
+    }
+    st->time_gather = enable != 0;
+    return FPHO_OK;
+}
+
+extern "C" int fpho_store_last_gather_ms(const fpho_store *st, float *ms) {
+    clear_error();
+    if (!st || !ms) return set_error(FPHO_ERR_INVALID, "NULL argument");
+    *ms = st->last_gather_ms;
     return FPHO_OK;
 }
 
 extern "C" int fpho_store_free(fpho_store *st) {
     clear_error();
     if (!st) return FPHO_OK;
+    if (st->ev0) cudaEventDestroy(st->ev0);
+    if (st->ev1) cudaEventDestroy(st->ev1);
     dfree(st->d_pix);
-    dfree(st->d_chunk); dfree(st->d_total); dfree(st->d_exps); dfree(st->d_start);
+    dfree(st->d_chunk); dfree(st->d_total); dfree(st->d_exps); dfree(st->d_spbase);
     dfree(st->d_bg); dfree(st->d_regions);
+    dfree(st->d_list_sp); dfree(st->d_list_exp); dfree(st->d_box);
     delete st;
     return FPHO_OK;
 }

@@ -20,7 +20,8 @@ import ctypes
 import numpy as np
 
 from .. import _lib
-from ..region import REGION_CIRCLE, REGION_RECT
+from ..region import REGION_CIRCLE, REGION_RECT, CircularRegion
+from ..wcs import TanWCSStack
 from .device_patch import DevicePatch, GPUPatchMixin
 from .pixel_patch import StorePatch
 
@@ -30,9 +31,23 @@ __all__ = ["DeviceStore", "GPUStorePatch", "REGION_DTYPE", "region_records"]
 REGION_DTYPE = np.dtype([("kind", np.int32), ("reserved", np.int32), ("p", np.float64, 14)])
 
 
-def region_records(region, wcses):
-    """One ``fpho_region`` record per exposure WCS."""
+def region_records(region, wcses, stack=None):
+    """One ``fpho_region`` record per exposure WCS.  A circle's centre and
+    radius are mapped to every exposure's pixels in one numpy pass over
+    `stack` (a :class:`~forcepho_b200.wcs.TanWCSStack` of `wcses`, built if
+    not given), with the arithmetic of ``CircularRegion.pixel_circle``."""
     out = np.zeros(len(wcses), dtype=REGION_DTYPE)
+    if len(wcses) == 0:
+        return out
+    if isinstance(region, CircularRegion):
+        stack = stack if stack is not None else TanWCSStack(wcses)
+        x, y = stack.world_to_pixel_values([region.ra, region.ra],
+                                           [region.dec, region.dec + region.radius])
+        xc, yc, xr, yr = x[:, 0], y[:, 0], x[:, 1], y[:, 1]
+        out["kind"] = REGION_CIRCLE
+        out["p"][:, 0], out["p"][:, 1] = xc, yc
+        out["p"][:, 2] = (xc - xr) ** 2 + (yc - yr) ** 2
+        return out
     for i, w in enumerate(wcses):
         kind, p = region.device_params(w)
         if kind not in (REGION_CIRCLE, REGION_RECT):
@@ -139,6 +154,16 @@ class DeviceStore:
         total = int(n.astype(np.int64).sum())
         return [b[:total] for b in bufs], start, n
 
+    def time_gather(self, enable=True):
+        """Time the gather kernel of every following :meth:`gather` with CUDA
+        events; :meth:`last_gather_ms` reads the last one."""
+        _lib.call("fpho_store_time_gather", self.handle, int(bool(enable)))
+
+    def last_gather_ms(self):
+        ms = ctypes.c_float()
+        _lib.call("fpho_store_last_gather_ms", self.handle, ctypes.byref(ms))
+        return ms.value
+
     def free(self):
         if getattr(self, "handle", None):
             _lib.lib.fpho_store_free(self.handle)
@@ -174,31 +199,53 @@ class GPUStorePatch(StorePatch, GPUPatchMixin):
         self.pixels = None
         self.device_patch = None
 
+    def _exposure_table(self, bandlist):
+        """(band, expID, wcs, store index) of every exposure of `bandlist`
+        in metadata-store order, and their WCS stack (cached)."""
+        key = tuple(bandlist)
+        if getattr(self, "_exp_table_key", None) != key:
+            rows = [(b, e, self.metastore.get_wcs(b, e), self.device_store.index(f"{b}/{e}"))
+                    for b in bandlist if b in self.metastore.headers
+                    for e in self.metastore.headers[b].keys()]
+            self._exp_table = (rows, TanWCSStack([r[2] for r in rows]) if rows else None)
+            self._exp_table_key = key
+        return self._exp_table
+
     def find_exposures(self, region, bandlist):
+        """As StorePatch.find_exposures: a corner of the region's bounding
+        box inside the image (all exposures in one numpy pass), then at least
+        one super-pixel in the region (the count kernel)."""
+        rows, stack = self._exposure_table(bandlist)
+        self._records = {}
+        if not rows:
+            return [], [], [], []
         imsize = np.zeros(2) + self.pixelstore.nside_full
         bra, bdec = region.bounding_box
-        cand = []
-        for band in bandlist:
-            if band not in self.metastore.headers:
-                continue
-            for expID in self.metastore.headers[band].keys():
-                wcs = self.metastore.get_wcs(band, expID)
-                bx, by = wcs.world_to_pixel_values(bra, bdec)
-                if np.any((bx > 0) & (bx < imsize[0]) & (by > 0) & (by < imsize[1])):
-                    cand.append((band, expID, wcs))
-        if not cand:
+        bx, by = stack.world_to_pixel_values(bra, bdec)
+        inim = np.any((bx > 0) & (bx < imsize[0]) & (by > 0) & (by < imsize[1]), axis=1)
+        sel = np.flatnonzero(inim)
+        if len(sel) == 0:
             return [], [], [], []
-        idx = [self.device_store.index(f"{b}/{e}") for b, e, _ in cand]
-        counts = self.device_store.count(idx, region_records(region, [w for _, _, w in cand]))
-        keep = [c for c, n in zip(cand, counts) if n > 0]
-        return ([self.metastore.headers[b][e] for b, e, _ in keep], [w for _, _, w in keep],
-                [f"{b}/{e}" for b, e, _ in keep], [b for b, _, _ in keep])
+        recs = region_records(region, [rows[i][2] for i in range(len(rows))], stack)[sel]
+        counts = self.device_store.count([rows[i][3] for i in sel], recs)
+        keep = [(rows[i], rec, n) for i, rec, n in zip(sel, recs, counts) if n > 0]
+        self._records = {f"{r[0]}/{r[1]}": (rec, int(n)) for r, rec, n in keep}
+        keep = [(r, rec) for r, rec, _ in keep]
+        return ([self.metastore.headers[r[0]][r[1]] for r, _ in keep], [r[2] for r, _ in keep],
+                [f"{r[0]}/{r[1]}" for r, _ in keep], [r[0] for r, _ in keep])
 
     def pack_pix(self, region, dtype=None):
         idx = [self.device_store.index(p) for p in self.epaths]
-        regs = region_records(region, self.wcses)
+        cached = getattr(self, "_records", {})
+        npix = None
+        if all(p in cached for p in self.epaths):     # from find_exposures: no second count
+            regs = np.array([cached[p][0] for p in self.epaths], dtype=REGION_DTYPE)
+            npix = sum(cached[p][1] for p in self.epaths) * self.device_store.super_pixel_size ** 2
+        else:
+            regs = region_records(region, self.wcses)
         pix, start, n = self.device_store.gather(idx, regs, background=self.background_offsets,
-                                                 max_snr=getattr(self, "max_snr", None))
+                                                 max_snr=getattr(self, "max_snr", None),
+                                                 npix=npix)
         self.pixels = dict(zip(["data", "ierr", "xpix", "ypix"], pix))
         for k in ("data", "ierr", "xpix", "ypix"):
             self.__dict__.pop(k, None)

@@ -17,7 +17,7 @@ Both methods are vectorised over numpy arrays and computed in float64.
 
 import numpy as np
 
-__all__ = ["TanWCS", "scale_at_sky", "sky_to_pix"]
+__all__ = ["TanWCS", "TanWCSStack", "scale_at_sky", "sky_to_pix"]
 
 _D2R = np.pi / 180.0
 _R2D = 180.0 / np.pi
@@ -141,3 +141,39 @@ def sky_to_pix(ra, dec, exp=None, ref_coords=0.0):
         CW, crval, crpix = CW[0], crval[0], crpix[0]
     sky = np.array([ra, dec]).T - (crval + ref_coords)
     return np.matmul(CW, sky[:, :, None])[..., 0] + crpix
+
+
+class TanWCSStack:
+    """Many TAN WCSs evaluated together: ``world_to_pixel_values(ra, dec)``
+    maps k sky positions through each of n WCSs at once, returning (n, k)
+    arrays -- the same formulas as :class:`TanWCS`, broadcast over a stack of
+    parameters (used to test a region against every exposure of a store in
+    one numpy pass)."""
+
+    def __init__(self, wcses):
+        self.crpix = np.array([w.crpix for w in wcses], dtype=np.float64).reshape(-1, 2)
+        self.crval = np.array([w.crval for w in wcses], dtype=np.float64).reshape(-1, 2)
+        self.cdinv = np.array([w.cdinv for w in wcses], dtype=np.float64).reshape(-1, 2, 2)
+        self.lonpole = np.array([w.lonpole for w in wcses], dtype=np.float64)
+
+    def __len__(self):
+        return len(self.lonpole)
+
+    def world_to_pixel_values(self, ra, dec):
+        ra = np.atleast_1d(np.asarray(ra, dtype=np.float64))[None, :] * _D2R
+        dec = np.atleast_1d(np.asarray(dec, dtype=np.float64))[None, :] * _D2R
+        a0, d0 = self.crval[:, :1] * _D2R, self.crval[:, 1:] * _D2R
+        da = ra - a0
+        sd, cd = np.sin(dec), np.cos(dec)
+        sd0, cd0 = np.sin(d0), np.cos(d0)
+        X = sd * cd0 - cd * sd0 * np.cos(da)
+        Y = -cd * np.sin(da)
+        Z = sd * sd0 + cd * cd0 * np.cos(da)
+        phi = self.lonpole[:, None] * _D2R + np.arctan2(Y, X)
+        r = _R2D * np.hypot(X, Y) / Z
+        xi = r * np.sin(phi)
+        eta = -r * np.cos(phi)
+        ci = self.cdinv
+        u = ci[:, 0, 0, None] * xi + ci[:, 0, 1, None] * eta
+        v = ci[:, 1, 0, None] * xi + ci[:, 1, 1, None] * eta
+        return u + self.crpix[:, :1] - 1.0, v + self.crpix[:, 1:] - 1.0

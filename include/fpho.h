@@ -425,6 +425,11 @@ FPHO_API int fpho_store_gather(fpho_store *st, int n_exp, const int32_t *exposur
                                float *data, float *ierr, float *xpix, float *ypix,
                                int64_t npix_capacity, int32_t *exposure_start,
                                int32_t *exposure_N, void *stream);
+/* Enable (1) or disable (0) CUDA events around the gather kernel of every
+ * following fpho_store_gather; fpho_store_last_gather_ms gives the last one's
+ * milliseconds (the gather synchronizes, so it is ready on return). */
+FPHO_API int fpho_store_time_gather(fpho_store *st, int enable);
+FPHO_API int fpho_store_last_gather_ms(const fpho_store *st, float *ms);
 FPHO_API int fpho_store_free(fpho_store *st);
 
 #ifdef __cplusplus

@@ -94,6 +94,32 @@ def test_gather_matches_oracle(nx, ny, s):
     st.free()
 
 
+def test_gather_random_small_circles():
+    """Many small circles: the chunk-level skip of the count and compact
+    kernels (chunks of 1024 super-pixels that start and end mid-row here,
+    48 super-pixels per row) must not change the selection."""
+    from forcepho_b200.patches.device_store import DeviceStore, REGION_DTYPE
+    nx, ny, s = 512, 384, 8
+    rng = np.random.default_rng(17)
+    sps = _random_store(nx, ny, s, 2, seed=5)
+    st = DeviceStore((nx, ny), s, max_exposures=2)
+    for sp in sps:
+        st.add(sp)
+    n = 40
+    order = rng.integers(0, 2, n)
+    regs = [(1, [rng.uniform(-20, nx + 20), rng.uniform(-20, ny + 20),
+                 rng.uniform(1.0, 60.0) ** 2]) for _ in range(n)]
+    recs = np.zeros(n, dtype=REGION_DTYPE)
+    recs["kind"] = 1
+    recs["p"][:, :3] = [r[1] for r in regs]
+    pix, start, cnt = st.gather(order, recs)
+    want = OP.pack([sps[e] for e in order], regs)
+    np.testing.assert_array_equal(cnt, want["exposure_N"])
+    for k, t in zip(("data", "ierr", "xpix", "ypix"), pix):
+        np.testing.assert_array_equal(t.cpu().numpy(), want[k], err_msg=k)
+    st.free()
+
+
 @pytest.fixture(scope="module")
 def store(tmp_path_factory):
     from forcepho_b200 import synth
