@@ -225,3 +225,71 @@ def test_superpixelize_matches_the_loop():
             want[ii, jj, :64] = im[ii * 8:ii * 8 + 8, jj * 8:jj * 8 + 8].flatten()
             want[ii, jj, 64:] = ie[ii * 8:ii * 8 + 8, jj * 8:jj * 8 + 8].flatten()
     np.testing.assert_array_equal(got, want)
+
+
+def test_pixelstore_add_exposure(tmp_path):
+    """PixelStore.add_exposure as forcepho/patches/storage.py:151-243:
+    background subtracted, masked and non-finite pixels get ierr = 0 and the
+    background value as flux, then super-pixel order; existing paths are
+    replaced."""
+    from forcepho_b200.patches.storage import ImageSet, PixelStore
+    rng = np.random.default_rng(8)
+    path = str(tmp_path / "pix.h5")
+    ps = PixelStore(path, nside_full=32, super_pixel_size=8)
+    im = rng.normal(size=(32, 32)).astype(np.float32)
+    ierr = np.abs(rng.normal(size=(32, 32))).astype(np.float32) + 0.5
+    bkg = np.full((32, 32), 0.25, dtype=np.float32)
+    mask = np.zeros((32, 32), dtype=np.int32)
+    mask[3, 4] = 4
+    im[5, 6] = np.nan
+    ierr[7, 8] = -1.0
+    ps.add_exposure(ImageSet(im=im.copy(), ierr=ierr.copy(), mask=mask, bkg=bkg, hdr={},
+                             band="F200W", expID="e1", names="e1.fits"), bitmask=4)
+    ps2 = PixelStore(path)
+    assert list(np.asarray(ps2.nside_full).reshape(-1)) in ([32], [32, 32])
+    assert ps2.super_pixel_size == 8
+    sp = ps2.data["F200W/e1/data"][:]
+    want_im, want_ie = im - bkg, ierr.copy()
+    bad = np.zeros_like(mask, dtype=bool)
+    bad[3, 4] = bad[5, 6] = bad[7, 8] = True
+    want_ie[bad] = 0.0
+    want_im[bad] = bkg[bad]
+    np.testing.assert_array_equal(sp, ps2.superpixelize(want_im, want_ie))
+    assert ps2.data["F200W/e1/data"].attrs["image_name"] == "e1.fits"
+    ps2.add_exposure(ImageSet(im=np.ones_like(im), ierr=np.ones_like(ierr), mask=None, bkg=None,
+                              hdr={},
+                              band="F200W", expID="e1", names=None))
+    ps2.close()
+    assert np.all(PixelStore(path).data["F200W/e1/data"][:] == 1.0)
+    assert PixelStore(path).exposure_paths() == ["F200W/e1"]
+
+
+def test_direct_patch_and_metastore(store):
+    """DirectPatch packs given arrays in header order; MetaStore finds the
+    exposures whose footprint holds a sky position; Region.overlaps."""
+    from forcepho_b200.patches.pixel_patch import DirectPatch
+    from forcepho_b200.patches.storage import MetaStore, PixelStore
+    from forcepho_b200.region import CircularRegion, RectangularRegion
+    ms, ps = MetaStore(store["metastore"]), PixelStore(store["pixelstore"])
+    s2 = ps.super_pixel_size ** 2
+    pix, hdrs = {}, {}
+    for ep in store["epaths"][:3]:
+        band, exp = ep.split("/")
+        sp = ps.data[ep + "/data"][:][:4, :4]
+        pix[ep] = dict(flux=sp[..., :s2].reshape(-1), ierr=sp[..., s2:].reshape(-1),
+                       xpix=ps.xpix[:4, :4].reshape(-1), ypix=ps.ypix[:4, :4].reshape(-1))
+        hdrs[ep] = ms.headers[band][exp]
+    p = DirectPatch(pixel_dict=pix, header_dict=hdrs, psfstore=store["psfstore"])
+    p.build_patch(None, store["catalog"], allbands=store["bands"])
+    assert list(p.epaths) == store["epaths"][:3]
+    np.testing.assert_array_equal(p.exposure_N, [16 * s2] * 3)
+    np.testing.assert_array_equal(p.data, np.concatenate([pix[e]["flux"] for e in p.epaths]))
+    np.testing.assert_array_equal(p.band_N, [2, 1])
+    assert p.D.shape == (3, len(store["catalog"]), 2, 2)
+    ids, bands = ms.find_exposures((53.16, -27.78), store["bands"])
+    assert len(ids) == len(store["epaths"])          # every dithered exposure covers the centre
+    ids, _ = ms.find_exposures((53.16 + 1.0, -27.78), store["bands"])
+    assert ids == []
+    hdr = ms.headers[store["bands"][0]]["exp00"]
+    assert CircularRegion(53.16, -27.78, 1.0 / 3600).overlaps(hdr)
+    assert not RectangularRegion(54.0, 54.1, -27.0, -26.9).overlaps(hdr)
