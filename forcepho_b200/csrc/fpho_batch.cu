@@ -157,16 +157,16 @@ namespace {
 template <typename T>
 int balloc(T **p, size_t n) {
     *p = nullptr;
-    cudaError_t e = cudaMalloc((void **)p, (n ? n : 1) * sizeof(T));
+    cudaError_t e = fpho::pool_malloc((void **)p, (n ? n : 1) * sizeof(T));
     if (e != cudaSuccess) {
         *p = nullptr;
-        return set_error(FPHO_ERR_NOMEM, "cudaMalloc: %s", cudaGetErrorString(e));
+        return set_error(FPHO_ERR_NOMEM, "device allocation failed: %s", cudaGetErrorString(e));
     }
     return FPHO_OK;
 }
 template <typename T>
 void bfree(T *&p) {
-    if (p) cudaFree((void *)p);
+    fpho::pool_free((void *)p);
     p = nullptr;
 }
 

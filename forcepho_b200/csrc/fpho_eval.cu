@@ -245,17 +245,17 @@ template <typename T>
 int dalloc(T **p, size_t n) {
     *p = nullptr;
     if (n == 0) n = 1;
-    cudaError_t e = cudaMalloc((void **)p, n * sizeof(T));
+    cudaError_t e = fpho::pool_malloc((void **)p, n * sizeof(T));
     if (e != cudaSuccess) {
         *p = nullptr;
-        return set_error(FPHO_ERR_NOMEM, "cudaMalloc of %zu bytes failed: %s", n * sizeof(T),
-                         cudaGetErrorString(e));
+        return set_error(FPHO_ERR_NOMEM, "device allocation of %zu bytes failed: %s",
+                         n * sizeof(T), cudaGetErrorString(e));
     }
     return FPHO_OK;
 }
 template <typename T>
 void dfree(T *&p) {
-    if (p) cudaFree((void *)p);
+    fpho::pool_free((void *)p);
     p = nullptr;
 }
 template <typename T>
@@ -431,6 +431,30 @@ int refresh_struct(fpho_patch *p, cudaStream_t s) {
 }  // namespace
 
 namespace fpho {
+
+cudaError_t pool_malloc(void **p, size_t bytes) {
+    static std::once_flag once[64];
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev >= 0 && dev < 64)
+        std::call_once(once[dev], [dev] {
+            cudaMemPool_t pool;
+            if (cudaDeviceGetDefaultMemPool(&pool, dev) == cudaSuccess) {
+                uint64_t keep = UINT64_MAX;
+                cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+            }
+        });
+    e = cudaMallocAsync(p, bytes, 0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+    return e;
+}
+
+void pool_free(void *p) {
+    if (!p) return;
+    cudaDeviceSynchronize();
+    cudaFreeAsync(p, 0);
+}
 
 PatchView make_view(const fpho_patch *p) {
     PatchView v;

@@ -30,4 +30,15 @@ int launch_tile_kernel(int variant, const TileArgs &A, int n_tiles, cudaStream_t
 
 PatchView make_view(const fpho_patch *p);
 
+// Device memory of handles (patches, batches, store scratch) comes from the
+// device's default memory pool, told to keep freed memory: creating and
+// freeing handles one after another then reuses pool memory instead of a
+// driver allocation each time (on a busy machine those took milliseconds to
+// seconds, erratically).  pool_malloc returns only once the allocation is
+// usable from any stream; pool_free first waits for the device, as cudaFree
+// does, so memory still read by a kernel is never reused.  The pool keeps
+// the high-water mark of handle memory until the process exits.
+cudaError_t pool_malloc(void **p, size_t bytes);
+void pool_free(void *p);
+
 }  // namespace fpho

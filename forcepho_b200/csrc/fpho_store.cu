@@ -297,20 +297,22 @@ store_copy(const float *__restrict__ pix, size_t exp_floats, const int *__restri
     }
 }
 
+// Scratch comes from the handle memory pool (fpho_internal.h); the exposure
+// array itself is one plain cudaMalloc at creation.
 template <typename T>
 int dalloc(T **p, size_t n) {
     *p = nullptr;
-    cudaError_t e = cudaMalloc((void **)p, std::max<size_t>(n, 1) * sizeof(T));
+    cudaError_t e = fpho::pool_malloc((void **)p, std::max<size_t>(n, 1) * sizeof(T));
     if (e != cudaSuccess) {
         *p = nullptr;
-        return set_error(FPHO_ERR_NOMEM, "cudaMalloc of %zu bytes failed: %s", n * sizeof(T),
-                         cudaGetErrorString(e));
+        return set_error(FPHO_ERR_NOMEM, "device allocation of %zu bytes failed: %s",
+                         n * sizeof(T), cudaGetErrorString(e));
     }
     return FPHO_OK;
 }
 template <typename T>
 void dfree(T *&p) {
-    if (p) cudaFree((void *)p);
+    fpho::pool_free((void *)p);
     p = nullptr;
 }
 
@@ -430,9 +432,12 @@ extern "C" int fpho_store_create(int nside_x, int nside_y, int super_pixel_size,
     st->s2 = s * s;
     st->cap = max_exposures;
     st->exp_floats = (size_t)st->nsx * st->nsy * 2 * st->s2;
-    if (int rc = dalloc(&st->d_pix, st->exp_floats * (size_t)max_exposures)) {
+    const size_t bytes = st->exp_floats * (size_t)max_exposures * sizeof(float);
+    if (cudaMalloc((void **)&st->d_pix, bytes) != cudaSuccess) {
+        st->d_pix = nullptr;
         delete st;
-        return rc;
+        return set_error(FPHO_ERR_NOMEM, "cudaMalloc of %zu bytes for %d exposures failed",
+                         bytes, max_exposures);
     }
     *out = st;
     return FPHO_OK;
@@ -570,7 +575,8 @@ extern "C" int fpho_store_free(fpho_store *st) {
     if (!st) return FPHO_OK;
     if (st->ev0) cudaEventDestroy(st->ev0);
     if (st->ev1) cudaEventDestroy(st->ev1);
-    dfree(st->d_pix);
+    if (st->d_pix) cudaFree(st->d_pix);
+    st->d_pix = nullptr;
     dfree(st->d_chunk); dfree(st->d_total); dfree(st->d_exps); dfree(st->d_spbase);
     dfree(st->d_bg); dfree(st->d_regions);
     dfree(st->d_list_sp); dfree(st->d_list_exp); dfree(st->d_box);

@@ -265,14 +265,35 @@ class Patch(PatchBase):
         self.crval = np.empty((self.n_exp, ns, 2), dtype=np.float32)
         ra0, dec0 = self.patch_reference_coordinates
         sky = np.stack([scene.params[:, nb] + ra0, scene.params[:, nb + 1] + dec0], axis=-1)
+        # cos(dec) of each source, as scale_at_sky computes it (scalar calls)
+        cosd = np.array([np.cos(np.deg2rad(d)) for d in sky[:, 1]])
         for j, wcs in enumerate(wcses):
-            for i in range(ns):
-                CW_mat, D_mat = scale_at_sky(sky[i], wcs)
-                self.D[j, i] = D_mat
-                self.CW[j, i] = CW_mat
+            if getattr(wcs, "has_distortion", True):
+                for i in range(ns):
+                    CW_mat, D_mat = scale_at_sky(sky[i], wcs)
+                    self.D[j, i] = D_mat
+                    self.CW[j, i] = CW_mat
+            else:
+                # scale_at_sky's linear branch for every source at once: D is
+                # the same for all sources, CW = (3600 D) diag(cos dec, 1), whose
+                # matrix product has exact zero and unit terms, so the columns
+                # are scaled elementwise with the same results
+                D_mat = np.linalg.inv(wcs.pixel_scale_matrix * 3600.0)
+                A = D_mat * 3600.0
+                self.D[j] = D_mat
+                self.CW[j, :, :, 0] = A[None, :, 0] * cosd[:, None]
+                self.CW[j, :, :, 1] = A[None, :, 1]
             self.crval[j] = sky - self.patch_reference_coordinates
-            x, y = wcs.world_to_pixel_values(sky[:, 0], sky[:, 1])
-            self.crpix[j] = np.stack([x, y], axis=-1)
+        # source positions in every exposure's pixels: one pass over a stack of
+        # TAN WCSs (elementwise the same arithmetic as one call per exposure)
+        from ..wcs import TanWCS, TanWCSStack
+        if wcses and all(isinstance(w, TanWCS) for w in wcses):
+            x, y = TanWCSStack(wcses).world_to_pixel_values(sky[:, 0], sky[:, 1])
+            self.crpix[:] = np.stack([x, y], axis=-1)
+        else:
+            for j, wcs in enumerate(wcses):
+                x, y = wcs.world_to_pixel_values(sky[:, 0], sky[:, 1])
+                self.crpix[j] = np.stack([x, y], axis=-1)
 
     def _pack_fluxcal(self, hdrs, tweakphot=None, dtype=None):
         self.G = np.ones(self.n_exp, dtype=np.float32)
@@ -288,10 +309,9 @@ class Patch(PatchBase):
         n_psfgauss = int((self.n_psf_per_source * np.asarray(self.n_exp_per_band) * ns).sum())
         self.psfgauss = np.empty(n_psfgauss, dtype=PSF_DTYPE)
         s = 0
-        for e in range(self.n_exp):
+        for e in range(self.n_exp):      # every source of an exposure gets its band's rows
             self.psfgauss_start[e] = s
             rows = self.psfstore.lookup(bands[e])
-            for _ in range(ns):
-                self.psfgauss[s:s + len(rows)] = rows
-                s += len(rows)
+            self.psfgauss[s:s + ns * len(rows)] = np.tile(rows, ns)
+            s += ns * len(rows)
         assert s == n_psfgauss

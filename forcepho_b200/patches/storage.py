@@ -275,24 +275,37 @@ class PSFStore:
 
     def __init__(self, h5file):
         self.h5file = h5file
+        self._rows = {}      # (band, location) -> rows, read once
+        self._locs = {}
 
     def lookup(self, band, xy=None):
         """(n_psf_per_source,) PSF rows of `band`: the detector location
         nearest to `xy` if the band has locations and `xy` is given, else
-        the first."""
-        g = self.data[band]
+        the first.  Rows are read from the file once per (band, location)."""
         choose = 0
-        if xy is not None and "detector_locations" in g:
-            xp, yp = g["detector_locations"][:]
-            choose = int(np.hypot(xy[0] - xp, xy[1] - yp).argmin())
-        return _as_psf_rows(g["parameters"][choose])
+        if xy is not None:
+            if band not in self._locs:
+                g = self.data[band]
+                self._locs[band] = (np.asarray(g["detector_locations"][:])
+                                    if "detector_locations" in g else None)
+            locs = self._locs[band]
+            if locs is not None:
+                xp, yp = locs
+                choose = int(np.hypot(xy[0] - xp, xy[1] - yp).argmin())
+        key = (band, choose)
+        if key not in self._rows:
+            self._rows[key] = _as_psf_rows(self.data[band]["parameters"][choose])
+        return self._rows[key].copy()
 
     def get_local_psf(self, band="F090W", source=None, wcs=None):
         xy = wcs.world_to_pixel_values(source.ra, source.dec) if wcs is not None else None
         return self.lookup(band, xy=xy)
 
     def n_psf_per_source(self, band):
-        return int(self.data[band].attrs["n_psf_per_source"])
+        key = ("npsf", band)
+        if key not in self._rows:
+            self._rows[key] = int(self.data[band].attrs["n_psf_per_source"])
+        return self._rows[key]
 
     @property
     def data(self):
