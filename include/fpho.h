@@ -11,7 +11,9 @@
  *     Calls are stream-ordered; a handle may be used by one host thread at a
  *     time.
  *   - Device memory is owned either by the caller (pointers passed in) or by
- *     a handle, freed by the matching *_free call.
+ *     a handle, freed by the matching *_free call.  Handle memory comes from
+ *     the device's default memory pool, which keeps freed memory for reuse
+ *     until the process exits; a *_free waits for the device first.
  *   - No torch, numpy or CUDA types appear in the signatures.
  *
  * Struct layouts below are the reference's device ABI and are byte-compatible
