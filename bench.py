@@ -44,6 +44,9 @@ WORKLOAD = "field20: 20 src, 8 bands x 4 exp x 128x128 px, 5-gauss PSF, 9 radii"
 # ncu capture (profiles/tile_kernel_dyn_64x4_field20.md): the 16 B per pixel
 # of the pixel arrays plus the image-Gaussian table, each read once.
 TILE_TRAFFIC_BYTES = 12673536
+# DRAM bytes of one store_copy launch packing a 471 k-pixel patch (ncu:
+# throughput x duration, profiles/store_kernels_packing32.md).
+STORE_COPY_TRAFFIC_BYTES = 3833600
 
 
 def parse():
@@ -545,7 +548,12 @@ def packing_leg(args, torch, n_patches):
             "identical_to_host": bool(identical), "store_upload_s": upload_s,
             "roofline": {"bound": "hbm", "kernel": "store_gather", "kernel_ms": g_ms,
                          "algorithmic_bytes_per_px": 24, "achieved": achieved, "peak": peak,
-                         "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_src}}
+                         "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_src,
+                         "traffic": STORE_COPY_TRAFFIC_BYTES,
+                         "traffic_source": "ncu DRAM bytes of one store_copy launch of a "
+                                           "471 k-pixel patch, "
+                                           "profiles/store_kernels_packing32.md (the reads; "
+                                           "the outputs stay in L2 during the kernel)"}}
 
 
 def differentiable_leg(args, torch, P, cfg, steps):
