@@ -491,6 +491,17 @@ def packing_leg(args, torch, n_patches):
         for r in regions[3:3 + n_host]:
             hp.build_patch(r, None, allbands=st["bands"])
         host_s = (time.perf_counter() - t0) / n_host
+        # all the regions in one count and one gather (GPUStorePatch.build_patches)
+        gp.build_patches(regions[3:], None, allbands=st["bands"])
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        many = gp.build_patches(regions[3:], None, allbands=st["bands"])
+        torch.cuda.synchronize()
+        many_s = time.perf_counter() - t0
+        many_ms = ds.last_gather_ms()
+        many_px = sum(q.npix for q in many)
+        del many
+
         # patches ready to evaluate: pixels, 20-source metadata, device handle
         cat = st["catalog"]
 
@@ -537,6 +548,12 @@ def packing_leg(args, torch, n_patches):
                         f"{mean_px:.0f} px per patch",
             "metric": "patches packed/s", "device_patches_per_s": 1.0 / dev_s,
             "host_patches_per_s": 1.0 / host_s, "speedup": host_s / dev_s,
+            "batched": {"what": f"{n_patches} patches per GPUStorePatch.build_patches call "
+                                "(one count, one gather)",
+                        "device_patches_per_s": n_patches / many_s,
+                        "gather_ms": many_ms, "pixels": many_px,
+                        "achieved_gbs": many_px * 24 / (many_ms * 1e-3) / 1e9,
+                        "frac": many_px * 24 / (many_ms * 1e-3) / 1e9 / peak},
             "ready": {"what": "pixels + 20-source metadata (pack_meta) + device patch handle "
                               "with its tile plan (send_to_device), per patch",
                       "device_per_s": 1.0 / dev_ready_s, "host_per_s": 1.0 / host_ready_s,
@@ -546,14 +563,22 @@ def packing_leg(args, torch, n_patches):
                            "reading only the selected super-pixels through a memory map (the "
                            "reference reads each exposure whole)",
             "identical_to_host": bool(identical), "store_upload_s": upload_s,
-            "roofline": {"bound": "hbm", "kernel": "store_gather", "kernel_ms": g_ms,
-                         "algorithmic_bytes_per_px": 24, "achieved": achieved, "peak": peak,
-                         "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_src,
-                         "traffic": STORE_COPY_TRAFFIC_BYTES,
-                         "traffic_source": "ncu DRAM bytes of one store_copy launch of a "
-                                           "471 k-pixel patch, "
-                                           "profiles/store_kernels_packing32.md (the reads; "
-                                           "the outputs stay in L2 during the kernel)"}}
+            "roofline": {"bound": "hbm", "kernel": "store_compact + store_copy",
+                         "workload": f"{n_patches} patches in one gather "
+                                     f"({many_px} pixels)",
+                         "kernel_ms": many_ms, "algorithmic_bytes_per_px": 24,
+                         "achieved": many_px * 24 / (many_ms * 1e-3) / 1e9, "peak": peak,
+                         "unit": "GB/s", "frac": many_px * 24 / (many_ms * 1e-3) / 1e9 / peak,
+                         "peak_source": peak_src, "traffic": None,
+                         "traffic_note": "the one-patch launch's DRAM traffic is the 8 B/px "
+                                         "of reads (profiles/store_kernels_packing32.md)"},
+            "single_patch_roofline": {
+                "kernel": "store_compact + store_copy", "kernel_ms": g_ms,
+                "achieved": achieved, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": STORE_COPY_TRAFFIC_BYTES,
+                "traffic_source": "ncu DRAM bytes of one store_copy launch of a 471 k-pixel "
+                                  "patch (the reads; the outputs stay in L2 during the "
+                                  "kernel)"}}
 
 
 def differentiable_leg(args, torch, P, cfg, steps):

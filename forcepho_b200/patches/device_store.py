@@ -154,6 +154,30 @@ class DeviceStore:
         total = int(n.astype(np.int64).sum())
         return [b[:total] for b in bufs], start, n
 
+    def gather_many(self, groups, max_snr=None, stream=None):
+        """Pack several patches in one count and one gather call.  `groups`
+        is a list of (indices, regions, background-or-None), one per patch;
+        returns, per patch, ((data, ierr, xpix, ypix) views of one shared
+        buffer, exposure_start relative to the patch, exposure_N)."""
+        if not groups:
+            return []
+        idx = np.concatenate([np.asarray(g[0], dtype=np.int32) for g in groups])
+        recs = np.concatenate([np.asarray(g[1], dtype=REGION_DTYPE) for g in groups])
+        bg = None
+        if any(g[2] is not None for g in groups):
+            bg = np.concatenate([np.zeros(len(g[0]), np.float32) if g[2] is None
+                                 else np.asarray(g[2], dtype=np.float32) for g in groups])
+        pix, start, n = self.gather(idx, recs, background=bg, max_snr=max_snr, stream=stream)
+        out, e0 = [], 0
+        for g in groups:
+            e1 = e0 + len(g[0])
+            p0 = int(start[e0]) if e1 > e0 else 0
+            p1 = p0 + int(np.asarray(n[e0:e1], dtype=np.int64).sum())
+            out.append(([t[p0:p1] for t in pix], (start[e0:e1] - p0).astype(np.int32),
+                        n[e0:e1].copy()))
+            e0 = e1
+        return out
+
     def time_gather(self, enable=True):
         """Time the gather kernel of every following :meth:`gather` with CUDA
         events; :meth:`last_gather_ms` reads the last one."""
@@ -246,6 +270,63 @@ class GPUStorePatch(StorePatch, GPUPatchMixin):
         pix, start, n = self.device_store.gather(idx, regs, background=self.background_offsets,
                                                  max_snr=getattr(self, "max_snr", None),
                                                  npix=npix)
+        self._install_pixels(pix, start, n)
+
+    def build_patches(self, regions, sourcecats=None, allbands=None, tweak_background=False):
+        """Build one patch per region with a single count and a single gather
+        over all of them (the copy kernel then moves every patch's pixels in
+        one launch).  Returns new GPUStorePatch objects sharing this one's
+        stores; each holds the same arrays ``build_patch`` gives for its
+        region.  `sourcecats`: one catalog per region, or None."""
+        import copy
+        allbands = list(allbands) if allbands is not None else list(self.metastore.headers)
+        rows, stack = self._exposure_table(allbands)
+        imsize = np.zeros(2) + self.pixelstore.nside_full
+        cands = []
+        for region in regions:
+            if not rows:
+                cands.append(([], None))
+                continue
+            bra, bdec = region.bounding_box
+            bx, by = stack.world_to_pixel_values(bra, bdec)
+            sel = np.flatnonzero(np.any((bx > 0) & (bx < imsize[0]) & (by > 0) &
+                                        (by < imsize[1]), axis=1))
+            recs = region_records(region, [r[2] for r in rows], stack)[sel]
+            cands.append((sel, recs))
+        all_idx = [rows[i][3] for sel, _ in cands for i in sel]
+        all_recs = [rec for sel, recs in cands if len(sel) for rec in recs]
+        counts = (self.device_store.count(all_idx, np.array(all_recs, dtype=REGION_DTYPE))
+                  if all_idx else np.zeros(0, np.int32))
+        patches, groups, k = [], [], 0
+        for (sel, recs), region in zip(cands, regions):
+            cnt = counts[k:k + len(sel)]
+            k += len(sel)
+            keep = [(rows[i], rec) for i, rec, c in zip(sel, recs if recs is not None else [],
+                                                          cnt) if c > 0]
+            if not keep:
+                raise ValueError("No exposures in the specified bands overlap the region")
+            p = copy.copy(self)
+            p.pixels, p.device_patch, p._records = None, None, {}
+            p.hdrs = [self.metastore.headers[r[0]][r[1]] for r, _ in keep]
+            p.wcses = [r[2] for r, _ in keep]
+            p.epaths = [f"{r[0]}/{r[1]}" for r, _ in keep]
+            p.bands = [r[0] for r, _ in keep]
+            p.background_offsets = ([h.get(tweak_background, 0.0) for h in p.hdrs]
+                                    if tweak_background else None)
+            p._set_band_index(allbands)
+            patches.append(p)
+            groups.append(([r[3] for r, _ in keep],
+                           np.array([rec for _, rec in keep], dtype=REGION_DTYPE),
+                           p.background_offsets))
+        packed = self.device_store.gather_many(groups, max_snr=getattr(self, "max_snr", None))
+        for i, (p, (pix, start, n)) in enumerate(zip(patches, packed)):
+            p._install_pixels(pix, start, n)
+            if sourcecats is not None:
+                p.pack_meta(p.set_scene(sourcecats[i]))
+            p._dirty_data = False
+        return patches
+
+    def _install_pixels(self, pix, start, n):
         self.pixels = dict(zip(["data", "ierr", "xpix", "ypix"], pix))
         for k in ("data", "ierr", "xpix", "ypix"):
             self.__dict__.pop(k, None)

@@ -258,3 +258,38 @@ def test_store_argument_errors():
         st.gather([0], rec, npix=64)              # the selection has more pixels
     assert st.count([0], rec)[0] > 1
     st.free()
+
+
+def test_build_patches_matches_one_at_a_time(store):
+    """GPUStorePatch.build_patches (one count and one gather for all the
+    regions) gives each patch the arrays build_patch gives it alone."""
+    from forcepho_b200.patches.device_store import DeviceStore, GPUStorePatch
+    from forcepho_b200.patches.storage import PixelStore
+    from forcepho_b200.region import CircularRegion
+    G = _cases()
+    ds = DeviceStore.from_pixelstore(PixelStore(store["pixelstore"]))
+    gp = GPUStorePatch(store["pixelstore"], store["metastore"], store["psfstore"],
+                       device_store=ds)
+    gp.max_snr = 100.0
+    rng = np.random.default_rng(4)
+    regions = [CircularRegion(53.16 + rng.uniform(-2, 2) / 3600, -27.78 + rng.uniform(-2, 2) / 3600,
+                              rng.uniform(1.0, 3.0) / 3600) for _ in range(6)]
+    regions.append(_region(*G.STORE_CASES[2][1:3]))           # an RA/Dec box
+    cats = [store["catalog"][: 1 + i % 4] for i in range(len(regions))]
+    many = gp.build_patches(regions, cats, allbands=store["bands"], tweak_background="BKG")
+    for region, cat, q in zip(regions, cats, many):
+        gp.build_patch(region, cat, allbands=store["bands"], tweak_background="BKG")
+        assert list(q.epaths) == list(gp.epaths)
+        for k in ("data", "ierr", "xpix", "ypix"):
+            np.testing.assert_array_equal(q.pixels[k].cpu().numpy(), gp.pixels[k].cpu().numpy())
+        for k in ("exposure_start", "exposure_N", "band_start", "band_N", "D", "CW", "crpix",
+                  "crval", "G", "psfgauss_start", "n_psf_per_source"):
+            np.testing.assert_array_equal(np.asarray(getattr(q, k)), np.asarray(getattr(gp, k)),
+                                          err_msg=k)
+    q = many[0]
+    q.send_to_device()                                        # a batch-packed patch evaluates
+    from forcepho_b200.proposal import GPUProposer
+    chi2, dchi2 = GPUProposer().evaluate_proposal(q.scene.get_proposal(), patch=q)
+    assert np.all(np.isfinite(chi2))
+    q.free()
+    ds.free()
