@@ -60,7 +60,7 @@ def _rect_params(rng, nx, ny):
     return RectangularRegion(ra - half, ra + half * 1.3, dec - half * 0.7, dec + half).device_params(w)
 
 
-@pytest.mark.parametrize("nx,ny,s", [(512, 384, 8), (256, 256, 4), (64, 136, 8)])
+@pytest.mark.parametrize("nx,ny,s", [(512, 384, 8), (256, 256, 4), (64, 136, 8), (96, 72, 3)])
 def test_gather_matches_oracle(nx, ny, s):
     from forcepho_b200.patches.device_store import DeviceStore, REGION_DTYPE
     rng = np.random.default_rng(nx + ny + s)
@@ -293,3 +293,36 @@ def test_build_patches_matches_one_at_a_time(store):
     assert np.all(np.isfinite(chi2))
     q.free()
     ds.free()
+
+
+def test_gather_unaligned_outputs():
+    """Output arrays that are not 16-byte aligned take the one-pixel-per-thread
+    copy; the result is the same as the oracle's."""
+    import ctypes
+    import torch
+    from forcepho_b200 import _lib
+    from forcepho_b200.patches.device_store import DeviceStore, REGION_DTYPE
+    nx, ny, s = 128, 96, 8
+    sps = _random_store(nx, ny, s, 2, seed=9)
+    st = DeviceStore((nx, ny), s, max_exposures=2)
+    for sp in sps:
+        st.add(sp)
+    regs = [(1, [40.5, 50.25, 30.0 ** 2]), (1, [100.0, 10.0, 25.0 ** 2])]
+    recs = np.zeros(2, dtype=REGION_DTYPE)
+    recs["kind"] = 1
+    recs["p"][:, :3] = [r[1] for r in regs]
+    want = OP.pack(sps, regs, max_snr=30.0)
+    npix = int(want["exposure_N"].sum())
+    bufs = [torch.zeros(npix + 1, dtype=torch.float32, device="cuda") for _ in range(4)]
+    start = np.zeros(2, np.int32)
+    n = np.zeros(2, np.int32)
+    idx = np.arange(2, dtype=np.int32)
+    _lib.call("fpho_store_gather", st.handle, 2, idx.ctypes.data, recs.ctypes.data, None,
+              ctypes.c_float(30.0), *[b.data_ptr() + 4 for b in bufs], npix, start.ctypes.data,
+              n.ctypes.data, torch.cuda.current_stream().cuda_stream)
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(n, want["exposure_N"])
+    for k, b in zip(("data", "ierr", "xpix", "ypix"), bufs):
+        np.testing.assert_array_equal(b[1:].cpu().numpy(), want[k], err_msg=k)
+        assert float(b[0]) == 0.0                 # nothing written before the output
+    st.free()
