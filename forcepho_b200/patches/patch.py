@@ -278,7 +278,13 @@ class Patch(PatchBase):
                 # the same for all sources, CW = (3600 D) diag(cos dec, 1), whose
                 # matrix product has exact zero and unit terms, so the columns
                 # are scaled elementwise with the same results
-                D_mat = np.linalg.inv(wcs.pixel_scale_matrix * 3600.0)
+                D_mat = getattr(wcs, "_linear_D", None)     # the same for every scene
+                if D_mat is None:
+                    D_mat = np.linalg.inv(wcs.pixel_scale_matrix * 3600.0)
+                    try:
+                        wcs._linear_D = D_mat
+                    except AttributeError:
+                        pass
                 A = D_mat * 3600.0
                 self.D[j] = D_mat
                 self.CW[j, :, :, 0] = A[None, :, 0] * cosd[:, None]
@@ -308,10 +314,13 @@ class Patch(PatchBase):
         self.psfgauss_start = np.zeros(self.n_exp, dtype=np.int32)
         n_psfgauss = int((self.n_psf_per_source * np.asarray(self.n_exp_per_band) * ns).sum())
         self.psfgauss = np.empty(n_psfgauss, dtype=PSF_DTYPE)
-        s = 0
+        blocks, tiled, s = [], {}, 0
         for e in range(self.n_exp):      # every source of an exposure gets its band's rows
+            if bands[e] not in tiled:
+                tiled[bands[e]] = np.tile(self.psfstore.lookup(bands[e]), ns)
             self.psfgauss_start[e] = s
-            rows = self.psfstore.lookup(bands[e])
-            self.psfgauss[s:s + ns * len(rows)] = np.tile(rows, ns)
-            s += ns * len(rows)
+            blocks.append(tiled[bands[e]])
+            s += len(tiled[bands[e]])
         assert s == n_psfgauss
+        self.psfgauss = np.concatenate(blocks).astype(PSF_DTYPE, copy=False) if blocks \
+            else self.psfgauss
