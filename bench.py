@@ -21,6 +21,10 @@ Printed JSON (rank 0):
              throughput measured live by a probe kernel on the same GPU;
   cpu_baseline  the reference's own CPU kernel (built from its sources into
              oracle/_ref) on all host cores, one evaluation of the same patch.
+Further legs on one GPU (each skippable): differentiable (LnLike + leapfrog
+in a CUDA graph), multichain (many HMC chains per launch), batched (256
+uneven patches in one persistent launch) and packing (patches packed from a
+GPU-resident exposure store against host packing of the same HDF5 store).
 The reference arm (--impl reference) times that CPU kernel over K steps.
 """
 
