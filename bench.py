@@ -73,7 +73,7 @@ def parse():
                     help="HMC chains of the multi-chain leg (single-source patch); 0 skips it")
     ap.add_argument("--no-differentiable", action="store_true",
                     help="skip the differentiable-form leg (20-source patch)")
-    ap.add_argument("--packing-patches", type=int, default=16,
+    ap.add_argument("--packing-patches", type=int, default=32,
                     help="patches packed from the exposure store in the packing leg; 0 skips it")
     return ap.parse_args()
 
