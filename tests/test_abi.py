@@ -92,3 +92,22 @@ def test_variants_listed():
     from forcepho_b200 import _lib
     v = _lib.variants()
     assert len(v) >= 4 and all(nt % 32 == 0 and k % 2 == 0 for nt, k in v)
+
+
+def test_store_and_device_pixel_create_reject_bad_arguments():
+    """Host-side checks of the exposure store and of
+    fpho_patch_create_device_pixels, made before any CUDA call."""
+    from forcepho_b200 import _lib
+    L = _lib.lib
+    h = ctypes.c_void_p()
+    assert L.fpho_store_create(100, 64, 8, 1, ctypes.byref(h)) == 1 and not h.value  # 100 % 8
+    assert "multiples" in _lib.last_error()
+    assert L.fpho_store_create(64, 64, 0, 1, ctypes.byref(h)) == 1
+    assert L.fpho_store_create(40000, 40000, 8, 1, ctypes.byref(h)) == 4
+    assert L.fpho_store_create(64, 64, 8, 0, ctypes.byref(h)) == 1
+    assert L.fpho_store_create(64, 64, 8, 1, None) == 1
+    counts = (ctypes.c_int32 * 1)()
+    assert L.fpho_store_count(None, 1, None, None, counts, None) == 1
+    assert L.fpho_store_free(None) == 0
+    rc = L.fpho_patch_create_device_pixels(None, 1, 0, None, ctypes.byref(h))
+    assert rc == 1 and "NULL" in _lib.last_error() and not h.value
