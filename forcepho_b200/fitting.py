@@ -9,11 +9,20 @@ conditional on their shapes, from ``patcher.design_matrix``).
 design matrix from one ``fpho_patch_design_matrix`` launch, the normal
 equations as FP64 matrix products (cuBLAS through torch), the solves by
 torch.linalg.
+
+:func:`run_hmc` and :func:`run_opt` keep the call shape and the result
+fields of forcepho's ``run_lmc`` and ``run_opt`` (fitting.py:255-342,
+415-454).  ``run_hmc`` samples with :class:`forcepho_b200.sampling.MultiChainHMC`
+on the GPU (static-length HMC with a jittered step size, one CUDA graph per
+iteration, any number of chains in one batched launch) instead of
+littlemcmc's NUTS on the host; ``run_opt`` is the same BFGS minimisation of
+the negative log posterior with scipy.
 """
 
 import numpy as np
 
-__all__ = ["optimize_one_band", "optimize_fluxes", "optimize_fluxes_device"]
+__all__ = ["optimize_one_band", "optimize_fluxes", "optimize_fluxes_device", "Result",
+           "run_hmc", "run_opt"]
 
 
 def optimize_one_band(X, w, y, fixedX=0):
@@ -68,3 +77,104 @@ def optimize_fluxes_device(patcher, active):
         fl.append(torch.linalg.solve(ata, Xp @ yp))
         pr.append(ata)
     return torch.stack(fl), torch.stack(pr)
+
+
+class Result:
+    """The fields forcepho's run_lmc / run_opt fill (fitting.py:318-342,
+    437-454): ndim, starting_position, chain, n_call, wall_time, and what
+    each sampler adds (lnp, fun, jac, message; accept, step_size)."""
+
+    def __init__(self, **kw):
+        self.__dict__.update(kw)
+
+
+def run_hmc(model, q, n_draws, warmup=(10,), n_chains=1, n_leapfrog=10, step_size=0.05,
+            target_accept=0.75, jitter=0.2, random_seed=0xDEADBEEF):
+    """HMC on the GPU with the call shape of forcepho's ``run_lmc``.
+
+    Parameters
+    ----------
+    model : forcepho_b200.autograd.DevicePosterior (one patch; chains are
+        device copies of it) or BatchPosterior (one chain per patch)
+    q : starting position in the constrained space, one chain's (broadcast
+        to every chain) or all chains' concatenated
+    n_draws : samples kept per chain
+    warmup : lengths of the tuning rounds; after each, the step size is
+        multiplied by exp(2 (acceptance - target_accept)), clipped to
+        [1/4, 4] per round
+    n_chains : chains of a DevicePosterior model (ignored for a batch)
+
+    Returns
+    -------
+    result : Result with ``chain`` of shape (n_draws, ndim) for one chain or
+        (n_chains, n_draws, ndim), in the constrained space, ``n_call`` (one
+        per chain per leapfrog step), ``wall_time``, ``accept`` (per chain,
+        production iterations), ``step_size``
+    sampler : the MultiChainHMC
+    """
+    import time
+    import torch
+    from .autograd import BatchPosterior, DevicePosterior
+    from .sampling import MultiChainHMC, chain_posterior
+    if isinstance(model, DevicePosterior):
+        lo = model.tr.lower.cpu().numpy()
+        hi = model.tr.upper.cpu().numpy()
+        post = chain_posterior(model.ev.patch, int(n_chains), lo, hi)
+    elif isinstance(model, BatchPosterior):
+        post, n_chains = model, model.n_patches
+    else:
+        raise TypeError("model must be a DevicePosterior or a BatchPosterior")
+    q = np.asarray(q, dtype=np.float64).reshape(-1)
+    if q.size * n_chains == post.ndim:
+        q = np.tile(q, n_chains)
+    if q.size != post.ndim:
+        raise ValueError(f"q has {q.size} entries; the chains need {post.ndim}")
+    z0 = post.inverse_transform(torch.as_tensor(q, device="cuda"))
+    hmc = MultiChainHMC(post, step_size, n_leapfrog, n_samples=int(n_draws),
+                        seed=int(random_seed) & 0x7FFFFFFF, jitter=jitter)
+    hmc.set_state(z0)
+    eps = float(step_size)
+    t0 = time.time()
+    for w in warmup:
+        hmc.n_accept.zero_()
+        hmc.run(int(w))
+        acc = float(np.mean(hmc.acceptance(int(w))))
+        eps *= float(np.clip(np.exp(2.0 * (acc - target_accept)), 0.25, 4.0))
+        hmc.set_eps(eps)
+    hmc.n_accept.zero_()
+    hmc.slot.zero_()
+    hmc.run(int(n_draws))
+    torch.cuda.synchronize()
+    wall = time.time() - t0
+    zs = hmc.samples[:int(n_draws)]
+    qs = post.transform(zs).cpu().numpy().reshape(int(n_draws), n_chains, -1)
+    chain = qs.transpose(1, 0, 2)
+    return Result(ndim=chain.shape[-1], starting_position=q.copy(),
+                  chain=chain[0] if n_chains == 1 else chain,
+                  n_call=int(n_chains * (sum(int(w) for w in warmup) + int(n_draws)) *
+                             n_leapfrog),
+                  wall_time=wall, accept=hmc.acceptance(int(n_draws)),
+                  step_size=hmc.eps), hmc
+
+
+def run_opt(model, q, jac=True, callback=None, **extras):
+    """BFGS minimisation of ``model.nll`` with scipy, as forcepho's run_opt:
+    start from the unconstrained image of `q`, return the optimum in the
+    constrained space (``chain`` of shape (1, ndim)), lnp = -fun/2."""
+    import time
+    from scipy.optimize import minimize
+    start = model.transform.inverse_transform(q) if model.transform is not None \
+        else np.array(q, dtype=np.float64)
+    t0 = time.time()
+    if jac:
+        res = minimize(model.nll, start.copy(), jac=True, method="BFGS", options=dict(extras),
+                       callback=callback)
+    else:
+        res = minimize(model.nll_nograd, start.copy(), jac=None, method="BFGS",
+                       options=dict(extras), callback=callback)
+    chain = np.atleast_2d(res.x)
+    if model.transform is not None:
+        chain = model.transform.transform(chain)
+    return Result(ndim=len(q), starting_position=np.array(q, dtype=np.float64).copy(),
+                  chain=chain, lnp=-0.5 * res.fun, wall_time=time.time() - t0, fun=res.fun,
+                  jac=res.jac, message=res.message), res

@@ -60,7 +60,9 @@ class MultiChainHMC:
 
     def __init__(self, posterior, eps, n_leapfrog, n_samples=0, seed=0, jitter=0.2):
         self.post = posterior
-        self.eps = float(eps)
+        # the step size lives on the device, so a captured iteration reads the
+        # current value (set_eps between replays tunes it)
+        self.eps_t = torch.full((), float(eps), dtype=torch.float64, device="cuda")
         self.jitter = float(jitter)
         self.L = int(n_leapfrog)
         n, k = posterior.ndim, posterior.n_patches
@@ -74,6 +76,14 @@ class MultiChainHMC:
         self.graph = None
         torch.cuda.manual_seed(seed)
 
+    @property
+    def eps(self):
+        return float(self.eps_t)
+
+    def set_eps(self, eps):
+        """New base step size for the following iterations (graph included)."""
+        self.eps_t.fill_(float(eps))
+
     def set_state(self, z0):
         self.z.copy_(torch.as_tensor(z0, dtype=torch.float64))
         _, g = self.post.lnprob_and_grad(self.z)
@@ -85,7 +95,7 @@ class MultiChainHMC:
         # a step size per chain, drawn uniformly within +-jitter of eps, so that
         # a fixed trajectory length cannot lock onto a period of the dynamics
         u = torch.rand(self.lnp.shape, dtype=torch.float64, device="cuda")
-        eps = (self.eps * (1.0 + self.jitter * (2.0 * u - 1.0)))[post.par_patch]
+        eps = (self.eps_t * (1.0 + self.jitter * (2.0 * u - 1.0)))[post.par_patch]
         h = 0.5 * eps
         p = torch.randn(self.z.shape, dtype=torch.float64, device="cuda")
         kin0 = _per_patch(post, p * p) * 0.5

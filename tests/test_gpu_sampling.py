@@ -126,3 +126,39 @@ def test_many_chains_on_single_source_patch():
     post.batch.free()
     for c in post.copies:
         c.free()
+
+
+def test_run_hmc_and_run_opt_call_shapes():
+    """fitting.run_hmc / run_opt keep the call shape and result fields of the
+    reference's run_lmc / run_opt (fitting.py:255-342, 415-454): chains in the
+    constrained space inside the bounds, call counts, a tuned step size that
+    a captured graph picks up, and BFGS raising the posterior."""
+    from forcepho_b200 import synth
+    from forcepho_b200.autograd import DevicePosterior, default_bounds
+    from forcepho_b200.fitting import run_hmc, run_opt
+    from forcepho_b200.model import FastPosterior
+    from forcepho_b200.proposal import GPUProposer
+    from forcepho_b200.sources import Scene
+    P = synth.make_workload("single", seed=4)
+    P.send_to_device()
+    lo, hi = default_bounds(P.params, P.n_bands)
+    post = DevicePosterior(P, lo, hi)
+    q0 = P.params.reshape(-1)
+    res, hmc = run_hmc(post, q0, n_draws=40, warmup=[30, 30], n_chains=4, n_leapfrog=8,
+                       step_size=0.05)
+    assert res.chain.shape == (4, 40, q0.size)
+    assert np.all(res.chain >= lo) and np.all(res.chain <= hi)
+    assert res.n_call == 4 * (60 + 40) * 8 and res.wall_time > 0
+    assert np.all(np.isfinite(res.chain)) and np.all(res.chain.std(axis=1) > 0)
+    assert 0.3 < res.accept.mean() <= 1.0 and res.step_size != 0.05
+    one, _ = run_hmc(post, q0, n_draws=10, warmup=[10], n_chains=1, n_leapfrog=5)
+    assert one.chain.shape == (10, q0.size)
+    fp = FastPosterior(GPUProposer(), P, scene=Scene(P.n_sources, P.n_bands, P.table),
+                       lower=lo, upper=hi)
+    start = 0.5 * (lo + hi) + 0.1 * (q0 - 0.5 * (lo + hi))
+    r, sci = run_opt(fp, start, maxiter=50)
+    assert r.chain.shape == (1, q0.size) and np.isfinite(r.lnp)
+    lnp_start = fp.lnprob(fp.transform.inverse_transform(start))
+    lnp_end = fp.lnprob(fp.transform.inverse_transform(r.chain[0]))
+    assert lnp_end > lnp_start
+    P.free()
