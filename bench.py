@@ -51,6 +51,9 @@ TILE_TRAFFIC_BYTES = 12673536
 # DRAM bytes of one store_copy launch packing a 471 k-pixel patch (ncu:
 # throughput x duration, profiles/store_kernels_packing32.md).
 STORE_COPY_TRAFFIC_BYTES = 3833600
+# ... and of the one store_copy launch packing the 32 patches of the packing
+# leg together (15.07 M pixels; same file).
+STORE_COPY_BATCH_TRAFFIC_BYTES = 261868000
 
 
 def parse():
@@ -573,9 +576,12 @@ def packing_leg(args, torch, n_patches):
                          "kernel_ms": many_ms, "algorithmic_bytes_per_px": 24,
                          "achieved": many_px * 24 / (many_ms * 1e-3) / 1e9, "peak": peak,
                          "unit": "GB/s", "frac": many_px * 24 / (many_ms * 1e-3) / 1e9 / peak,
-                         "peak_source": peak_src, "traffic": None,
-                         "traffic_note": "the one-patch launch's DRAM traffic is the 8 B/px "
-                                         "of reads (profiles/store_kernels_packing32.md)"},
+                         "peak_source": peak_src,
+                         "traffic": STORE_COPY_BATCH_TRAFFIC_BYTES if n_patches == 32 else None,
+                         "traffic_source": "ncu DRAM bytes (throughput x duration) of the "
+                                           "32-patch store_copy launch, "
+                                           "profiles/store_kernels_packing32.md; part of the "
+                                           "written output is still in L2 at its end"},
             "single_patch_roofline": {
                 "kernel": "store_compact + store_copy", "kernel_ms": g_ms,
                 "achieved": achieved, "unit": "GB/s", "frac": achieved / peak,
