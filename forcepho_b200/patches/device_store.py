@@ -345,6 +345,31 @@ class GPUStorePatch(StorePatch, GPUPatchMixin):
     def npix(self):
         return int(np.asarray(self.exposure_N, dtype=np.int64).sum())
 
+    def host_struct(self, residual=None, pointers=None):
+        """As PatchBase.host_struct, with the pixel fields pointing at the
+        device arrays (fpho_patch_replace_meta reads only the metadata
+        fields; patch creation copies the device arrays)."""
+        ptrs = {k: t.data_ptr() for k, t in (self.pixels or {}).items()
+                if k not in self.__dict__}
+        ptrs.update(pointers or {})
+        return super().host_struct(residual=residual, pointers=ptrs)
+
+    def _pixel_array(self, attr):
+        a = self.__dict__.get(attr)
+        if a is None and self.pixels is not None and attr in self.pixels:
+            a = self.pixels[attr].cpu().numpy()
+        return a if a is not None else getattr(self, attr)
+
+    def split_pix(self, attr):
+        """Per-exposure pieces of a pixel array (copied from the device when
+        the patch holds it there)."""
+        return np.split(self._pixel_array(attr), np.cumsum(self.exposure_N[:-1]))
+
+    def split_band(self, attr):
+        """Per-band pieces of a pixel array (copied from the device when the
+        patch holds it there)."""
+        return np.split(self._pixel_array(attr), np.cumsum(self.band_N_pix[:-1]))
+
     def pixels_to_host(self):
         """Copy the device pixel arrays into ``data``, ``ierr``, ``xpix``,
         ``ypix`` (numpy), as the host StorePatch holds them."""

@@ -326,3 +326,43 @@ def test_gather_unaligned_outputs():
         np.testing.assert_array_equal(b[1:].cpu().numpy(), want[k], err_msg=k)
         assert float(b[0]) == 0.0                 # nothing written before the output
     st.free()
+
+
+def test_fixed_sources_on_a_store_patch(store):
+    """The reference's fixed-source flow on a patch packed on the device:
+    subtract_fixed(fixed, active) leaves data - model(fixed) on the device, so
+    evaluating the active scene then gives the joint residual of all sources;
+    design_matrix and optimize_fluxes run on it (device_patch.py:113-238,
+    fitting.py:597-627)."""
+    from forcepho_b200.fitting import optimize_fluxes
+    from forcepho_b200.patches.device_store import GPUStorePatch
+    G = _cases()
+    region = _region(*G.STORE_CASES[0][1:3])
+    cat = store["catalog"]
+    fixed, active = cat[:2], cat[2:]
+
+    def patcher():
+        p = GPUStorePatch(store["pixelstore"], store["metastore"], store["psfstore"],
+                          return_residual=True)
+        p.build_patch(region, None, allbands=store["bands"])
+        return p
+
+    joint = patcher()
+    joint.pack_meta(joint.set_scene(cat))
+    joint.send_to_device()
+    _, _, r_joint = joint.get_proposer().evaluate_proposal(joint.scene.get_proposal(),
+                                                           patch=joint, unpack=False)
+    data = joint.retrieve_array("data")
+    joint.free()
+
+    seq = patcher()
+    proposer, scene = seq.subtract_fixed(fixed, active=active)
+    _, _, r_seq = proposer.evaluate_proposal(scene.get_proposal(), patch=seq, unpack=False)
+    scale = np.abs(data - r_joint).max()
+    assert scale > 0
+    np.testing.assert_allclose(r_seq, r_joint, rtol=0, atol=1e-4 * scale)
+    Xes, ys = seq.design_matrix(active)
+    assert len(Xes) == len(store["bands"]) and Xes[0].shape[0] == len(active)
+    fluxes, precisions = optimize_fluxes(seq, active)
+    assert np.all(np.isfinite(np.asarray(fluxes, dtype=float)))
+    seq.free()
