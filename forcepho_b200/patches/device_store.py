@@ -381,8 +381,6 @@ class GPUStorePatch(StorePatch, GPUPatchMixin):
         if self.pixels is None:
             raise RuntimeError("build_patch (or pack_pix) must run before send_to_device")
         ptrs = {k: t.data_ptr() for k, t in self.pixels.items()}
-        for k in ("data", "ierr", "xpix", "ypix"):   # host_struct coerces these if present
-            self.__dict__.pop(k, None)
         self.device_patch = DevicePatch(self, return_residual=self.return_residual,
                                         device_pixels=ptrs)
         self._dirty_data = False

@@ -153,6 +153,9 @@ def test_gpu_store_patch_matches_reference(store):
                   "crval", "G", "psfgauss_start"):
             np.testing.assert_array_equal(np.asarray(getattr(p, k)), gold[f"{name}/{k}"],
                                           err_msg=f"{name}/{k}")
+        p.send_to_device()                 # with host copies present: still the device arrays
+        np.testing.assert_array_equal(p.retrieve_array("data"), p.data)
+        p.free()
     dstore.free()
 
 
