@@ -92,7 +92,10 @@ class RectangularRegion(Region):
 
     def device_params(self, wcs):
         """The box and the TAN parameters the kernel needs to map corners to
-        the sky: crpix (1-based), CD, crval, lonpole."""
+        the sky: crpix (1-based), CD, crval, lonpole.  The kernel maps pixels
+        with the TAN projection alone, so distorted (SIP) WCSs are refused."""
+        if getattr(wcs, "has_distortion", False):
+            raise NotImplementedError("RA/Dec boxes on the device need an undistorted TAN WCS")
         p = [self.ra_min, self.ra_max, self.dec_min, self.dec_max,
              wcs.crpix[0], wcs.crpix[1], wcs.cd[0, 0], wcs.cd[0, 1], wcs.cd[1, 0], wcs.cd[1, 1],
              wcs.crval[0], wcs.crval[1], wcs.lonpole]

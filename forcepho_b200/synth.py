@@ -419,7 +419,7 @@ def store_header(band, nside, crval, crpix, rot_deg, scale=PIXEL_SCALE, bkg=0.0)
 
 def make_store(directory, n_bands=3, exposures_per_band=2, nside=256, super_pixel_size=8,
                seed=0, n_psf=3, n_sources=6, ra0=53.16, dec0=DEC0, rot_deg=20.0,
-               mask_frac=0.02, n_locations=2):
+               mask_frac=0.02, n_locations=2, sip=False):
     """Write a seeded pixel store (HDF5), metadata store (JSON) and PSF store
     (HDF5) in forcepho's layouts into `directory`, and return
     ``dict(pixelstore=, metastore=, psfstore=, bands=, catalog=, epaths=)``.
@@ -449,6 +449,14 @@ def make_store(directory, n_bands=3, exposures_per_band=2, nside=256, super_pixe
             crpix = (nx / 2.0 + rng.uniform(-3, 3), ny / 2.0 + rng.uniform(-3, 3))
             bkg = float(rng.normal(0.0, 0.01))
             hdr = store_header(b, (nx, ny), crval, crpix, rng.uniform(-rot_deg, rot_deg), bkg=bkg)
+            if sip:
+                hdr.update(CTYPE1="RA---TAN-SIP", CTYPE2="DEC--TAN-SIP", A_ORDER=3, B_ORDER=3)
+                scale = 4.0 / max(nx, ny) ** 2       # a few pixels at the image edge
+                for name in ("A", "B"):
+                    for p_, q_ in ((2, 0), (1, 1), (0, 2)):
+                        hdr[f"{name}_{p_}_{q_}"] = float(rng.normal(0.0, scale))
+                    for p_, q_ in ((3, 0), (2, 1), (1, 2), (0, 3)):
+                        hdr[f"{name}_{p_}_{q_}"] = float(rng.normal(0.0, scale / max(nx, ny)))
             xx, yy = np.meshgrid(np.arange(nx), np.arange(ny), indexing="ij")
             sky = 0.02 * np.sin(xx / 37.0) * np.cos(yy / 23.0) + bkg
             sigma = 0.05

@@ -8,9 +8,15 @@ forcepho/patches/patch.py:301-337).  astropy is not a dependency here;
 exposures carry -- ``RA---TAN``/``DEC--TAN`` with a ``CD`` or ``PC``+``CDELT``
 matrix, no distortion -- from the published projection equations (Calabretta &
 Greisen 2002, A&A 395, 1077: the zenithal TAN projection, eqs. 54-55, and the
-spherical rotation of eqs. 2 and 5 with the native pole at theta_0 = 90 deg).
-Pixel coordinates are 0-based, as astropy's ``*_values`` methods return them.
-Headers with SIP or other distortion keywords are refused.
+spherical rotation of eqs. 2 and 5 with the native pole at theta_0 = 90 deg),
+with the SIP polynomial distortion convention (Shupe et al. 2005, ASP Conf.
+Ser. 347, 491) for ``RA---TAN-SIP`` headers: (u, v) = pixel - CRPIX,
+(xi, eta) = CD (u + f(u, v), v + g(u, v)) with f = sum A_p_q u^p v^q and
+g = sum B_p_q u^p v^q.  The sky-to-pixel direction solves those polynomials
+by Newton iteration to 1e-10 pixel, starting from the inverse polynomials
+AP_p_q / BP_p_q when the header has them.  Pixel coordinates are 0-based, as
+astropy's ``*_values`` methods return them.  Other distortions (TPV, lookup
+tables) are refused.
 
 Both methods are vectorised over numpy arrays and computed in float64.
 """
@@ -36,8 +42,14 @@ class TanWCS:
         ct1, ct2 = str(hdr.get("CTYPE1", "")).strip(), str(hdr.get("CTYPE2", "")).strip()
         if not (ct1.startswith("RA---TAN") and ct2.startswith("DEC--TAN")):
             raise NotImplementedError(f"only RA---TAN/DEC--TAN is supported (got {ct1}, {ct2})")
-        if ct1 != "RA---TAN" or ct2 != "DEC--TAN" or "A_ORDER" in hdr or "B_ORDER" in hdr:
-            raise NotImplementedError("distortion (SIP, TPV, ...) is not supported")
+        sip = ct1 == "RA---TAN-SIP" and ct2 == "DEC--TAN-SIP"
+        if not sip and (ct1 != "RA---TAN" or ct2 != "DEC--TAN"):
+            raise NotImplementedError(f"distortion {ct1}/{ct2} is not supported (TAN and TAN-SIP "
+                                      "are)")
+        if not sip and ("A_ORDER" in hdr or "B_ORDER" in hdr):
+            raise NotImplementedError("SIP coefficients without a -SIP projection code")
+        self.sip = _read_sip(hdr) if sip else None
+        self.has_distortion = self.sip is not None
         self.crpix = np.array([float(hdr["CRPIX1"]), float(hdr["CRPIX2"])])
         self.crval = np.array([float(hdr["CRVAL1"]), float(hdr["CRVAL2"])])
         if "CD1_1" in hdr:
@@ -63,6 +75,8 @@ class TanWCS:
         y = np.asarray(y, dtype=np.float64)
         u = x + 1.0 - self.crpix[0]
         v = y + 1.0 - self.crpix[1]
+        if self.sip is not None:
+            u, v = u + _poly(self.sip["A"], u, v), v + _poly(self.sip["B"], u, v)
         xi = self.cd[0, 0] * u + self.cd[0, 1] * v
         eta = self.cd[1, 0] * u + self.cd[1, 1] * v
         r = np.hypot(xi, eta)
@@ -95,6 +109,8 @@ class TanWCS:
         eta = -r * np.cos(phi)
         u = self.cdinv[0, 0] * xi + self.cdinv[0, 1] * eta
         v = self.cdinv[1, 0] * xi + self.cdinv[1, 1] * eta
+        if self.sip is not None:
+            u, v = _sip_invert(self.sip, u, v)
         return u + self.crpix[0] - 1.0, v + self.crpix[1] - 1.0
 
     # astropy's older names
@@ -104,6 +120,67 @@ class TanWCS:
     def all_world2pix(self, ra, dec, origin=0):
         x, y = self.world_to_pixel_values(ra, dec)
         return x + origin, y + origin
+
+
+def _read_sip(hdr):
+    """SIP coefficient tables {name: {(p, q): value}} for A, B (and AP, BP if
+    present) from a header."""
+    out = {}
+    for name in ("A", "B", "AP", "BP"):
+        order = hdr.get(f"{name}_ORDER")
+        if order is None:
+            if name in ("A", "B"):
+                raise ValueError(f"TAN-SIP header without {name}_ORDER")
+            continue
+        coef = {}
+        for p in range(int(order) + 1):
+            for q in range(int(order) + 1 - p):
+                c = hdr.get(f"{name}_{p}_{q}")
+                if c:
+                    coef[(p, q)] = float(c)
+        out[name] = coef
+    return out
+
+
+def _poly(coef, u, v):
+    """sum over (p, q) of coef * u^p v^q."""
+    out = np.zeros(np.broadcast(u, v).shape)
+    for (p, q), c in coef.items():
+        out = out + c * u ** p * v ** q
+    return out
+
+
+def _poly_grad(coef, u, v):
+    du = np.zeros(np.broadcast(u, v).shape)
+    dv = np.zeros_like(du)
+    for (p, q), c in coef.items():
+        if p:
+            du = du + c * p * u ** (p - 1) * v ** q
+        if q:
+            dv = dv + c * q * u ** p * v ** (q - 1)
+    return du, dv
+
+
+def _sip_invert(sip, U, V, tol=1e-10, max_iter=50):
+    """(u, v) with u + f(u, v) = U, v + g(u, v) = V (Newton iteration from the
+    inverse polynomials, or from (U, V))."""
+    U = np.asarray(U, dtype=np.float64)
+    V = np.asarray(V, dtype=np.float64)
+    if "AP" in sip and "BP" in sip:
+        u, v = U + _poly(sip["AP"], U, V), V + _poly(sip["BP"], U, V)
+    else:
+        u, v = U.copy(), V.copy()
+    for _ in range(max_iter):
+        fu, gu = u + _poly(sip["A"], u, v) - U, v + _poly(sip["B"], u, v) - V
+        if np.all(np.abs(fu) < tol) and np.all(np.abs(gu) < tol):
+            break
+        adu, adv = _poly_grad(sip["A"], u, v)
+        bdu, bdv = _poly_grad(sip["B"], u, v)
+        j11, j12, j21, j22 = 1.0 + adu, adv, bdu, 1.0 + bdv
+        det = j11 * j22 - j12 * j21
+        u = u - (j22 * fu - j12 * gu) / det
+        v = v - (j11 * gu - j21 * fu) / det
+    return u, v
 
 
 def scale_at_sky(sky, wcs, dpix=1.0, make_approx=False):
@@ -151,6 +228,8 @@ class TanWCSStack:
     one numpy pass)."""
 
     def __init__(self, wcses):
+        self.wcses = list(wcses)
+        self.distorted = any(getattr(w, "has_distortion", False) for w in self.wcses)
         self.crpix = np.array([w.crpix for w in wcses], dtype=np.float64).reshape(-1, 2)
         self.crval = np.array([w.crval for w in wcses], dtype=np.float64).reshape(-1, 2)
         self.cdinv = np.array([w.cdinv for w in wcses], dtype=np.float64).reshape(-1, 2, 2)
@@ -160,6 +239,11 @@ class TanWCSStack:
         return len(self.lonpole)
 
     def world_to_pixel_values(self, ra, dec):
+        if self.distorted:      # SIP: one WCS at a time
+            xy = [w.world_to_pixel_values(np.atleast_1d(ra), np.atleast_1d(dec))
+                  for w in self.wcses]
+            return (np.array([p[0] for p in xy]).reshape(len(xy), -1),
+                    np.array([p[1] for p in xy]).reshape(len(xy), -1))
         ra = np.atleast_1d(np.asarray(ra, dtype=np.float64))[None, :] * _D2R
         dec = np.atleast_1d(np.asarray(dec, dtype=np.float64))[None, :] * _D2R
         a0, d0 = self.crval[:, :1] * _D2R, self.crval[:, 1:] * _D2R

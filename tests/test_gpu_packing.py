@@ -369,3 +369,27 @@ def test_fixed_sources_on_a_store_patch(store):
     fluxes, precisions = optimize_fluxes(seq, active)
     assert np.all(np.isfinite(np.asarray(fluxes, dtype=float)))
     seq.free()
+
+
+def test_gpu_store_patch_with_sip_headers(tmp_path):
+    """Exposures whose headers carry SIP distortion: the device packing (circle
+    centre and radius mapped by the SIP-aware WCS on the host) equals the host
+    StorePatch's; RA/Dec boxes, which the kernel maps with TAN alone, are
+    refused for them."""
+    from forcepho_b200 import synth
+    from forcepho_b200.patches.device_store import GPUStorePatch
+    from forcepho_b200.patches.pixel_patch import StorePatch
+    from forcepho_b200.region import CircularRegion, RectangularRegion
+    st = synth.make_store(str(tmp_path), seed=5, sip=True, n_bands=2, exposures_per_band=2)
+    region = CircularRegion(53.16, -27.78, 2.5 / 3600)
+    host = StorePatch(st["pixelstore"], st["metastore"], st["psfstore"])
+    host.build_patch(region, st["catalog"], allbands=st["bands"])
+    dev = GPUStorePatch(st["pixelstore"], st["metastore"], st["psfstore"])
+    dev.build_patch(region, st["catalog"], allbands=st["bands"])
+    assert list(dev.epaths) == list(host.epaths)
+    for k in ("data", "ierr", "xpix", "ypix"):
+        np.testing.assert_array_equal(dev.pixels[k].cpu().numpy(), getattr(host, k), err_msg=k)
+    np.testing.assert_array_equal(dev.CW, host.CW)
+    with pytest.raises(NotImplementedError):
+        dev.build_patch(RectangularRegion(53.159, 53.161, -27.781, -27.779), None,
+                        allbands=st["bands"])

@@ -293,3 +293,60 @@ def test_direct_patch_and_metastore(store):
     hdr = ms.headers[store["bands"][0]]["exp00"]
     assert CircularRegion(53.16, -27.78, 1.0 / 3600).overlaps(hdr)
     assert not RectangularRegion(54.0, 54.1, -27.0, -26.9).overlaps(hdr)
+
+
+def test_tan_sip_wcs():
+    """TAN-SIP (Shupe et al. 2005): zero coefficients give TAN exactly; the
+    sky-to-pixel Newton inversion round-trips a distortion of several pixels
+    to 1e-8 px, from the inverse polynomials when present; scale_at_sky takes
+    the finite-difference branch and matches the local Jacobian."""
+    from forcepho_b200 import synth
+    from forcepho_b200.wcs import TanWCS, scale_at_sky
+    h = synth.store_header("F200W", (2048, 2048), (53.1, -27.8), (1024.3, 1020.7), 17.0)
+    h0 = dict(h, CTYPE1="RA---TAN-SIP", CTYPE2="DEC--TAN-SIP", A_ORDER=3, B_ORDER=3)
+    w, w0 = TanWCS(h), TanWCS(h0)
+    xy = np.random.default_rng(1).uniform(-100, 2100, (2, 400))
+    np.testing.assert_array_equal(np.array(w.pixel_to_world_values(*xy)),
+                                  np.array(w0.pixel_to_world_values(*xy)))
+    h1 = dict(h0, A_2_0=2e-6, A_1_1=-3e-6, A_0_2=1e-6, A_3_0=4e-10, B_2_0=-1e-6, B_0_2=3e-6,
+              B_1_2=-2e-10)
+    w1 = TanWCS(h1)
+    assert w1.has_distortion and not w.has_distortion
+    rd = w1.pixel_to_world_values(*xy)
+    assert np.abs(np.array(w.world_to_pixel_values(*rd)) - xy).max() > 3.0
+    np.testing.assert_allclose(np.array(w1.world_to_pixel_values(*rd)), xy, rtol=0, atol=1e-8)
+    h2 = dict(h1, AP_ORDER=2, BP_ORDER=2, AP_2_0=-2e-6, AP_1_1=3e-6, AP_0_2=-1e-6, BP_2_0=1e-6,
+              BP_0_2=-3e-6)
+    np.testing.assert_allclose(np.array(TanWCS(h2).world_to_pixel_values(*rd)), xy, rtol=0,
+                               atol=1e-8)
+    sky = (53.1003, -27.7996)
+    CW, D = scale_at_sky(sky, w1)
+    x0, y0 = w1.world_to_pixel_values(*sky)
+    d = 1e-3
+    J = np.array([np.subtract(w1.pixel_to_world_values(x0 + d, y0),
+                              w1.pixel_to_world_values(x0 - d, y0)),
+                  np.subtract(w1.pixel_to_world_values(x0, y0 + d),
+                              w1.pixel_to_world_values(x0, y0 - d))]).T / (2 * d)
+    np.testing.assert_allclose(CW, np.linalg.inv(J), rtol=1e-4)
+    with pytest.raises(NotImplementedError):
+        TanWCS(dict(h, CTYPE1="RA---TPV", CTYPE2="DEC--TPV"))
+
+
+def test_store_patch_with_sip_headers(tmp_path):
+    """A store whose headers carry SIP distortion packs on the host: the
+    super-pixels selected are those whose corners the SIP-aware WCS puts in
+    the circle, and the astrometry uses the finite-difference scale."""
+    from oracle import packing as OP
+    from forcepho_b200 import synth
+    from forcepho_b200.patches.pixel_patch import StorePatch
+    from forcepho_b200.region import CircularRegion
+    st = synth.make_store(str(tmp_path), seed=5, sip=True, n_bands=2, exposures_per_band=2)
+    p = StorePatch(st["pixelstore"], st["metastore"], st["psfstore"])
+    region = CircularRegion(53.16, -27.78, 2.5 / 3600)
+    p.build_patch(region, st["catalog"], allbands=st["bands"])
+    assert all(w.has_distortion for w in p.wcses)
+    sps = [np.asarray(p.pixelstore.data[e + "/data"].array()) for e in p.epaths]
+    want = OP.pack(sps, [region.device_params(w) for w in p.wcses])
+    for k in ("data", "ierr", "xpix", "ypix"):
+        np.testing.assert_array_equal(getattr(p, k), want[k], err_msg=k)
+    assert np.all(np.isfinite(p.CW)) and np.all(np.isfinite(p.crpix))
