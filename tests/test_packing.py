@@ -350,3 +350,68 @@ def test_store_patch_with_sip_headers(tmp_path):
     for k in ("data", "ierr", "xpix", "ypix"):
         np.testing.assert_array_equal(getattr(p, k), want[k], err_msg=k)
     assert np.all(np.isfinite(p.CW)) and np.all(np.isfinite(p.crpix))
+
+
+def test_h5_random_trees_roundtrip(tmp_path):
+    """Random trees of groups and datasets (dtypes, shapes incl. scalars and
+    empty arrays, attributes) survive h5lite.write -> h5lite.read_tree."""
+    from hypothesis import given, settings, strategies as stn
+    from forcepho_b200 import h5lite
+
+    dtypes = [np.int8, np.uint16, np.int32, np.int64, np.float32, np.float64]
+    names = stn.text(alphabet="abcdefghijklmnopqrstuvwxyz0123456789_", min_size=1, max_size=8)
+
+    @settings(max_examples=25, deadline=None)
+    @given(stn.dictionaries(stn.lists(names, min_size=1, max_size=3).map("/".join),
+                            stn.tuples(stn.sampled_from(dtypes),
+                                       stn.lists(stn.integers(0, 5), max_size=3),
+                                       stn.integers(0, 2 ** 31)),
+                            min_size=1, max_size=12),
+           stn.floats(allow_nan=False, allow_infinity=False), stn.integers(-2 ** 40, 2 ** 40))
+    def check(spec, fattr, iattr):
+        # a path may not be both a dataset and a group
+        paths = sorted(spec)
+        keep = [p for p in paths if not any(q.startswith(p + "/") for q in paths)]
+        ds = {}
+        for p in keep:
+            dt, shape, seed = spec[p]
+            rng = np.random.default_rng(seed)
+            a = (rng.normal(size=shape) * 100).astype(dt) if shape else dt(rng.integers(0, 100))
+            ds[p] = a
+        path = str(tmp_path / "r.h5")
+        h5lite.write(path, ds, {"/": {"f": fattr, "i": iattr, "s": "x"}})
+        data, attrs = h5lite.read_tree(path)
+        assert set(data) == set(ds)
+        for p, a in ds.items():
+            got = np.asarray(data[p])
+            assert got.dtype == np.asarray(a).dtype and got.shape == np.shape(a), p
+            np.testing.assert_array_equal(got, a)
+        assert attrs["/"]["f"] == fattr and attrs["/"]["i"] == iattr and attrs["/"]["s"] == "x"
+
+    check()
+
+
+def test_wcs_random_roundtrip():
+    """Random TAN and TAN-SIP WCSs (rotation, scale, reference point, pole
+    distance) map pixels to the sky and back to 1e-7 px."""
+    from hypothesis import given, settings, strategies as stn
+    from forcepho_b200 import synth
+    from forcepho_b200.wcs import TanWCS
+
+    @settings(max_examples=60, deadline=None)
+    @given(stn.floats(0.0, 359.9), stn.floats(-85.0, 85.0), stn.floats(-180.0, 180.0),
+           stn.floats(0.01, 0.2), stn.booleans(), stn.integers(0, 2 ** 31))
+    def check(ra0, dec0, rot, scale, sip, seed):
+        rng = np.random.default_rng(seed)
+        h = synth.store_header("F200W", (2048, 2048), (ra0, dec0), (1024.5, 1000.0), rot,
+                               scale=scale)
+        if sip:
+            h.update(CTYPE1="RA---TAN-SIP", CTYPE2="DEC--TAN-SIP", A_ORDER=2, B_ORDER=2,
+                     A_2_0=rng.normal(0, 1e-6), A_1_1=rng.normal(0, 1e-6),
+                     B_0_2=rng.normal(0, 1e-6))
+        w = TanWCS(h)
+        xy = rng.uniform(-500, 2500, (2, 50))
+        back = np.array(w.world_to_pixel_values(*w.pixel_to_world_values(*xy)))
+        assert np.abs(back - xy).max() < 1e-7
+
+    check()
