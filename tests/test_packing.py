@@ -415,3 +415,28 @@ def test_wcs_random_roundtrip():
         assert np.abs(back - xy).max() < 1e-7
 
     check()
+
+
+def test_store_helpers(store, tmp_path):
+    """MetaStore write/read round trip, header_to_id (storage.py:39-57) and
+    PSFStore's nearest-detector-location lookup (storage.py:548-562)."""
+    from forcepho_b200.patches.storage import MetaStore, PSFStore, header_to_id
+    ms = MetaStore(store["metastore"])
+    out = str(tmp_path / "meta2.json")
+    ms.write_to_file(out)
+    ms2 = MetaStore(out)
+    assert ms2.headers == ms.headers and ms2.nexp == ms.nexp == len(store["epaths"])
+    hdr = {"FILTER": "F444W", "DETECTOR": "NRCALONG"}
+    assert header_to_id(hdr, "/data/frames/sub/jw001_cal.fits") == ("F444W", "jw001_cal")
+    assert header_to_id(hdr, "/data/frames/sub/jw001_cal.fits",
+                        framedir="/data/frames") == ("F444W", "sub/jw001_cal")
+    assert header_to_id(hdr, "x.fits", split_by_detector=["F444W"]) == ("F444WA", "x")
+    psf = PSFStore(store["psfstore"])
+    band = store["bands"][0]
+    locs = np.asarray(psf.data[band]["detector_locations"][:])
+    pars = psf.data[band]["parameters"][:]
+    for k in range(locs.shape[1]):
+        rows = psf.lookup(band, xy=(locs[0, k] + 0.1, locs[1, k] - 0.1))
+        np.testing.assert_array_equal(rows["amp"], pars[k]["amp"])
+    np.testing.assert_array_equal(psf.lookup(band)["Cxx"], pars[0]["Cxx"])
+    assert psf.n_psf_per_source(band) == pars.shape[1]
