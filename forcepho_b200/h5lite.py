@@ -19,7 +19,10 @@ those files directly, following the published HDF5 File Format Specification
 
 Chunked or compressed datasets, dense attribute storage and the "latest"
 link-message groups are not supported; opening such an object raises
-``NotImplementedError``.  Contiguous datasets are returned as read-only
+``NotImplementedError``.  The reader is checked on forcepho's own data files
+(Sersic tables, PSF store); the writer follows the same structures and is
+checked by round trips through the reader, not against libhdf5, which is not
+available here.  Contiguous datasets are returned as read-only
 ``numpy.memmap`` views, so slicing a large pixel store reads only what is
 used.
 """
