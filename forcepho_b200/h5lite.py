@@ -395,8 +395,10 @@ class File(Group):
         self.close()
 
 
-def read_tree(path):
-    """{path: array} of every dataset and {path: attrs} of every object."""
+def read_tree(path, memmap=False):
+    """{path: array} of every dataset and {path: attrs} of every object.
+    With `memmap`, contiguous datasets come back as read-only memory maps
+    (nothing is read until used)."""
     data, attrs = {}, {}
     with File(path) as f:
         def walk(g, prefix):
@@ -407,7 +409,12 @@ def read_tree(path):
                 if isinstance(node, Group):
                     walk(node, p)
                 else:
-                    data[p] = node[...] if not node.shape else np.array(node[:])
+                    if not node.shape:
+                        data[p] = node[...]
+                    elif memmap:
+                        data[p] = node.array()
+                    else:
+                        data[p] = np.array(node[:])
                     attrs[p] = dict(node.attrs)
         walk(f, "")
     return data, attrs
@@ -491,18 +498,41 @@ def _attr_message(name, value):
 
 
 class _Out:
+    """The file being laid out: structures are kept as (address, bytes);
+    dataset contents as (address, array) and streamed to the file at the
+    end, so writing a large store needs memory for its structures only."""
+
     def __init__(self):
-        self.buf = bytearray(b"\0" * 96)
+        self.end = 96                 # the superblock comes first
+        self.chunks = {}
+        self.raw = []
 
     def alloc(self, n, align=8):
-        pad = (-len(self.buf)) % align
-        self.buf += b"\0" * pad
-        addr = len(self.buf)
-        self.buf += b"\0" * n
+        self.end += (-self.end) % align
+        addr = self.end
+        self.end += n
         return addr
 
     def put(self, addr, b):
-        self.buf[addr:addr + len(b)] = b
+        self.chunks[addr] = bytes(b)
+
+    def put_array(self, addr, a):
+        self.raw.append((addr, a))
+
+    def get(self, addr, n):
+        return self.chunks[addr][:n]
+
+    def save(self, f, block=1 << 26):
+        f.truncate(self.end)
+        for addr, b in self.chunks.items():
+            f.seek(addr)
+            f.write(b)
+        for addr, a in self.raw:
+            flat = a.reshape(-1)
+            step = max(1, block // max(a.itemsize, 1))
+            f.seek(addr)
+            for i in range(0, flat.size, step):
+                f.write(np.ascontiguousarray(flat[i:i + step]).tobytes())
 
 
 def _header(out, msgs):
@@ -582,7 +612,7 @@ def _write_dataset(out, ds):
     if a.dtype.byteorder == ">":
         a = a.astype(a.dtype.newbyteorder("<"))
     raw = out.alloc(a.nbytes)
-    out.put(raw, a.tobytes())
+    out.put_array(raw, a)
     msgs = [(0x01, _space_message(a.shape)),
             (0x03, _dt_message(a.dtype)),
             (0x05, struct.pack("<BBBB", 2, 2, 2, 0)),   # fill value: never written
@@ -620,25 +650,25 @@ def write(path, datasets, attrs=None):
 
     out = _Out()
     root_addr = _write_group(out, root)
-    eof = len(out.buf)
     sb = _SIG + struct.pack("<BBBBBBBBHHI", 0, 0, 0, 0, 0, 8, 8, 0, _LEAF_K, _NODE_K, 0)
-    sb += struct.pack("<QQQQ", 0, _UNDEF, eof, _UNDEF)
+    sb += struct.pack("<QQQQ", 0, _UNDEF, out.end, _UNDEF)
     # root symbol table entry, caching the root's B-tree and heap
-    msgs = dict(_messages_in_buffer(out.buf, root_addr))
+    msgs = dict(_messages_in_header(out, root_addr))
     btree, heap = struct.unpack("<QQ", msgs[0x11][:16])
     sb += struct.pack("<QQII", 0, root_addr, 1, 0) + struct.pack("<QQ", btree, heap)
     out.put(0, sb)
     tmp = path + ".tmp"
     with open(tmp, "wb") as f:
-        f.write(out.buf)
+        out.save(f)
     os.replace(tmp, path)
 
 
-def _messages_in_buffer(buf, addr):
-    version, _, n, _, hsize = struct.unpack("<BBHII", bytes(buf[addr:addr + 12]))
-    q, end, out = addr + 16, addr + 16 + hsize, []
+def _messages_in_header(out, addr):
+    b = out.chunks[addr]
+    version, _, n, _, hsize = struct.unpack("<BBHII", b[:12])
+    q, end, msgs = 16, 16 + hsize, []
     while q + 8 <= end:
-        mtype, msize = struct.unpack("<HH", bytes(buf[q:q + 4]))
-        out.append((mtype, bytes(buf[q + 8:q + 8 + msize])))
+        mtype, msize = struct.unpack("<HH", b[q:q + 4])
+        msgs.append((mtype, b[q + 8:q + 8 + msize]))
         q += 8 + msize
-    return out
+    return msgs

@@ -131,7 +131,7 @@ class PixelStore:
         """Background-subtract, mask, optionally flux-calibrate and
         super-pixelize one exposure and write it as ``band/expID/data``
         (storage.py:151-243; an existing dataset of that path is replaced).
-        The whole file is rewritten."""
+        The whole file is rewritten (see write_exposures)."""
         band, expID, hdr = imset.band, imset.expID, imset.hdr
         im = np.array(imset.im, dtype=np.float64 if np.asarray(imset.im).dtype == np.float64
                       else np.float32)
@@ -173,9 +173,11 @@ class PixelStore:
         self.write_exposures({EXP_FMT.format(band, expID): (superpixels, attrs)})
 
     def write_exposures(self, exposures):
-        """Add or replace exposures: {"band/expID": (superpixels, attrs)}."""
+        """Add or replace exposures: {"band/expID": (superpixels, attrs)}.
+        The file is rewritten; existing exposures are streamed from a memory
+        map of the old file, so memory use does not grow with the store."""
         self.close()
-        data, attrs = h5lite.read_tree(self.h5file)
+        data, attrs = h5lite.read_tree(self.h5file, memmap=True)
         for path, (sp, at) in exposures.items():
             data[path + "/data"] = np.asarray(sp, dtype=self.pix_dtype)
             attrs[path + "/data"] = dict(at)

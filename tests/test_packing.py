@@ -440,3 +440,26 @@ def test_store_helpers(store, tmp_path):
         np.testing.assert_array_equal(rows["amp"], pars[k]["amp"])
     np.testing.assert_array_equal(psf.lookup(band)["Cxx"], pars[0]["Cxx"])
     assert psf.n_psf_per_source(band) == pars.shape[1]
+
+
+def test_h5_streamed_write_in_blocks(tmp_path, monkeypatch):
+    """Dataset contents are streamed to the file in blocks (here forced to 1000
+    bytes) and a rewrite reads the old datasets through memory maps."""
+    from forcepho_b200 import h5lite
+    from forcepho_b200.patches.storage import PixelStore
+    monkeypatch.setattr(h5lite._Out.save, "__defaults__", (1000,))
+    rng = np.random.default_rng(2)
+    big = rng.normal(size=(37, 11, 29)).astype(np.float64)
+    path = str(tmp_path / "s.h5")
+    h5lite.write(path, {"g/big": big, "g/small": np.arange(3, dtype=np.int16)})
+    data, _ = h5lite.read_tree(path, memmap=True)
+    assert isinstance(data["g/big"], np.memmap)
+    np.testing.assert_array_equal(data["g/big"], big)
+    ps = PixelStore(str(tmp_path / "p.h5"), nside_full=16, super_pixel_size=8)
+    sp = [rng.normal(size=(2, 2, 128)).astype(np.float32) for _ in range(3)]
+    for i, a in enumerate(sp):
+        ps.write_exposures({f"F200W/e{i}": (a, {"k": i})})
+    ps2 = PixelStore(str(tmp_path / "p.h5"))
+    for i, a in enumerate(sp):
+        np.testing.assert_array_equal(ps2.data[f"F200W/e{i}/data"][:], a)
+        assert ps2.data[f"F200W/e{i}/data"].attrs["k"] == i
