@@ -84,8 +84,46 @@ class Result:
     437-454): ndim, starting_position, chain, n_call, wall_time, and what
     each sampler adds (lnp, fun, jac, message; accept, step_size)."""
 
-    def __init__(self, **kw):
+    def __init__(self, filename=None, **kw):
         self.__dict__.update(kw)
+        if filename is not None:
+            self.read_from_h5(filename)
+
+    def dump_to_h5(self, filename, verbose=False):
+        """Save the attributes to an HDF5 file as forcepho's Result does
+        (fitting.py:186-207): arrays as datasets, other values as attributes
+        of the root group; returns messages for values that cannot be stored."""
+        import os
+        from . import h5lite
+        datasets, attrs, msgs = {}, {}, []
+        for name, value in vars(self).items():
+            if isinstance(value, np.ndarray) and value.dtype != object:
+                datasets[name] = value
+            elif isinstance(value, (str, bytes, bool, int, float, np.generic)):
+                attrs[name] = value
+            else:
+                msgs.append(f"could not save {name} with value {value!r} to {filename}")
+        if verbose:
+            for m in msgs:
+                print(m)
+        d = os.path.dirname(filename)
+        if d:
+            os.makedirs(d, exist_ok=True)
+        h5lite.write(filename, datasets, {"/": attrs})
+        return msgs
+
+    def read_from_h5(self, filename):
+        """Read the datasets and root attributes of an HDF5 file (written by
+        :meth:`dump_to_h5` or by forcepho) into attributes."""
+        from . import h5lite
+        with h5lite.File(filename) as f:
+            for k in f.keys():
+                node = f[k]
+                if not isinstance(node, h5lite.Group):
+                    setattr(self, k, node[...] if not node.shape else np.array(node[:]))
+            for k, v in f.attrs.items():
+                setattr(self, k, v)
+        return self
 
 
 def run_hmc(model, q, n_draws, warmup=(10,), n_chains=1, n_leapfrog=10, step_size=0.05,

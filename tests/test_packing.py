@@ -463,3 +463,18 @@ def test_h5_streamed_write_in_blocks(tmp_path, monkeypatch):
     for i, a in enumerate(sp):
         np.testing.assert_array_equal(ps2.data[f"F200W/e{i}/data"][:], a)
         assert ps2.data[f"F200W/e{i}/data"].attrs["k"] == i
+
+
+def test_result_h5_roundtrip(tmp_path):
+    """fitting.Result.dump_to_h5 / read_from_h5 as forcepho's Result
+    (fitting.py:186-218): arrays as datasets, scalars and strings as
+    attributes, anything else reported."""
+    from forcepho_b200.fitting import Result
+    r = Result(ndim=7, chain=np.arange(21.0).reshape(3, 7), wall_time=1.5, message="ok",
+               accept=np.array([0.8, 0.7]), sampler=object())
+    msgs = r.dump_to_h5(str(tmp_path / "out" / "r.h5"))
+    assert len(msgs) == 1 and "sampler" in msgs[0]
+    back = Result(filename=str(tmp_path / "out" / "r.h5"))
+    np.testing.assert_array_equal(back.chain, r.chain)
+    np.testing.assert_array_equal(back.accept, r.accept)
+    assert back.ndim == 7 and back.wall_time == 1.5 and back.message == "ok"
