@@ -104,6 +104,31 @@ class SersicTable:
             return np.zeros(self.n_radii)
         return np.array([float(sp(sersic, rhalf, dy=1)[0, 0]) for sp in self.splines])
 
+    def amplitudes_many(self, sersic, rhalf):
+        """(amplitudes, d/dsersic, d/drh), each (n, n_radii), for arrays of
+        sources: the values ``amplitudes`` / ``damplitude_dsersic`` /
+        ``damplitude_drh`` give one source at a time (the splines are
+        evaluated at all points in one call each, with identical results),
+        with the same branches for sersic below the grid and rh < 0."""
+        n = np.atleast_1d(np.asarray(sersic, dtype=np.float64))
+        r = np.atleast_1d(np.asarray(rhalf, dtype=np.float64))
+        m = len(n)
+        amp = np.zeros((m, self.n_radii))
+        dn = np.zeros((m, self.n_radii))
+        dr = np.zeros((m, self.n_radii))
+        low = n < self.sersic_range[0]
+        neg = ~low & (r < 0)
+        ok = ~low & ~neg
+        if ok.any():
+            for i, sp in enumerate(self.splines):
+                amp[ok, i] = sp(n[ok], r[ok], grid=False)
+                dn[ok, i] = sp(n[ok], r[ok], dx=1, grid=False)
+                dr[ok, i] = sp(n[ok], r[ok], dy=1, grid=False)
+        for j in np.flatnonzero(low):
+            amp[j, np.argmin(np.abs(r[j] - self.radii))] = 1.0
+        amp[neg, 0] = 1.0
+        return amp, dn, dr
+
     def knots_and_coeffs(self):
         """(tx, ty, coeffs[n_radii, len(tx)-4, len(ty)-4]) of the bicubic
         splines; all radii share the knot vectors."""
@@ -138,14 +163,13 @@ def proposal_from_params(params, n_bands, table=None):
     params = np.asarray(params, dtype=np.float64).reshape(-1, n_bands + 6)
     out = np.zeros(len(params), dtype=source_struct_dtype)
     nr = table.n_radii
-    for i, p in enumerate(params):
-        out["fluxes"][i, :n_bands] = p[:n_bands]
-        ra, dec, q, pa, n, rh = p[n_bands:]
-        out["ra"][i], out["dec"][i], out["q"][i], out["pa"][i] = ra, dec, q, pa
-        out["nsersic"][i], out["rh"][i] = n, rh
-        out["mixture_amplitudes"][i, :nr] = table.amplitudes(n, rh)
-        out["damplitude_drh"][i, :nr] = table.damplitude_drh(n, rh)
-        out["damplitude_dnsersic"][i, :nr] = table.damplitude_dsersic(n, rh)
+    out["fluxes"][:, :n_bands] = params[:, :n_bands]
+    for k, name in enumerate(["ra", "dec", "q", "pa", "nsersic", "rh"]):
+        out[name] = params[:, n_bands + k]
+    amp, dn, dr = table.amplitudes_many(params[:, n_bands + 4], params[:, n_bands + 5])
+    out["mixture_amplitudes"][:, :nr] = amp
+    out["damplitude_drh"][:, :nr] = dr
+    out["damplitude_dnsersic"][:, :nr] = dn
     return out
 
 
