@@ -342,21 +342,26 @@ def batched_leg(args, torch, lib, steps):
     from forcepho_b200.model import FastPosterior
     from forcepho_b200.proposal import GPUProposer
     from forcepho_b200.sources import Scene
-    fps = [FastPosterior(GPUProposer(), P, scene=Scene(P.n_sources, P.n_bands, P.table),
-                         lower=lo, upper=hi) for P, lo, hi in zip(patches, lows, highs)]
-    zs = [f.transform.inverse_transform(P.params.reshape(-1)) for f, P in zip(fps, patches)]
-    rng = np.random.default_rng(7)
+    def dropin_ms(per_source):
+        fps = [FastPosterior(GPUProposer(), P,
+                             scene=Scene(P.n_sources, P.n_bands, P.table, per_source=per_source),
+                             lower=lo, upper=hi) for P, lo, hi in zip(patches, lows, highs)]
+        zs = [f.transform.inverse_transform(P.params.reshape(-1)) for f, P in zip(fps, patches)]
+        rng = np.random.default_rng(7)
 
-    def dropin():
-        for f, z in zip(fps, zs):
-            f.lnprob_and_grad(z + 1e-6 * rng.standard_normal(z.shape))
+        def dropin():
+            for f, z in zip(fps, zs):
+                f.lnprob_and_grad(z + 1e-6 * rng.standard_normal(z.shape))
 
-    dropin()
-    reps = 2
-    t0 = time.perf_counter()
-    for _ in range(reps):
         dropin()
-    ms_dropin = (time.perf_counter() - t0) / reps * 1e3
+        reps = 2
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            dropin()
+        return (time.perf_counter() - t0) / reps * 1e3
+
+    ms_dropin = dropin_ms(None)
+    ms_dropin_ps = dropin_ms(True)
     out.update({
         "batched_leapfrog_ms_per_step": ms_leap,
         "batched_leapfrog_patch_evals_per_s": n / (ms_leap * 1e-3),
@@ -364,7 +369,12 @@ def batched_leg(args, torch, lib, steps):
         "dropin_patch_evals_per_s": n / (ms_dropin * 1e-3),
         "speedup_batched_differentiable_vs_dropin": ms_dropin / ms_leap,
         "dropin": "FastPosterior.lnprob_and_grad per patch: host Scene proposal (scipy "
-                  "splines), GPUProposer.evaluate_proposal with host I/O; host wall clock",
+                  "splines, all sources per call), GPUProposer.evaluate_proposal with host "
+                  "I/O; host wall clock",
+        "dropin_per_source_ms_per_step": ms_dropin_ps,
+        "speedup_batched_differentiable_vs_dropin_per_source": ms_dropin_ps / ms_leap,
+        "dropin_per_source": "the same with the proposal built one source at a time, as the "
+                             "reference's Galaxy.proposal does",
     })
     del lf
     batch.free()
@@ -636,16 +646,21 @@ def differentiable_leg(args, torch, P, cfg, steps):
     h1 = float(lf50.hamiltonian())
     err = post.ev.error_word()
 
-    fp = FastPosterior(GPUProposer(), P, scene=Scene(P.n_sources, P.n_bands, P.table),
-                       lower=lo, upper=hi)
-    z = fp.transform.inverse_transform(P.params.reshape(-1))
-    rng = np.random.default_rng(3)
-    fp.lnprob_and_grad(z)
-    n = 20
-    t0 = time.perf_counter()
-    for _ in range(n):
-        fp.lnprob_and_grad(z + 1e-6 * rng.standard_normal(z.shape))
-    ms_dropin = (time.perf_counter() - t0) / n * 1e3
+    def dropin_ms(per_source):
+        fp = FastPosterior(GPUProposer(), P,
+                           scene=Scene(P.n_sources, P.n_bands, P.table, per_source=per_source),
+                           lower=lo, upper=hi)
+        z = fp.transform.inverse_transform(P.params.reshape(-1))
+        rng = np.random.default_rng(3)
+        fp.lnprob_and_grad(z)
+        n = 20
+        t0 = time.perf_counter()
+        for _ in range(n):
+            fp.lnprob_and_grad(z + 1e-6 * rng.standard_normal(z.shape))
+        return (time.perf_counter() - t0) / n * 1e3
+
+    ms_dropin = dropin_ms(None)
+    ms_dropin_ps = dropin_ms(True)
     out = {"workload": "field20 differentiable: 20-source patch, 280 parameters, leapfrog eps 1e-3 in "
                        "unconstrained coordinates",
            "graph_step_ms": ms_step, "graph_evals_per_s": 1e3 / ms_step,
@@ -653,6 +668,10 @@ def differentiable_leg(args, torch, P, cfg, steps):
            "trajectory_dH": h1 - h0, "error_word": err,
            "dropin_ms_per_eval": ms_dropin, "dropin_evals_per_s": 1e3 / ms_dropin,
            "speedup_vs_dropin": ms_dropin / ms_step,
+           "dropin_per_source_ms_per_eval": ms_dropin_ps,
+           "speedup_vs_dropin_per_source": ms_dropin_ps / ms_step,
+           "dropin_per_source": "the same with the proposal built one source at a time, as "
+                                "the reference's Galaxy.proposal does",
            "timing": "graph step: CUDA events per replay, L2 flushed between steps; "
                      "trajectory: CUDA events around 10 replays of 50 steps (L2 warm); "
                      "drop-in: host wall clock per FastPosterior.lnprob_and_grad"}

@@ -155,10 +155,13 @@ def default_table():
     return _default_table
 
 
-def proposal_from_params(params, n_bands, table=None):
+def proposal_from_params(params, n_bands, table=None, per_source=None):
     """Pack parameters of shape (n_sources, n_bands + 6), in Scene order, into
     a ``source_struct_dtype`` array (as ``Galaxy.proposal``,
-    forcepho/sources.py:607-621)."""
+    forcepho/sources.py:607-621).  The amplitude splines are evaluated for all
+    sources in one call per radius, or, with `per_source` (the default for one
+    or two sources, where it is faster), one source at a time as the
+    reference does; the bytes are the same either way."""
     table = table or default_table()
     params = np.asarray(params, dtype=np.float64).reshape(-1, n_bands + 6)
     out = np.zeros(len(params), dtype=source_struct_dtype)
@@ -166,6 +169,15 @@ def proposal_from_params(params, n_bands, table=None):
     out["fluxes"][:, :n_bands] = params[:, :n_bands]
     for k, name in enumerate(["ra", "dec", "q", "pa", "nsersic", "rh"]):
         out[name] = params[:, n_bands + k]
+    if per_source is None:
+        per_source = len(params) <= 2
+    if per_source:
+        for i, p in enumerate(params):
+            n, rh = p[n_bands + 4], p[n_bands + 5]
+            out["mixture_amplitudes"][i, :nr] = table.amplitudes(n, rh)
+            out["damplitude_drh"][i, :nr] = table.damplitude_drh(n, rh)
+            out["damplitude_dnsersic"][i, :nr] = table.damplitude_dsersic(n, rh)
+        return out
     amp, dn, dr = table.amplitudes_many(params[:, n_bands + 4], params[:, n_bands + 5])
     out["mixture_amplitudes"][:, :nr] = amp
     out["damplitude_drh"][:, :nr] = dr
@@ -179,9 +191,10 @@ class Scene:
     ``get_all_source_params``, ``get_proposal``), for ``n_sources`` Sersic
     galaxies of ``n_bands`` fluxes each, in Scene order."""
 
-    def __init__(self, n_sources, n_bands, table=None, params=None):
+    def __init__(self, n_sources, n_bands, table=None, params=None, per_source=None):
         self.n_sources, self.n_bands = int(n_sources), int(n_bands)
         self.table = table or default_table()
+        self.per_source = per_source       # see proposal_from_params
         self.n_params_per_source = self.n_bands + 6
         self.params = np.zeros((self.n_sources, self.n_params_per_source))
         if params is not None:
@@ -197,4 +210,5 @@ class Scene:
         return self.params.reshape(-1).copy()
 
     def get_proposal(self, active=True):
-        return proposal_from_params(self.params, self.n_bands, self.table)
+        return proposal_from_params(self.params, self.n_bands, self.table,
+                                    per_source=self.per_source)
