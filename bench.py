@@ -45,14 +45,14 @@ METRIC = "chi2+grad evals/s & pixÂ·gauss/s: batched vs plain, 1 B200, rel err â‰
 FLOPS_PER_PAIR = 105          # 18 (model) + 87 (gradient) FP32 flops, FMA = 2
 WORKLOAD = "field20: 20 src, 8 bands x 4 exp x 128x128 px, 5-gauss PSF, 9 radii"
 # DRAM bytes (read + write) of one tile-kernel launch on this workload, from an
-# ncu capture (profiles/tile_kernel_dyn_64x4_field20.md): the 16 B per pixel
-# of the pixel arrays plus the image-Gaussian table, each read once.
+# ncu capture of one launch: the 16 B per pixel of the pixel arrays plus the
+# image-Gaussian table, each read once.
 TILE_TRAFFIC_BYTES = 12673536
 # DRAM bytes of one store_copy launch packing a 471 k-pixel patch (ncu:
-# throughput x duration, profiles/store_kernels_packing32.md).
+# throughput x duration of one launch).
 STORE_COPY_TRAFFIC_BYTES = 3833600
 # ... and of the one store_copy launch packing the 32 patches of the packing
-# leg together (15.07 M pixels; same file).
+# leg together (15.07 M pixels; same capture method).
 STORE_COPY_BATCH_TRAFFIC_BYTES = 261868000
 
 
@@ -190,6 +190,12 @@ def _cpu_model():
     return None
 
 
+def workload_config(P):
+    """The `config` of the JSON line, identical in both arms (run details of
+    this implementation go under `run_config`)."""
+    return {"workload": WORKLOAD, "pairs_per_eval": int(P.pairs_per_eval)}
+
+
 def make_workload(seed, device_render):
     from forcepho_b200 import synth
     render = synth.render_model_gpu if device_render else None
@@ -212,7 +218,7 @@ def run_reference(args):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": sec * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": WORKLOAD, "pairs_per_eval": P.pairs_per_eval},
+        "config": workload_config(P),
         "pix_gauss_per_s": P.pairs_per_eval * value,
         "cpu_baseline": {"value": value, "unit": "evals/s", "cores": min(cores, P.n_bands),
                          "kind": "reference",
@@ -308,6 +314,23 @@ def batched_leg(args, torch, lib, steps):
         plain()
     ms_plain = timed(plain, max(3, steps // 4))
     n = len(patches)
+
+    # after the timed runs: the batch's outputs (one more graph replay) against
+    # the per-patch evaluations the plain loop left in its buffers
+    graph.replay()
+    torch.cuda.synchronize()
+    bc, bg = batch.split_outputs(chi2.cpu().numpy(), dchi2.cpu().numpy())
+    chi2_rel, grad_rel = 0.0, 0.0
+    for (h, q, c, g, ns), c_b, g_b in zip(bufs, bc, bg):
+        c_p = c.cpu().numpy()
+        g_p = g.cpu().numpy().reshape(g_b.shape)
+        chi2_rel = max(chi2_rel, float(np.max(np.abs(c_b - c_p) / np.abs(c_p))))
+        grad_rel = max(grad_rel, float(np.max(np.abs(g_b - g_p)) / max(np.abs(g_p).max(), 1e-30)))
+    batch_err = batch.error_word()
+    if not (chi2_rel <= 1e-6 and grad_rel <= 1e-5 and batch_err == 0):
+        raise RuntimeError(f"batched evaluation differs from the per-patch one: chi2 rel "
+                           f"{chi2_rel:.3g}, gradient {grad_rel:.3g} of its largest component, "
+                           f"error word {batch_err}")
     out = {"workload": f"uneven: {n} patches, sources U{{1..30}}, bands U{{1..8}}, "
                        "exposures/band U{1..8}, side U[32,200] px",
            "patches": n, "nominal_pairs_per_step": nominal, "evaluated_pairs_per_step": evaluated,
@@ -321,7 +344,12 @@ def batched_leg(args, torch, lib, steps):
                         "achieved": evaluated * FLOPS_PER_PAIR / (tile_ms * 1e-3) / 1e12,
                         "unit": "TFLOP/s"},
            "timing": "CUDA events per step, L2 flushed between steps; batched step replayed "
-                     "from a CUDA graph"}
+                     "from a CUDA graph",
+           "check_vs_per_patch": {"chi2_max_rel": chi2_rel, "grad_max_rel_of_patch_max": grad_rel,
+                                  "what": "after the timed replays: every patch's chi2 and "
+                                          "gradient from the batch against its own "
+                                          "fpho_evaluate_proposal (asserted: chi2 <= 1e-6, "
+                                          "gradient <= 1e-5 of the patch's largest component)"}}
     del graph
 
     # the batched differentiable form: device-side proposals (splines) and
@@ -589,8 +617,7 @@ def packing_leg(args, torch, n_patches):
                          "peak_source": peak_src,
                          "traffic": STORE_COPY_BATCH_TRAFFIC_BYTES if n_patches == 32 else None,
                          "traffic_source": "ncu DRAM bytes (throughput x duration) of the "
-                                           "32-patch store_copy launch, "
-                                           "profiles/store_kernels_packing32.md; part of the "
+                                           "32-patch store_copy launch; part of the "
                                            "written output is still in L2 at its end"},
             "single_patch_roofline": {
                 "kernel": "store_compact + store_copy", "kernel_ms": g_ms,
@@ -827,11 +854,11 @@ def run_ours(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic",
-            "config": {"workload": WORKLOAD, "pairs_per_eval": P.pairs_per_eval,
-                       "evaluated_pairs": evaluated_pairs, "l2": "flushed between steps",
-                       "tile_variant": list(_lib.variants()[cfg["variant"]]),
-                       "live_cap": cfg["live_cap"], "schedule": cfg.get("schedule", 0),
-                       "parallelism": f"patch-parallel x{world}"},
+            "config": workload_config(P),
+            "run_config": {"evaluated_pairs": evaluated_pairs, "l2": "flushed between steps",
+                           "tile_variant": list(_lib.variants()[cfg["variant"]]),
+                           "live_cap": cfg["live_cap"], "schedule": cfg.get("schedule", 0),
+                           "parallelism": f"patch-parallel x{world}"},
             "pix_gauss_per_s": P.pairs_per_eval * value,
             "evaluated_pix_gauss_per_s": evaluated_pairs * value,
             "e2e": {"value": e2e_value, "unit": "evals/s",
@@ -842,7 +869,7 @@ def run_ours(args):
                          "unit": "TFLOP/s", "frac": achieved / fp32_tflops,
                          "traffic": TILE_TRAFFIC_BYTES,
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum "
-                                           "of one launch, profiles/tile_kernel_dyn_64x4_field20.md",
+                                           "of one launch",
                          "peak_source": "measured live: packed FP32 FMA probe kernel",
                          "kernel": "tile_kernel", "kernel_ms": tile_s * 1e3,
                          "sfu_gops": sfu, "sfu_peak_gops": ex2_gops, "sfu_frac": sfu / ex2_gops},

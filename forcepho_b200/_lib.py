@@ -1,9 +1,12 @@
 """ctypes binding of ``libfpho.so`` (the C ABI declared in include/fpho.h).
 
-The library is built in-tree by :mod:`forcepho_b200.build`.  Importing this
-module loads it; if it is missing it is compiled (nvcc is present wherever the
-package is built), and if that is impossible the import fails loudly: there is
-no CPU fallback for the hot path.
+The library is built in-tree by :mod:`forcepho_b200.build`.  It is loaded on
+first use (the first access to ``lib`` or the first call through this
+module), so that code which only needs the package's host-side pieces -- the
+synthetic patches, the packing and the file readers -- does not map it.  If
+it is missing it is compiled (nvcc is present wherever the package is built),
+and if that is impossible the first use fails loudly: there is no CPU
+fallback for the hot path.
 """
 
 import ctypes
@@ -37,9 +40,6 @@ def _load():
         raise ImportError(f"forcepho_b200: CUDA library {path} is missing and could not be built")
     return ctypes.CDLL(path)
 
-
-lib = _load()
-
 c_void_p = ctypes.c_void_p
 c_int = ctypes.c_int
 c_uint = ctypes.c_uint
@@ -71,6 +71,7 @@ _SIGS = {
     "fpho_store_last_gather_ms": (c_int, [c_void_p, ctypes.POINTER(ctypes.c_float)]),
     "fpho_patch_set_config": (c_int, [c_void_p, c_int, c_int, c_void_p]),
     "fpho_patch_set_schedule": (c_int, [c_void_p, c_int]),
+    "fpho_patch_set_exact_residual": (c_int, [c_void_p, c_int]),
     "fpho_patch_set_test_stall": (c_int, [c_void_p, c_int]),
     "fpho_patch_design_matrix": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p]),
     "fpho_variant_info": (c_int, [c_int, ctypes.POINTER(c_int)]),
@@ -106,11 +107,11 @@ _SIGS = {
 }
 
 
-def _bind():
+def _bind(L):
     missing = []
     for name, (res, args) in _SIGS.items():
         try:
-            f = getattr(lib, name)
+            f = getattr(L, name)
         except AttributeError:
             missing.append(name)
             continue
@@ -120,11 +121,28 @@ def _bind():
         raise ImportError(f"libfpho.so lacks symbols: {missing}")
 
 
-_bind()
+_loaded = None
+
+
+def get():
+    """The loaded and bound library (loads it on the first call)."""
+    global _loaded
+    if _loaded is None:
+        L = _load()
+        _bind(L)
+        _loaded = L
+        globals()["lib"] = L
+    return _loaded
+
+
+def __getattr__(name):
+    if name == "lib":
+        return get()
+    raise AttributeError(f"module {__name__!r} has no attribute {name!r}")
 
 
 def last_error():
-    return lib.fpho_last_error().decode(errors="replace")
+    return get().fpho_last_error().decode(errors="replace")
 
 
 def check(rc, func="fpho"):
@@ -135,16 +153,17 @@ def check(rc, func="fpho"):
 
 def call(name, *args):
     """Call a C-ABI function and raise FphoError on a non-zero status."""
-    return check(getattr(lib, name)(*args), name)
+    return check(getattr(get(), name)(*args), name)
 
 
 def variants():
     """List of (threads per CTA, pixels per thread) of the compiled tile kernels."""
     out = (c_int * 2)()
-    n = lib.fpho_variant_info(0, out)
+    L = get()
+    n = L.fpho_variant_info(0, out)
     res = []
     for v in range(n):
-        lib.fpho_variant_info(v, out)
+        L.fpho_variant_info(v, out)
         res.append((out[0], out[1]))
     return res
 
