@@ -297,6 +297,52 @@ int fpo_evaluate_band_f32(int band, const fpo_patch *P, const fpo_source *S,
     return 0;
 }
 
+/* The reference's own float per-pixel gradient contributions, summed exactly.
+ * Identical to fpo_evaluate_band_f32 (float image Gaussians, float residual,
+ * float per-pixel and per-source terms dp[] in the reference's operation
+ * order), except that the per-pixel terms are accumulated into double
+ * dchi2[n_sources*7] instead of the reference's running float sums
+ * (compute_gaussians_kernel.cc:300-305).  The difference between the
+ * reference's result and this one is therefore exactly the rounding of the
+ * reference's sequential float accumulation over the band's pixels. */
+int fpo_evaluate_band_f32_dsum(int band, const fpo_patch *P, const fpo_source *S,
+                               double *chi2_out, double *dchi2) {
+    int nsrc = P->n_sources;
+    int npsf = P->n_psf_per_source[band];
+    int bN = P->band_N[band], b0 = P->band_start[band];
+    int ntot = nsrc * npsf;
+    fpo_imgauss *ig = (fpo_imgauss *)malloc(sizeof(fpo_imgauss) * (size_t)(ntot > 0 ? ntot : 1));
+    if (!ig) return -1;
+    for (int i = 0; i < nsrc * FPO_NPARAMS; i++) dchi2[i] = 0.0;
+    double chi2 = 0.0;
+    float dp[FPO_NPARAMS];
+    for (int ee = 0; ee < bN; ee++) {
+        int e = b0 + ee;
+        int npix = P->exposure_N[e];
+        for (int g = 0; g < nsrc; g++) convolve_source_f32(band, e, g, npsf, P, S, ig);
+        for (int p = 0; p < npix; p++) {
+            int pix = P->exposure_start[e] + p;
+            float xp = P->xpix[pix], yp = P->ypix[pix];
+            float data = P->data[pix], ierr = P->ierr[pix];
+            float r = residual_f32(xp, yp, data, ig, ntot);
+            r *= ierr;
+            data *= ierr;
+            double c2 = ((double)r - (double)data);
+            c2 *= ((double)r + (double)data);
+            chi2 += c2;
+            r *= ierr;
+            for (int gal = 0; gal < nsrc; gal++) {
+                for (int j = 0; j < FPO_NPARAMS; j++) dp[j] = 0.0f;
+                derivative_f32(xp, yp, r, ig + gal * npsf, dp, npsf);
+                for (int j = 0; j < FPO_NPARAMS; j++) dchi2[gal * FPO_NPARAMS + j] += (double)dp[j];
+            }
+        }
+    }
+    free(ig);
+    *chi2_out = chi2;
+    return 0;
+}
+
 /* Image Gaussians of one exposure in float, exactly as the reference builds
  * them (21 floats per Gaussian, source-major, PSF-minor). */
 int fpo_image_gaussians_f32(int band, int e, const fpo_patch *P, const fpo_source *S,

@@ -27,10 +27,12 @@ REF_DIR = os.path.join(HERE, "_ref")
 
 
 def build(ref=None):
-    """make -C oracle (and the reference build when its sources are present)."""
+    """make -C oracle, and the reference build when a reference checkout is
+    given (`ref`, else the FPHO_REFERENCE environment variable) and holds
+    its sources."""
     subprocess.run(["make", "-s", "-C", HERE, "all", f"PY={sys.executable}"], check=True)
-    src = ref if ref is not None else "/root/reference"
-    if os.path.isdir(os.path.join(src, "forcepho", "src")):
+    src = ref if ref is not None else os.environ.get("FPHO_REFERENCE", "")
+    if src and os.path.isdir(os.path.join(src, "forcepho", "src")):
         subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={src}", f"PY={sys.executable}"],
                        check=True)
 
@@ -94,6 +96,103 @@ def oracle_evaluate(patch, proposal, precision="f32", cutoff=True, residual=Fals
         dchi2[b] = g.reshape(ns, 7)
     if residual:
         return chi2, dchi2, res
+    return chi2, dchi2
+
+
+def oracle_f32_dsum(patch, proposal):
+    """chi2 (n_bands,) and dchi2 (n_bands, n_src, 7) float64: the reference
+    CPU kernel's own float per-pixel gradient terms (bit-identical to its
+    arithmetic) accumulated in double instead of its running float sums
+    (see fpo_evaluate_band_f32_dsum)."""
+    L = lib()
+    if not hasattr(L, "_dsum_bound"):
+        vp, ip = ctypes.c_void_p, ctypes.c_int
+        L.fpo_evaluate_band_f32_dsum.argtypes = [ip, vp, vp, vp, vp]
+        L.fpo_evaluate_band_f32_dsum.restype = ip
+        L._dsum_bound = True
+    st = patch.host_struct()
+    prop = np.ascontiguousarray(proposal)
+    nb, ns = patch.n_bands, patch.n_sources
+    chi2 = np.zeros(nb)
+    dchi2 = np.zeros((nb, ns, 7))
+    for b in range(nb):
+        c = ctypes.c_double(0.0)
+        g = np.zeros(ns * 7)
+        if L.fpo_evaluate_band_f32_dsum(b, st.ctypes.data, prop.ctypes.data, ctypes.byref(c),
+                                        g.ctypes.data) != 0:
+            raise MemoryError("oracle allocation failed")
+        chi2[b], dchi2[b] = c.value, g.reshape(ns, 7)
+    return chi2, dchi2
+
+
+def _worker_f32_dsum(payload, proposal, band):
+    """(band, chi2, dchi2 (n_src, 7)) of oracle_f32_dsum for one band, in a
+    worker process."""
+    L = lib()
+    vp, ip = ctypes.c_void_p, ctypes.c_int
+    L.fpo_evaluate_band_f32_dsum.argtypes = [ip, vp, vp, vp, vp]
+    L.fpo_evaluate_band_f32_dsum.restype = ip
+    arrays, ns, nr = _resolve(payload)
+    st = _struct_from_arrays(arrays, ns, nr)
+    prop = np.ascontiguousarray(proposal)
+    c = ctypes.c_double(0.0)
+    g = np.zeros(ns * 7)
+    if L.fpo_evaluate_band_f32_dsum(band, st.ctypes.data, prop.ctypes.data, ctypes.byref(c),
+                                    g.ctypes.data) != 0:
+        raise MemoryError("oracle allocation failed")
+    return band, c.value, g.reshape(ns, 7)
+
+
+def _worker_f32_res(payload, proposal, band):
+    """(band, chi2, dchi2 (n_src, 7) float32, first pixel, residual of the
+    band's pixels) of the f32 oracle (the reference kernel restated) for one
+    band, in a worker process."""
+    L = lib()
+    arrays, ns, nr = _resolve(payload)
+    st = _struct_from_arrays(arrays, ns, nr)
+    prop = np.ascontiguousarray(proposal)
+    e0 = int(arrays["band_start"][band])
+    e1 = e0 + int(arrays["band_N"][band])
+    lo = int(arrays["exposure_start"][e0])
+    hi = int(arrays["exposure_start"][e1 - 1] + arrays["exposure_N"][e1 - 1])
+    res = np.zeros(hi, dtype=np.float32)
+    c = ctypes.c_double(0.0)
+    g = np.zeros(ns * 7, dtype=np.float32)
+    if L.fpo_evaluate_band_f32(band, st.ctypes.data, prop.ctypes.data, ctypes.byref(c),
+                               g.ctypes.data, res.ctypes.data) != 0:
+        raise MemoryError("oracle allocation failed")
+    return band, c.value, g.reshape(ns, 7), lo, res[lo:hi].copy()
+
+
+def f32_residual_many(patch, proposal, pool, bands=None, payload=None):
+    """The f32 oracle (bit-identical to the reference CPU kernel) with its
+    residual image, bands spread over `pool`: chi2 (n_bands,), dchi2
+    (n_bands, n_src, 7) float32, residual (npix,) float32 (NaN outside the
+    bands evaluated)."""
+    payload = payload or _patch_payload(patch)
+    nb, ns = patch.n_bands, patch.n_sources
+    bands = range(nb) if bands is None else bands
+    chi2 = np.full(nb, np.nan)
+    dchi2 = np.full((nb, ns, 7), np.nan, dtype=np.float32)
+    res = np.full(patch.npix, np.nan, dtype=np.float32)
+    prop = np.ascontiguousarray(proposal)
+    for b, c, g, lo, r in pool.starmap(_worker_f32_res, [(payload, prop, b) for b in bands]):
+        chi2[b], dchi2[b] = c, g
+        res[lo:lo + len(r)] = r
+    return chi2, dchi2, res
+
+
+def f32_dsum_many(patch, proposal, pool, bands=None, payload=None):
+    """oracle_f32_dsum with the bands spread over `pool` (see oracle_pool);
+    bands not in `bands` are left zero."""
+    payload = payload or _patch_payload(patch)
+    nb, ns = patch.n_bands, patch.n_sources
+    bands = range(nb) if bands is None else bands
+    chi2 = np.zeros(nb)
+    dchi2 = np.zeros((nb, ns, 7))
+    prop = np.ascontiguousarray(proposal)
+    for b, c, g in pool.starmap(_worker_f32_dsum, [(payload, prop, b) for b in bands]):
+        chi2[b], dchi2[b] = c, g
     return chi2, dchi2
 
 

@@ -1,9 +1,9 @@
 """Generate the golden vectors in tests/golden/*.npz.
 
-Run in a checkout that has the reference at /root/reference (or pass its path
-with --ref) after ``make -C oracle all ref``:
+Run with the reference checkout named by --ref (or the FPHO_REFERENCE
+environment variable) after ``make -C oracle all ref``:
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py --ref <reference checkout>
 
 For each small seeded synthetic patch (forcepho_b200.synth) it stores the
 packed patch arrays, the packed proposal and
@@ -121,8 +121,10 @@ def cases():
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("FPHO_REFERENCE"))
     a = ap.parse_args()
+    if not a.ref:
+        ap.error("name the reference checkout with --ref or FPHO_REFERENCE")
     O.build(ref=a.ref)
     gm = import_slow(a.ref)
     for name, P in cases():

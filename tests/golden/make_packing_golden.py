@@ -150,4 +150,7 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("FPHO_REFERENCE")
+    if not ref:
+        sys.exit("usage: make_packing_golden.py <reference checkout> (or set FPHO_REFERENCE)")
+    main(ref)

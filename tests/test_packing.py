@@ -20,7 +20,8 @@ import numpy as np
 import pytest
 
 GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
-REF_DATA = "/root/reference/tests/data"
+# the reference checkout's test data, when FPHO_REFERENCE names a checkout
+REF_DATA = os.path.join(os.environ.get("FPHO_REFERENCE", "/nonexistent"), "tests", "data")
 
 
 def _digest(a):
