@@ -5,24 +5,30 @@
 // keeps all of its scratch (tile plan, image-Gaussian records and culling
 // boxes, per-tile partial sums) in one file-scope device array of
 // FPHO_NOALLOC_SCRATCH_BYTES.  It is meant for callers that cannot call
-// cudaMalloc: code that runs while a CUDA graph is being captured, plugins
-// whose host framework owns every device allocation, and long-running services
-// that must not grow or fragment device memory after start-up.
+// cudaMalloc: plugins whose host framework owns every device allocation (its
+// allocator alone may take device memory, so that its accounting and limits
+// hold), and long-running services that must not grow or fragment device
+// memory after start-up.
 //
 // Semantics a caller must know:
 //   * The array exists once per device, in every process that loads the
 //     library, until the process exits (FPHO_NOALLOC_SCRATCH_BYTES of device
 //     memory per device used).
 //   * The first call on a device looks up the array's device address
-//     (cudaGetSymbolAddress) and sets the tile kernel's shared-memory limit;
-//     make that first call before any stream capture.
+//     (cudaGetSymbolAddress) and raises the tile kernel's shared-memory limit
+//     to the device's ceiling, so that no later call changes a kernel
+//     attribute; make that first call before any stream capture.  The address
+//     is kept for the life of the process: a device reset
+//     (cudaDeviceReset, or a reset of the primary context) is not supported.
 //   * Every call shares the array and it keeps the last call's contents; each
 //     call rebuilds what it needs (the plan and the error word are written by
 //     the first kernel of the call).  Calls whose kernels overlap on the GPU
 //     (on different streams, or from different threads) race on the array and
 //     give wrong results: serialize them.
 //   * The patch arrays are not validated on the host (they are device memory);
-//     index inconsistencies found on the device are reported in *dev_status.
+//     index inconsistencies found on the device are reported in *dev_status,
+//     and any error makes every dev_chi2 entry NaN, so that a failed call
+//     never looks like a result, whether or not dev_status is given.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -90,9 +96,14 @@ Layout make_layout(int n_bands, int n_exp, long long n_tiles_max, long long n_ga
 
 // One thread builds the plan: band of each exposure, image-Gaussian offsets,
 // tile list.  Clears the error word first.
+// Every exposure's pixel run [exposure_start, exposure_start + exposure_N) must
+// lie inside the caller's pixel arrays of total_pixels entries, and every
+// exposure with PSF components needs psfgauss_start >= 0; otherwise the plan
+// is empty and NA_ERR_INDEX is set, before any pixel is read.
 __global__ void noalloc_plan(const int16_t *band_start, const int16_t *band_N,
                              const int *exposure_start, const int *exposure_N,
-                             const int *n_psf_per_source, int n_bands, int n_exp, int nsrc,
+                             const int *n_psf_per_source, const int *psfgauss_start,
+                             long long total_pixels, int n_bands, int n_exp, int nsrc,
                              int max_npsf, int n_tiles_max, int n_gauss_max, Header *hdr,
                              int *exp_band, int *exp_npsf, int *gauss_start,
                              int *tile_band_start, TileDesc *tiles) {
@@ -118,6 +129,7 @@ __global__ void noalloc_plan(const int16_t *band_start, const int16_t *band_N,
             err |= NA_ERR_BOUND;
             npsf = 0;
         }
+        if (npsf > 0 && psfgauss_start[e] < 0) err |= NA_ERR_INDEX;
         exp_npsf[e] = npsf;
         gauss_start[e] = (int)(acc < n_gauss_max ? acc : n_gauss_max);
         acc += (long long)nsrc * npsf;
@@ -131,7 +143,7 @@ __global__ void noalloc_plan(const int16_t *band_start, const int16_t *band_N,
         if (s < 0 || n < 0 || s + n > n_exp) continue;
         for (int e = s; e < s + n; ++e) {
             const int N = exposure_N[e], p0 = exposure_start[e];
-            if (N < 0 || p0 < 0) {
+            if (N < 0 || p0 < 0 || (long long)p0 + N > total_pixels) {
                 err |= NA_ERR_INDEX;
                 continue;
             }
@@ -197,13 +209,20 @@ __global__ void __launch_bounds__(NA_THREADS) noalloc_tiles(TileArgs A, const He
     tile_body<NA_THREADS, NA_K>(A, blockIdx.x, smem, &mbar, phase);
 }
 
-__global__ void noalloc_finish(const Header *hdr, int *dev_status) {
-    if (threadIdx.x == 0 && blockIdx.x == 0) *dev_status = hdr->err;
+// Last kernel of a call: the status word, and NaN in every chi2 entry when
+// any kernel of the call reported an error (a plan that failed leaves the
+// band sums at zero, which would otherwise read as a valid chi2).
+__global__ void noalloc_finish(const Header *hdr, int *dev_status, double *chi2, int n_bands) {
+    const int err = hdr->err;
+    if (threadIdx.x == 0 && dev_status) *dev_status = err;
+    if (err)
+        for (int b = threadIdx.x; b < n_bands; b += blockDim.x)
+            chi2[b] = __longlong_as_double(0x7ff8000000000000ll);  // quiet NaN
 }
 
 std::mutex g_setup_mu;
-void *g_scratch_ptr[64];
-size_t g_smem_set[64];
+void *g_scratch_ptr[64];  // device address of the scratch array, per device
+int g_max_dyn_smem[64];   // dynamic shared memory the tile kernel was allowed, per device
 
 }  // namespace
 }  // namespace fpho
@@ -260,7 +279,8 @@ extern "C" int fpho_evaluate_proposal_noalloc(const fpho_patch_struct *patch, in
                          "exceeds 227 KB", smem, idx_cap);
 
     // once per device (the device current for this call): the array's device
-    // address and the tile kernel's dynamic shared-memory limit
+    // address, and the tile kernel's dynamic shared-memory limit raised to the
+    // device's ceiling at once, so that later calls never touch kernel attributes
     int dev = 0;
     cudaError_t ce = cudaGetDevice(&dev);
     if (ce != cudaSuccess) return set_error(FPHO_ERR_CUDA, "cudaGetDevice: %s", cudaGetErrorString(ce));
@@ -269,6 +289,20 @@ extern "C" int fpho_evaluate_proposal_noalloc(const fpho_patch_struct *patch, in
     {
         std::lock_guard<std::mutex> lk(g_setup_mu);
         if (!g_scratch_ptr[dev]) {
+            // the ceiling: the device's opt-in shared memory per block less
+            // the kernel's static shared memory
+            int optin = 0;
+            cudaFuncAttributes fa;
+            ce = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+            if (ce == cudaSuccess) ce = cudaFuncGetAttributes(&fa, (const void *)noalloc_tiles);
+            if (ce != cudaSuccess)
+                return set_error(FPHO_ERR_CUDA, "shared-memory limits: %s", cudaGetErrorString(ce));
+            const int max_dyn = optin - (int)fa.sharedSizeBytes;
+            ce = cudaFuncSetAttribute((const void *)noalloc_tiles,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, max_dyn);
+            if (ce != cudaSuccess)
+                return set_error(FPHO_ERR_CUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(ce));
+            g_max_dyn_smem[dev] = max_dyn;
             void *ptr = nullptr;
             ce = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
             if (ce != cudaSuccess || !ptr)
@@ -276,14 +310,11 @@ extern "C" int fpho_evaluate_proposal_noalloc(const fpho_patch_struct *patch, in
                                  cudaGetErrorString(ce));
             g_scratch_ptr[dev] = ptr;
         }
-        if (g_smem_set[dev] < smem) {
-            ce = cudaFuncSetAttribute((const void *)noalloc_tiles,
-                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-            if (ce != cudaSuccess)
-                return set_error(FPHO_ERR_CUDA, "cudaFuncSetAttribute: %s", cudaGetErrorString(ce));
-            g_smem_set[dev] = smem;
-        }
         base = (unsigned char *)g_scratch_ptr[dev];
+        if (smem > (size_t)g_max_dyn_smem[dev])
+            return set_error(FPHO_ERR_LIMIT, "shared memory %zu for %d image Gaussians per "
+                             "exposure exceeds the %d bytes a block may use", smem, idx_cap,
+                             g_max_dyn_smem[dev]);
     }
     Header *hdr = (Header *)(base + L.hdr);
     int *exp_band = (int *)(base + L.exp_band);
@@ -300,7 +331,8 @@ extern "C" int fpho_evaluate_proposal_noalloc(const fpho_patch_struct *patch, in
 
     cudaStream_t s = (cudaStream_t)stream;
     noalloc_plan<<<1, 32, 0, s>>>(h.band_start, h.band_N, h.exposure_start, h.exposure_N,
-                                  h.n_psf_per_source, n_bands, n_exp, nsrc, max_psf_per_source,
+                                  h.n_psf_per_source, h.psfgauss_start, (long long)total_pixels,
+                                  n_bands, n_exp, nsrc, max_psf_per_source,
                                   (int)n_tiles_max, (int)n_gauss_max, hdr, exp_band, exp_npsf,
                                   gauss_start, tile_band_start, tiles);
     PatchView pv;
@@ -333,7 +365,7 @@ extern "C" int fpho_evaluate_proposal_noalloc(const fpho_patch_struct *patch, in
     noalloc_tiles<<<(unsigned)n_tiles_max, NA_THREADS, smem, s>>>(A, hdr);
     reduce_bands<<<dim3(n_bands, (dchi2_stride + 127) / 128), 128, 0, s>>>(
         tile_band_start, pchi2, pgrad, stride, dev_chi2, dev_dchi2, dchi2_stride);
-    if (dev_status) noalloc_finish<<<1, 1, 0, s>>>(hdr, dev_status);
+    noalloc_finish<<<1, 32, 0, s>>>(hdr, dev_status, dev_chi2, n_bands);
     ce = cudaGetLastError();
     if (ce != cudaSuccess) return set_error(FPHO_ERR_CUDA, "launch: %s", cudaGetErrorString(ce));
     return FPHO_OK;
