@@ -23,7 +23,9 @@ Printed JSON (rank 0):
              oracle/_ref) on all host cores, one evaluation of the same patch.
 Further legs on one GPU (each skippable): differentiable (LnLike + leapfrog
 in a CUDA graph), multichain (many HMC chains per launch), batched (256
-uneven patches in one persistent launch) and packing (patches packed from a
+uneven patches in one persistent launch, launch configuration from the batch
+autotuner), flux_solve (the fused linear flux solve against the design
+matrix + cuBLAS and the host path) and packing (patches packed from a
 GPU-resident exposure store against host packing of the same HDF5 store).
 The reference arm (--impl reference) times that CPU kernel over K steps.
 """
@@ -76,6 +78,8 @@ def parse():
                     help="HMC chains of the multi-chain leg (single-source patch); 0 skips it")
     ap.add_argument("--no-differentiable", action="store_true",
                     help="skip the differentiable-form leg (20-source patch)")
+    ap.add_argument("--no-flux", action="store_true",
+                    help="skip the flux-solve leg (20-source patch, fixed shapes)")
     ap.add_argument("--packing-patches", type=int, default=32,
                     help="patches packed from the exposure store in the packing leg; 0 skips it")
     return ap.parse_args()
@@ -263,7 +267,11 @@ def batched_leg(args, torch, lib, steps):
     for P in patches:
         P.return_residual = False
         P.send_to_device()
-    batch = PatchBatch(patches)
+    # the batch autotuner: tile variant, stage size and persistent-grid cap,
+    # timed on this batch (cached by the batch's signature)
+    from forcepho_b200.autotune import choose_batch_config
+    bcfg = choose_batch_config(patches)
+    batch = PatchBatch(patches, config=bcfg)
     dprop, chi2, dchi2 = batch.device_buffers()
     s = torch.cuda.current_stream()
     nominal = int(sum(P.pairs_per_eval for P in patches))
@@ -335,6 +343,8 @@ def batched_leg(args, torch, lib, steps):
                        "exposures/band U{1..8}, side U[32,200] px",
            "patches": n, "nominal_pairs_per_step": nominal, "evaluated_pairs_per_step": evaluated,
            "work_items": batch.n_work, "persistent_grid": batch.grid,
+           "batch_config": dict(batch.config,
+                                tile_shape=list(lib.variant_shapes()[batch.config["variant"]])),
            "batched_ms_per_step": ms_batched, "plain_ms_per_step": ms_plain,
            "batched_patch_evals_per_s": n / (ms_batched * 1e-3),
            "plain_patch_evals_per_s": n / (ms_plain * 1e-3),
@@ -628,6 +638,81 @@ def packing_leg(args, torch, n_patches):
                                   "kernel)"}}
 
 
+def flux_leg(args, torch, steps):
+    """The linear flux solve of the 20 sources of the 20-source patch at
+    fixed shapes (forcepho's optimize_fluxes): the fused device solve
+    (fpho_patch_optimize_fluxes: per-tile FP64 normal equations without a
+    stored design matrix, Cholesky per band) against the design matrix
+    written to HBM and the normal equations as FP64 cuBLAS products with a
+    batched solve (torch), both on device buffers and CUDA-event timed; and
+    the host path as the reference runs it (design matrix copied to the host,
+    numpy normal equations and solves), wall clock."""
+    from forcepho_b200 import _lib, synth
+    from forcepho_b200.fitting import optimize_fluxes
+    P = synth.make_workload("field20", seed=args.seed, render=synth.render_model_gpu)
+    P.return_residual = False
+    P.send_to_device()
+    scene = P.set_scene(np.arange(P.n_sources), params=P.truth)
+    P.pack_meta(scene)
+    P.replace_device_meta_ptrs()
+    prop = np.ascontiguousarray(scene.get_proposal())
+    ns, nb = len(prop), P.n_bands
+    s = torch.cuda.current_stream()
+    dprop = torch.from_numpy(prop.view(np.uint8).copy()).cuda()
+    flux = torch.empty((nb, ns), dtype=torch.float64, device="cuda")
+    prec = torch.empty((nb, ns, ns), dtype=torch.float64, device="cuda")
+    status = torch.zeros(nb, dtype=torch.int32, device="cuda")
+    y = torch.as_tensor(P.data, device="cuda", dtype=torch.float64)
+    w = torch.as_tensor(P.ierr, device="cuda", dtype=torch.float64)
+    cuts = [int(c) for c in np.concatenate([[0], np.cumsum(P.band_N_pix)])]
+
+    def fused():
+        _lib.call("fpho_patch_optimize_fluxes", P.device_patch.handle, dprop.data_ptr(), ns,
+                  flux.data_ptr(), prec.data_ptr(), status.data_ptr(), s.cuda_stream)
+
+    def unfused():
+        X = P.design_matrix_device(prop).to(torch.float64)
+        ata = torch.stack([(X[:, a:b] * w[a:b]) @ (X[:, a:b] * w[a:b]).T
+                           for a, b in zip(cuts[:-1], cuts[1:])])
+        atb = torch.stack([(X[:, a:b] * w[a:b]) @ (y[a:b] * w[a:b])
+                           for a, b in zip(cuts[:-1], cuts[1:])])
+        return torch.linalg.solve(ata, atb), ata
+
+    def timed(fn, n):
+        for _ in range(3):
+            fn()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+               for _ in range(n)]
+        for e0, e1 in evs:
+            e0.record(s)
+            fn()
+            e1.record(s)
+        torch.cuda.synchronize()
+        return float(np.median([a.elapsed_time(b) for a, b in evs]))
+
+    ms_fused = timed(fused, steps)
+    ms_unfused = timed(unfused, steps)
+    fl_u, pr_u = unfused()
+    torch.cuda.synchronize()
+    rel_prec = float((prec - pr_u).abs().max() / pr_u.abs().max())
+    rel_flux = float(((flux - fl_u).abs() / fl_u.abs().clamp_min(1e-300)).max())
+    optimize_fluxes(P, scene)
+    t0 = time.perf_counter()
+    n_host = 3
+    for _ in range(n_host):
+        optimize_fluxes(P, scene)
+    host_ms = (time.perf_counter() - t0) / n_host * 1e3
+    P.free()
+    return {"workload": "field20 flux solve: 20 sources, 8 bands x 4 exposures x 128x128 px, "
+                        "fixed shapes",
+            "fused_ms": ms_fused, "design_matrix_plus_cublas_ms": ms_unfused,
+            "host_reference_path_ms": host_ms, "speedup_vs_design_matrix": ms_unfused / ms_fused,
+            "speedup_vs_host": host_ms / ms_fused, "max_rel_diff_precision": rel_prec,
+            "max_rel_diff_flux": rel_flux, "status": int(status.sum().item()),
+            "timing": "device: CUDA events per call (median); host: wall clock of "
+                      "fitting.optimize_fluxes (device design matrix, copied to the host, numpy)"}
+
+
 def differentiable_leg(args, torch, P, cfg, steps):
     """The 20-source patch through the autograd Function and the
     device posterior, HMC leapfrog steps of 1e-3 in the unconstrained
@@ -830,6 +915,10 @@ def run_ours(args):
         rb.update({"peak": fp32_tflops, "frac": rb["achieved"] / fp32_tflops,
                    "peak_source": "measured live: packed FP32 FMA probe kernel"})
 
+    flux = None
+    if rank == 0 and world == 1 and not args.no_flux:
+        flux = flux_leg(args, torch, steps=max(3, min(args.steps, 50)))
+
     packing = None
     if rank == 0 and world == 1 and args.packing_patches > 0:
         packing = packing_leg(args, torch, args.packing_patches)
@@ -856,7 +945,10 @@ def run_ours(args):
             "data": "synthetic",
             "config": workload_config(P),
             "run_config": {"evaluated_pairs": evaluated_pairs, "l2": "flushed between steps",
-                           "tile_variant": list(_lib.variants()[cfg["variant"]]),
+                           "tile_variant": cfg["variant"],
+                           "tile_shape": dict(zip(("threads", "pixels_per_tile",
+                                                   "warps_sharing_gaussians"),
+                                                  _lib.variant_shapes()[cfg["variant"]])),
                            "live_cap": cfg["live_cap"], "schedule": cfg.get("schedule", 0),
                            "parallelism": f"patch-parallel x{world}"},
             "pix_gauss_per_s": P.pairs_per_eval * value,
@@ -871,13 +963,18 @@ def run_ours(args):
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum "
                                            "of one launch",
                          "peak_source": "measured live: packed FP32 FMA probe kernel",
-                         "kernel": "tile_kernel", "kernel_ms": tile_s * 1e3,
+                         "kernel": ("split_kernel_dyn" if _lib.variant_shapes()[cfg["variant"]][2]
+                                    else "tile_kernel_dyn") if cfg.get("schedule", 0) == 1 else
+                                   ("split_kernel" if _lib.variant_shapes()[cfg["variant"]][2]
+                                    else "tile_kernel"),
+                         "kernel_ms": tile_s * 1e3,
                          "sfu_gops": sfu, "sfu_peak_gops": ex2_gops, "sfu_frac": sfu / ex2_gops},
             "clocks": clk.summary(),
             "cpu_baseline": cpu,
             "differentiable": differentiable,
             "multichain": multichain,
             "batched": batched,
+            "flux_solve": flux,
             "packing": packing,
         }
         print(json.dumps(line), flush=True)

@@ -74,7 +74,12 @@ _SIGS = {
     "fpho_patch_set_exact_residual": (c_int, [c_void_p, c_int]),
     "fpho_patch_set_test_stall": (c_int, [c_void_p, c_int]),
     "fpho_patch_design_matrix": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p]),
+    "fpho_patch_flux_normal_equations": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p,
+                                                 c_void_p]),
+    "fpho_patch_optimize_fluxes": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p,
+                                           c_void_p, c_void_p]),
     "fpho_variant_info": (c_int, [c_int, ctypes.POINTER(c_int)]),
+    "fpho_variant_shape": (c_int, [c_int, ctypes.POINTER(c_int)]),
     "fpho_patch_count_pairs": (c_int, [c_void_p, c_int, ctypes.POINTER(ctypes.c_longlong)]),
     "fpho_patch_error_word": (c_int, [c_void_p, ctypes.POINTER(c_int)]),
     "fpho_evaluate_proposal": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_int,
@@ -86,6 +91,10 @@ _SIGS = {
                                                c_void_p]),
     "fpho_batch_create": (c_int, [c_void_p, c_int, c_int, c_void_p, ctypes.POINTER(c_void_p)]),
     "fpho_batch_info": (c_int, [c_void_p, c_int64_p]),
+    "fpho_batch_create_config": (c_int, [c_void_p, c_int, c_int, c_int, c_int, c_void_p,
+                                         ctypes.POINTER(c_void_p)]),
+    "fpho_batch_variants": (c_int, [ctypes.POINTER(c_int), c_int]),
+    "fpho_batch_config": (c_int, [c_void_p, ctypes.POINTER(c_int)]),
     "fpho_batch_evaluate": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_uint, c_void_p]),
     "fpho_batch_count_pairs": (c_int, [c_void_p, c_int, ctypes.POINTER(ctypes.c_longlong)]),
     "fpho_batch_time_tiles": (c_int, [c_void_p, c_int]),
@@ -165,6 +174,19 @@ def variants():
     for v in range(n):
         L.fpho_variant_info(v, out)
         res.append((out[0], out[1]))
+    return res
+
+
+def variant_shapes():
+    """List of (threads per CTA, pixels per tile, warps sharing a tile's
+    Gaussians -- 0 for the classic body) of the compiled tile kernels."""
+    out = (c_int * 3)()
+    L = get()
+    n = L.fpho_variant_shape(0, out)
+    res = []
+    for v in range(n):
+        L.fpho_variant_shape(v, out)
+        res.append((out[0], out[1], out[2]))
     return res
 
 

@@ -17,7 +17,14 @@ from . import _lib
 from .kernel_limits import NPARAMS
 from .proposal import source_struct_dtype
 
-__all__ = ["PatchBatch"]
+__all__ = ["PatchBatch", "batch_variants"]
+
+
+def batch_variants():
+    """The tile variants that have a batched kernel (fpho_batch_variants)."""
+    out = (ctypes.c_int * 16)()
+    n = _lib.lib.fpho_batch_variants(out, 16)
+    return [out[i] for i in range(min(n, 16)) if out[i] >= 0]
 
 
 class PatchBatch:
@@ -27,16 +34,30 @@ class PatchBatch:
     ----------
     patches : list of patch objects with a ``device_patch`` (DevicePatch)
     live_cap : image-Gaussian records per shared-memory stage
+    variant : tile variant of the batched kernel (one of :func:`batch_variants`;
+        None: the default, 64 threads x 8 pixels)
+    ctas_per_sm : cap on the persistent grid's resident CTAs per SM (0: none)
+    config : a dict from :func:`forcepho_b200.autotune.choose_batch_config`
+        (``variant``, ``live_cap``, ``ctas_per_sm``), overriding the above
     """
 
-    def __init__(self, patches, live_cap=128, stream=None):
+    def __init__(self, patches, live_cap=128, stream=None, variant=None, ctas_per_sm=0,
+                 config=None):
+        if config is not None:
+            variant = config.get("variant", variant)
+            live_cap = config.get("live_cap", live_cap)
+            ctas_per_sm = config.get("ctas_per_sm", ctas_per_sm)
         self.patches = list(patches)
         handles = (ctypes.c_void_p * len(self.patches))(
             *[p.device_patch.handle for p in self.patches])
         h = ctypes.c_void_p()
-        _lib.call("fpho_batch_create", handles, len(self.patches), int(live_cap), stream,
-                  ctypes.byref(h))
+        _lib.call("fpho_batch_create_config", handles, len(self.patches),
+                  -1 if variant is None else int(variant), int(live_cap), int(ctas_per_sm),
+                  stream, ctypes.byref(h))
         self.handle = h.value
+        cfg = (ctypes.c_int * 4)()
+        _lib.call("fpho_batch_config", self.handle, cfg)
+        self.config = {"variant": cfg[0], "live_cap": cfg[1], "ctas_per_sm": cfg[2]}
         info = (ctypes.c_int64 * 7)()
         _lib.call("fpho_batch_info", self.handle, info)
         self.n_sources_total, self.n_bands_total, self.n_dchi2 = info[1], info[2], info[3]

@@ -28,16 +28,6 @@
 namespace fpho {
 namespace {
 
-constexpr int BT_THREADS = 64;  // the batched tile shape: 64 threads x 8 pixels
-constexpr int BT_K = 8;
-
-// index of the batched tile shape among the compiled variants
-int batched_variant() {
-    for (int v = 0; v < variant_count(); ++v)
-        if (variant_threads(v) == BT_THREADS && variant_tile_pixels(v) == BT_THREADS * BT_K)
-            return v;
-    return -1;
-}
 
 struct BatchPatch {
     PatchView pv;
@@ -70,7 +60,9 @@ __global__ void batch_gaussians(const BatchPatch *bps, const int2 *expmap,
                        bp.gbox + g0 + i);
 }
 
-template <int NT, int K>
+// SPLIT = 0: tile_body with NT threads x K pixels per tile; SPLIT = NW:
+// tile_body_split with NW warps (NT = 32 NW) and K pixels per thread.
+template <int NT, int K, int SPLIT>
 __global__ void __launch_bounds__(NT) batch_tiles(const TileArgs *args, const int2 *work,
                                                   int n_work, int *counter) {
     extern __shared__ __align__(128) unsigned char smem[];
@@ -89,7 +81,10 @@ __global__ void __launch_bounds__(NT) batch_tiles(const TileArgs *args, const in
         __syncthreads();  // all threads hold `it` before s_item is rewritten
         if (it >= n_work) break;
         const int2 w = work[it];
-        tile_body<NT, K>(args[w.x], w.y, smem, &mbar, phase);
+        if constexpr (SPLIT > 0)
+            tile_body_split<SPLIT, K>(args[w.x], w.y, smem, &mbar, phase);
+        else
+            tile_body<NT, K>(args[w.x], w.y, smem, &mbar, phase);
         __syncthreads();  // shared memory of this tile fully consumed
     }
 }
@@ -111,8 +106,34 @@ __global__ void batch_reduce(const BandJob *jobs, double *chi2, float *dchi2, in
     if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) *counter = 0;
 }
 
+// The tile shapes compiled for batches: (threads, pixels per tile, warps
+// sharing a tile's Gaussians) and the kernel; each runs the patches planned
+// with the patch variant of the same shape.
+struct BatchShape {
+    int nt, tile, split;
+    const void *fn;
+};
+const BatchShape kBatchShapes[] = {
+    {64, 512, 0, (const void *)batch_tiles<64, 8, 0>},    // default: 64 threads x 8 pixels
+    {64, 256, 0, (const void *)batch_tiles<64, 4, 0>},
+    {128, 512, 0, (const void *)batch_tiles<128, 4, 0>},
+    {128, 256, 4, (const void *)batch_tiles<128, 8, 4>},  // 4 warps share 256-pixel tiles
+    {64, 256, 2, (const void *)batch_tiles<64, 8, 2>},    // 2 warps share 256-pixel tiles
+};
+constexpr int kNumBatchShapes = sizeof(kBatchShapes) / sizeof(kBatchShapes[0]);
+
+// the patch variant planned like batch shape `i`, or -1 if none is compiled
+int shape_variant(int i) {
+    const BatchShape &B = kBatchShapes[i];
+    for (int v = 0; v < variant_count(); ++v)
+        if (variant_threads(v) == B.nt && variant_tile_pixels(v) == B.tile &&
+            variant_split(v) == B.split)
+            return v;
+    return -1;
+}
+
 std::mutex g_attr_mu;
-size_t g_attr_set[64];
+size_t g_attr_set[64][kNumBatchShapes];
 
 }  // namespace
 }  // namespace fpho
@@ -122,6 +143,9 @@ using namespace fpho;
 struct fpho_batch {
     std::vector<fpho_patch *> patches;
     int live_cap = 256;
+    int shape = 0;         // index into kBatchShapes
+    int variant = -1;      // the patches' tile variant
+    int ctas_per_sm = 0;   // cap on resident CTAs per SM of the persistent grid (0: none)
     int n_work = 0, n_exp_total = 0, max_g = 0, n_jobs = 0, max_stride = 0;
     int n_src_total = 0, n_band_total = 0;
     long long n_dchi2 = 0;
@@ -181,25 +205,44 @@ void destroy_batch(fpho_batch *b) {
 
 }  // namespace
 
-extern "C" int fpho_batch_create(fpho_patch *const *patches, int n, int live_cap, void *stream,
-                                 fpho_batch **out) {
+extern "C" int fpho_batch_variants(int *out, int cap) {
+    clear_error();
+    for (int i = 0; i < kNumBatchShapes && out && i < cap; ++i) out[i] = shape_variant(i);
+    return kNumBatchShapes;
+}
+
+extern "C" int fpho_batch_create_config(fpho_patch *const *patches, int n, int variant,
+                                        int live_cap, int ctas_per_sm, void *stream,
+                                        fpho_batch **out) {
     clear_error();
     if (!patches || !out || n < 1) return set_error(FPHO_ERR_INVALID, "bad batch arguments");
     *out = nullptr;
     if (live_cap < 32 || live_cap > 4096)
         return set_error(FPHO_ERR_INVALID, "live_cap %d outside [32, 4096]", live_cap);
-    // the batched tile kernel is compiled for one tile shape (64 threads x 8 pixels)
+    if (ctas_per_sm < 0 || ctas_per_sm > 32)
+        return set_error(FPHO_ERR_INVALID, "ctas_per_sm %d outside [0, 32]", ctas_per_sm);
+    int shape = -1;
+    for (int i = 0; i < kNumBatchShapes; ++i)
+        if (shape_variant(i) >= 0 && (variant < 0 ? i == 0 : shape_variant(i) == variant)) {
+            shape = i;
+            break;
+        }
+    if (shape < 0)
+        return set_error(FPHO_ERR_INVALID, "no batched tile kernel is compiled for variant %d",
+                         variant);
+    variant = shape_variant(shape);
     for (int i = 0; i < n; ++i) {
         if (!patches[i]) return set_error(FPHO_ERR_INVALID, "patch %d is NULL", i);
-        if (batched_variant() < 0)
-            return set_error(FPHO_ERR_STATE, "the batched tile shape is not compiled");
-        int rc = fpho_patch_set_config(patches[i], batched_variant(), live_cap, stream);
+        int rc = fpho_patch_set_config(patches[i], variant, live_cap, stream);
         if (rc) return rc;
     }
     fpho_batch *b = new (std::nothrow) fpho_batch();
     if (!b) return set_error(FPHO_ERR_NOMEM, "host allocation failed");
     b->patches.assign(patches, patches + n);
     b->live_cap = live_cap;
+    b->shape = shape;
+    b->variant = variant;
+    b->ctas_per_sm = ctas_per_sm;
     std::vector<BatchPatch> bps(n);
     std::vector<int2> expmap;
     std::vector<std::pair<double, int2>> items;
@@ -292,8 +335,7 @@ extern "C" int fpho_batch_create(fpho_patch *const *patches, int n, int live_cap
     if (!rc && cudaMemsetAsync(b->d_counter, 0, sizeof(int), s) != cudaSuccess)
         rc = set_error(FPHO_ERR_CUDA, "cudaMemsetAsync failed");
     if (!rc) {
-        b->smem = tile_smem_bytes(batched_variant(), live_cap, std::max(b->max_g, 1),
-                                  b->max_stride);
+        b->smem = tile_smem_bytes(b->variant, live_cap, std::max(b->max_g, 1), b->max_stride);
         if (b->smem > 227 * 1024)
             rc = set_error(FPHO_ERR_LIMIT, "shared memory %zu exceeds 227 KB", b->smem);
     }
@@ -301,21 +343,26 @@ extern "C" int fpho_batch_create(fpho_patch *const *patches, int n, int live_cap
         int dev = 0, sms = 0, per_sm = 0;
         cudaError_t e = cudaGetDevice(&dev);
         if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        const void *fn = (const void *)batch_tiles<BT_THREADS, BT_K>;
+        const BatchShape &B = kBatchShapes[b->shape];
         if (e == cudaSuccess) {
             std::lock_guard<std::mutex> lk(g_attr_mu);
-            if (dev < 64 && g_attr_set[dev] < b->smem) {
-                e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+            if (dev < 64 && g_attr_set[dev][b->shape] < b->smem) {
+                e = cudaFuncSetAttribute(B.fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          (int)b->smem);
-                if (e == cudaSuccess) g_attr_set[dev] = b->smem;
+                if (e == cudaSuccess) g_attr_set[dev][b->shape] = b->smem;
             }
         }
         if (e == cudaSuccess)
-            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, BT_THREADS, b->smem);
+            e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, B.fn, B.nt, b->smem);
         if (e != cudaSuccess)
             rc = set_error(FPHO_ERR_CUDA, "batch launch setup: %s", cudaGetErrorString(e));
-        else
-            b->grid = std::max(1, std::min(b->n_work, sms * std::max(per_sm, 1)));
+        else if (per_sm < 1)
+            rc = set_error(FPHO_ERR_LIMIT, "the batched tile kernel cannot be resident with "
+                           "%zu bytes of shared memory", b->smem);
+        else {
+            if (b->ctas_per_sm > 0) per_sm = std::min(per_sm, b->ctas_per_sm);
+            b->grid = std::max(1, std::min(b->n_work, sms * per_sm));
+        }
     }
     if (!rc && cudaStreamSynchronize(s) != cudaSuccess)
         rc = set_error(FPHO_ERR_CUDA, "cudaStreamSynchronize failed");
@@ -324,6 +371,21 @@ extern "C" int fpho_batch_create(fpho_patch *const *patches, int n, int live_cap
         return rc;
     }
     *out = b;
+    return FPHO_OK;
+}
+
+extern "C" int fpho_batch_create(fpho_patch *const *patches, int n, int live_cap, void *stream,
+                                 fpho_batch **out) {
+    return fpho_batch_create_config(patches, n, -1, live_cap, 0, stream, out);
+}
+
+extern "C" int fpho_batch_config(const fpho_batch *b, int out[4]) {
+    clear_error();
+    if (!b || !out) return set_error(FPHO_ERR_INVALID, "NULL argument");
+    out[0] = b->variant;
+    out[1] = b->live_cap;
+    out[2] = b->ctas_per_sm;
+    out[3] = b->grid;
     return FPHO_OK;
 }
 
@@ -391,9 +453,13 @@ static int batch_enqueue(fpho_batch *b, const fpho_source *d_props, double *d_ch
     }
     if (b->ev0) CUDA_TRY(cudaEventRecord(b->ev0, s));
     if (b->n_work > 0) {
-        batch_tiles<BT_THREADS, BT_K><<<b->grid, BT_THREADS, b->smem, s>>>(b->d_args, b->d_work,
-                                                                          b->n_work, b->d_counter);
-        CUDA_TRY(cudaGetLastError());
+        const BatchShape &B = kBatchShapes[b->shape];
+        const TileArgs *args = b->d_args;
+        const int2 *work = b->d_work;
+        int n_work = b->n_work;
+        int *counter = b->d_counter;
+        void *kargs[] = {(void *)&args, (void *)&work, (void *)&n_work, (void *)&counter};
+        CUDA_TRY(cudaLaunchKernel(B.fn, dim3(b->grid), dim3(B.nt), kargs, b->smem, s));
     }
     if (b->ev1) CUDA_TRY(cudaEventRecord(b->ev1, s));
     if (b->n_jobs > 0) {

@@ -65,7 +65,7 @@ extern "C" int fpho_sizeof(int which) {
 // ======================================================================= kernels
 namespace fpho {
 
-template <int NT, int K, bool GRAD>
+template <int NT, int K, bool GRAD, bool EXACT = false>
 __global__ void __launch_bounds__(NT) tile_kernel(TileArgs A) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ uint64_t mbar;
@@ -75,14 +75,14 @@ __global__ void __launch_bounds__(NT) tile_kernel(TileArgs A) {
     }
     __syncthreads();
     uint32_t phase = 0;
-    tile_body<NT, K, GRAD>(A, blockIdx.x, smem, &mbar, phase);
+    tile_body<NT, K, GRAD, EXACT>(A, blockIdx.x, smem, &mbar, phase);
 }
 
 // Persistent form: each CTA takes tiles from `order` through an atomic counter
 // (reset by order_tiles) until the list is exhausted, so the most expensive
 // tiles start first and the cheap ones fill the gaps at the end.  The counter
 // only hands out indices; no CTA waits on another.
-template <int NT, int K, bool GRAD>
+template <int NT, int K, bool GRAD, bool EXACT = false>
 __global__ void __launch_bounds__(NT) tile_kernel_dyn(TileArgs A, const int *order, int n_tiles,
                                                       int *counter) {
     extern __shared__ __align__(128) unsigned char smem[];
@@ -99,7 +99,7 @@ __global__ void __launch_bounds__(NT) tile_kernel_dyn(TileArgs A, const int *ord
         __syncthreads();
         const int item = s_item;
         if (item >= n_tiles) break;
-        tile_body<NT, K, GRAD>(A, order[item], smem, &mbar, phase);
+        tile_body<NT, K, GRAD, EXACT>(A, order[item], smem, &mbar, phase);
         __syncthreads();
     }
 }
@@ -118,41 +118,119 @@ __global__ void __launch_bounds__(NT) design_kernel(TileArgs A, float *X, long l
     design_body<NT, K>(A, blockIdx.x, smem, &mbar, phase, X, npix);
 }
 
+// Split tiles (tile_body_split): NW warps share each tile's Gaussians, K
+// pixels per thread, 32 K pixels per tile.  MINB > 1 asks the compiler for at
+// least MINB resident CTAs per SM (a register cap of 64K / (32 NW MINB)).
+template <int NW, int K, bool GRAD, int MINB = 1>
+__global__ void __launch_bounds__(32 * NW, MINB) split_kernel(TileArgs A) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ uint64_t mbar;
+    if (threadIdx.x == 0) {
+        mbar_init(&mbar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    uint32_t phase = 0;
+    tile_body_split<NW, K, GRAD>(A, blockIdx.x, smem, &mbar, phase);
+}
+
+template <int NW, int K, bool GRAD, int MINB = 1>
+__global__ void __launch_bounds__(32 * NW, MINB) split_kernel_dyn(TileArgs A, const int *order,
+                                                                  int n_tiles, int *counter) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ uint64_t mbar;
+    __shared__ int s_item;
+    if (threadIdx.x == 0) {
+        mbar_init(&mbar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    uint32_t phase = 0;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = atomicAdd(counter, 1);
+        __syncthreads();
+        const int item = s_item;
+        if (item >= n_tiles) break;
+        tile_body_split<NW, K, GRAD>(A, order[item], smem, &mbar, phase);
+        __syncthreads();
+    }
+}
+
 // ------------------------------------------------------------ variants
+// Kernel kinds of a variant: chi2 only, chi2 + gradient, and chi2 + gradient
+// with the residual pass in the reference's float arithmetic (the
+// exact-residual mode; compiled for the default 64x4 tile only).
+enum { KIND_CHI2 = 0, KIND_GRAD = 1, KIND_EXACT = 2, N_KINDS = 3 };
 struct Variant {
-    int nt, k;
-    const void *fn[2];   // [0] chi2 only, [1] chi2 + gradient
-    const void *dyn[2];  // persistent forms of the same
-    const void *design;  // design-matrix rows with the same tile shape
+    int nt;                    // threads per CTA
+    int tile;                  // pixels per tile
+    int split;                 // 0: tile_body (every thread its own pixels); NW: tile_body_split
+    const void *fn[N_KINDS];   // one CTA per tile, by kind (nullptr: not compiled)
+    const void *dyn[N_KINDS];  // persistent forms of the same
+    const void *design;        // design-matrix rows over tiles of the same size
+    int design_nt;             // its threads per CTA
 };
 #define FPHO_VARIANT(NT, K)                                                                      \
-    {NT, K, {(const void *)tile_kernel<NT, K, false>, (const void *)tile_kernel<NT, K, true>},  \
-     {(const void *)tile_kernel_dyn<NT, K, false>, (const void *)tile_kernel_dyn<NT, K, true>}, \
-     (const void *)design_kernel<NT, K>}
+    {NT, NT * K, 0,                                                                              \
+     {(const void *)tile_kernel<NT, K, false>, (const void *)tile_kernel<NT, K, true>, nullptr}, \
+     {(const void *)tile_kernel_dyn<NT, K, false>, (const void *)tile_kernel_dyn<NT, K, true>,  \
+      nullptr},                                                                                  \
+     (const void *)design_kernel<NT, K>, NT}
+#define FPHO_VARIANT_EXACT(NT, K)                                                                \
+    {NT, NT * K, 0,                                                                              \
+     {(const void *)tile_kernel<NT, K, false>, (const void *)tile_kernel<NT, K, true>,           \
+      (const void *)tile_kernel<NT, K, true, true>},                                             \
+     {(const void *)tile_kernel_dyn<NT, K, false>, (const void *)tile_kernel_dyn<NT, K, true>,  \
+      (const void *)tile_kernel_dyn<NT, K, true, true>},                                         \
+     (const void *)design_kernel<NT, K>, NT}
+// DNT x DK: the design kernel's shape over the same 32 K pixel tiles
+#define FPHO_SPLIT(NW, K, DNT, DK)                                                               \
+    {32 * NW, 32 * K, NW,                                                                        \
+     {(const void *)split_kernel<NW, K, false>, (const void *)split_kernel<NW, K, true>,         \
+      nullptr},                                                                                  \
+     {(const void *)split_kernel_dyn<NW, K, false>, (const void *)split_kernel_dyn<NW, K, true>, \
+      nullptr},                                                                                  \
+     (const void *)design_kernel<DNT, DK>, DNT}
+#define FPHO_SPLIT_MINB(NW, K, MINB, DNT, DK)                                                    \
+    {32 * NW, 32 * K, NW,                                                                        \
+     {(const void *)split_kernel<NW, K, false, MINB>, (const void *)split_kernel<NW, K, true, MINB>, \
+      nullptr},                                                                                  \
+     {(const void *)split_kernel_dyn<NW, K, false, MINB>,                                        \
+      (const void *)split_kernel_dyn<NW, K, true, MINB>, nullptr},                               \
+     (const void *)design_kernel<DNT, DK>, DNT}
+// Indices are part of the tuning interface (fpho_patch_set_config): new
+// shapes are appended.
 static const Variant kVariants[] = {
-    FPHO_VARIANT(128, 4), FPHO_VARIANT(128, 2), FPHO_VARIANT(256, 2), FPHO_VARIANT(64, 4),
+    FPHO_VARIANT(128, 4), FPHO_VARIANT(128, 2), FPHO_VARIANT(256, 2), FPHO_VARIANT_EXACT(64, 4),
     FPHO_VARIANT(256, 4), FPHO_VARIANT(128, 8), FPHO_VARIANT(64, 8), FPHO_VARIANT(32, 8),
+    FPHO_SPLIT(4, 8, 64, 4), FPHO_SPLIT(2, 8, 64, 4), FPHO_SPLIT(8, 8, 64, 4),
+    FPHO_SPLIT(4, 4, 32, 4), FPHO_SPLIT_MINB(4, 8, 5, 64, 4),
 };
 #undef FPHO_VARIANT
+#undef FPHO_VARIANT_EXACT
+#undef FPHO_SPLIT
+#undef FPHO_SPLIT_MINB
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
 int variant_count() { return kNumVariants; }
-int variant_tile_pixels(int v) { return kVariants[v].nt * kVariants[v].k; }
+bool variant_has_exact(int v) { return kVariants[v].fn[KIND_EXACT] != nullptr; }
+int variant_tile_pixels(int v) { return kVariants[v].tile; }
 int variant_threads(int v) { return kVariants[v].nt; }
+int variant_split(int v) { return kVariants[v].split; }
 
 static std::mutex g_attr_mu;
-// per device, variant, gradient flag, form: the dynamic shared memory the
+// per device, variant, kernel kind, form: the dynamic shared memory the
 // attribute allows, and for the persistent form the resident CTAs per SM and
 // the SM count at that size
-static size_t g_attr_set[64][kNumVariants][2][2];
-static int g_occ[64][kNumVariants][2], g_sms[64];
-static size_t g_occ_smem[64][kNumVariants][2];
+static size_t g_attr_set[64][kNumVariants][N_KINDS][2];
+static int g_occ[64][kNumVariants][N_KINDS], g_sms[64];
+static size_t g_occ_smem[64][kNumVariants][N_KINDS];
 
-static int prepare_fn(const void *fn, int dev, int variant, int grad, int form, size_t smem) {
+static int prepare_fn(const void *fn, int dev, int variant, int kind, int form, size_t smem) {
     std::lock_guard<std::mutex> lk(g_attr_mu);
-    if (dev < 64 && g_attr_set[dev][variant][grad][form] < smem) {
+    if (dev < 64 && g_attr_set[dev][variant][kind][form] < smem) {
         CUDA_TRY(cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-        g_attr_set[dev][variant][grad][form] = smem;
+        g_attr_set[dev][variant][kind][form] = smem;
     }
     return FPHO_OK;
 }
@@ -168,16 +246,20 @@ int device_sms() {
 }
 
 int launch_tile_kernel(int variant, const TileArgs &A, int n_tiles, cudaStream_t stream,
-                       bool grad, const int *order, int *counter) {
+                       bool grad, const int *order, int *counter, bool exact) {
     if (n_tiles <= 0) return FPHO_OK;
     const Variant &V = kVariants[variant];
     const bool dyn = order && counter;
-    const void *fn = dyn ? V.dyn[grad ? 1 : 0] : V.fn[grad ? 1 : 0];
+    const int kind = exact ? KIND_EXACT : (grad ? KIND_GRAD : KIND_CHI2);
+    const void *fn = dyn ? V.dyn[kind] : V.fn[kind];
+    if (!fn)
+        return set_error(FPHO_ERR_STATE, "the exact-residual kernel is not compiled for the "
+                         "%d-thread, %d-pixel tile", V.nt, V.tile);
     const size_t smem = tile_smem_bytes(variant, A.live_cap, A.idx_cap, A.pgrad_stride);
     int dev = 0;
     CUDA_TRY(cudaGetDevice(&dev));
     if (dev >= 64) return set_error(FPHO_ERR_LIMIT, "device ordinal %d >= 64", dev);
-    int rc = prepare_fn(fn, dev, variant, grad, dyn ? 1 : 0, smem);
+    int rc = prepare_fn(fn, dev, variant, kind, dyn ? 1 : 0, smem);
     if (rc) return rc;
     if (!dyn) {
         void *args[] = {(void *)&A};
@@ -187,14 +269,14 @@ int launch_tile_kernel(int variant, const TileArgs &A, int n_tiles, cudaStream_t
     int occ = 0, sms = 0;
     {
         std::lock_guard<std::mutex> lk(g_attr_mu);
-        if (g_occ_smem[dev][variant][grad] != smem || g_occ[dev][variant][grad] == 0) {
-            CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_occ[dev][variant][grad], fn,
+        if (g_occ_smem[dev][variant][kind] != smem || g_occ[dev][variant][kind] == 0) {
+            CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&g_occ[dev][variant][kind], fn,
                                                                    V.nt, smem));
-            g_occ_smem[dev][variant][grad] = smem;
+            g_occ_smem[dev][variant][kind] = smem;
             if (!g_sms[dev])
                 CUDA_TRY(cudaDeviceGetAttribute(&g_sms[dev], cudaDevAttrMultiProcessorCount, dev));
         }
-        occ = g_occ[dev][variant][grad];
+        occ = g_occ[dev][variant][kind];
         sms = g_sms[dev];
     }
     if (occ < 1) return set_error(FPHO_ERR_LIMIT, "tile kernel cannot be resident (smem %zu)", smem);
@@ -211,7 +293,8 @@ int launch_design_kernel(int variant, const TileArgs &A, int n_tiles, float *X, 
                          cudaStream_t stream) {
     if (n_tiles <= 0) return FPHO_OK;
     const Variant &V = kVariants[variant];
-    const size_t smem = tile_smem_bytes(variant, A.live_cap, A.idx_cap, A.pgrad_stride);
+    const size_t smem =
+        tile_smem_layout_bytes(V.design_nt / 32, A.live_cap, A.idx_cap, A.pgrad_stride);
     int dev = 0;
     CUDA_TRY(cudaGetDevice(&dev));
     if (dev >= 64) return set_error(FPHO_ERR_LIMIT, "device ordinal %d >= 64", dev);
@@ -224,12 +307,15 @@ int launch_design_kernel(int variant, const TileArgs &A, int n_tiles, float *X, 
         }
     }
     void *args[] = {(void *)&A, (void *)&X, (void *)&npix};
-    CUDA_TRY(cudaLaunchKernel(V.design, dim3(n_tiles), dim3(V.nt), args, smem, stream));
+    CUDA_TRY(cudaLaunchKernel(V.design, dim3(n_tiles), dim3(V.design_nt), args, smem, stream));
     return FPHO_OK;
 }
 
 size_t tile_smem_bytes(int variant, int live_cap, int idx_cap, int stride) {
-    return tile_smem_layout_bytes(kVariants[variant].nt / 32, live_cap, idx_cap, stride);
+    const Variant &V = kVariants[variant];
+    if (V.split)
+        return split_smem_layout_bytes(V.split, V.tile / 32, live_cap, idx_cap, stride);
+    return tile_smem_layout_bytes(V.nt / 32, live_cap, idx_cap, stride);
 }
 
 }  // namespace fpho
@@ -635,7 +721,7 @@ static void destroy_patch(fpho_patch *p) {
     dfree(p->d_data); dfree(p->d_ierr); dfree(p->d_xpix); dfree(p->d_ypix); dfree(p->d_residual);
     dfree(p->d_exposure_start); dfree(p->d_exposure_N); dfree(p->d_band_start);
     dfree(p->d_band_N); dfree(p->d_struct); dfree(p->d_chi2_out); dfree(p->d_dchi2_out);
-    dfree(p->d_err); dfree(p->d_pairs);
+    dfree(p->d_err); dfree(p->d_pairs); dfree(p->d_pnorm); dfree(p->d_atb);
     if (p->ev_tile0) cudaEventDestroy(p->ev_tile0);
     if (p->ev_tile1) cudaEventDestroy(p->ev_tile1);
     delete p;
@@ -660,6 +746,9 @@ extern "C" int fpho_patch_set_config(fpho_patch *p, int variant, int live_cap, v
     if (tile_smem_bytes(variant, live_cap, p->max_g, 7 * p->n_sources) > 227 * 1024)
         return set_error(FPHO_ERR_LIMIT, "shared memory for live_cap %d exceeds 227 KB",
                          live_cap);
+    if (p->exact_residual && !variant_has_exact(variant))
+        return set_error(FPHO_ERR_STATE, "variant %d has no exact-residual kernel; turn the "
+                         "exact-residual mode off first", variant);
     const bool replan = variant_tile_pixels(variant) != variant_tile_pixels(p->variant);
     p->variant = variant;
     p->live_cap = live_cap;
@@ -682,6 +771,17 @@ extern "C" int fpho_patch_set_test_stall(fpho_patch *p, int on) {
     return FPHO_OK;
 }
 
+extern "C" int fpho_patch_set_exact_residual(fpho_patch *p, int on) {
+    clear_error();
+    if (!p) return set_error(FPHO_ERR_INVALID, "NULL patch");
+    if (on && !variant_has_exact(p->variant))
+        return set_error(FPHO_ERR_STATE, "the exact-residual mode needs a tile variant that "
+                         "compiles it (variant 3, 64 threads x 4 pixels); this patch uses %d",
+                         p->variant);
+    p->exact_residual = on ? 1 : 0;
+    return FPHO_OK;
+}
+
 extern "C" int fpho_patch_set_schedule(fpho_patch *p, int schedule) {
     clear_error();
     if (!p) return set_error(FPHO_ERR_INVALID, "NULL patch");
@@ -697,6 +797,16 @@ extern "C" int fpho_variant_info(int variant, int out[2]) {
         return set_error(FPHO_ERR_INVALID, "bad variant");
     out[0] = variant_threads(variant);
     out[1] = variant_tile_pixels(variant) / variant_threads(variant);
+    return variant_count();
+}
+
+extern "C" int fpho_variant_shape(int variant, int out[3]) {
+    clear_error();
+    if (variant < 0 || variant >= variant_count() || !out)
+        return set_error(FPHO_ERR_INVALID, "bad variant");
+    out[0] = variant_threads(variant);
+    out[1] = variant_tile_pixels(variant);
+    out[2] = variant_split(variant);
     return variant_count();
 }
 
@@ -754,9 +864,10 @@ int enqueue_evaluate(fpho_patch *p, const fpho_source *d_prop, double *d_chi2, f
                                        p->d_tile_counter);
         CUDA_TRY(cudaGetLastError());
         rc = launch_tile_kernel(p->variant, A, p->n_tiles, s, grad, p->d_tile_order,
-                                p->d_tile_counter);
+                                p->d_tile_counter, p->exact_residual != 0);
     } else {
-        rc = launch_tile_kernel(p->variant, A, p->n_tiles, s, grad);
+        rc = launch_tile_kernel(p->variant, A, p->n_tiles, s, grad, nullptr, nullptr,
+                                p->exact_residual != 0);
     }
     if (rc) return rc;
     if (p->ev_tile1) CUDA_TRY(cudaEventRecord(p->ev_tile1, s));

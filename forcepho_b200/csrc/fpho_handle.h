@@ -45,6 +45,9 @@ struct fpho_patch {
     // tile scheduling: 0 = one CTA per tile (hardware order), 1 = persistent
     // CTAs taking tiles by decreasing cost of the previous evaluation
     int schedule = 1;
+    // 1: the residual pass in the reference's float arithmetic (see
+    // fpho_patch_set_exact_residual)
+    int exact_residual = 0;
     int test_extra_tx = 0;  // see fpho_patch_set_test_stall
     int *d_tile_cost = nullptr, *d_tile_order = nullptr, *d_tile_counter = nullptr;
     // workspace
@@ -58,6 +61,9 @@ struct fpho_patch {
     int d_dchi2_cap = 0;
     int *d_err = nullptr;
     long long *d_pairs = nullptr;
+    // flux solve (fpho_flux.cu): per-tile normal-equation partials and ATb
+    double *d_pnorm = nullptr, *d_atb = nullptr;
+    size_t d_pnorm_cap = 0, d_atb_cap = 0;
     int count_pairs = 0;
     // optional events recorded around the tile kernel (timing of the dominant kernel)
     cudaEvent_t ev_tile0 = nullptr, ev_tile1 = nullptr;

@@ -21,12 +21,16 @@ void clear_error();
 int variant_count();
 int variant_tile_pixels(int v);
 int variant_threads(int v);
+bool variant_has_exact(int v);  // exact-residual kernels compiled for variant v
+int variant_split(int v);       // 0: tile_body; NW: tile_body_split with NW warps per tile
 size_t tile_smem_bytes(int variant, int live_cap, int idx_cap, int stride);
 int device_sms();  // SMs of the current device (cached)
 // One CTA per tile; or, with `order` and `counter` (both device pointers), the
 // persistent form taking tiles in that order (see order_tiles).
+// `exact` selects the exact-residual kernel (variant_has_exact must hold).
 int launch_tile_kernel(int variant, const TileArgs &A, int n_tiles, cudaStream_t stream,
-                       bool grad, const int *order = nullptr, int *counter = nullptr);
+                       bool grad, const int *order = nullptr, int *counter = nullptr,
+                       bool exact = false);
 
 PatchView make_view(const fpho_patch *p);
 

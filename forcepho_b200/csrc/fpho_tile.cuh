@@ -267,6 +267,42 @@ __device__ __forceinline__ void residual_pairs2(const v2 (&X)[KP], const v2 (&Y)
     }
 }
 
+// Pass 1 in the reference's float arithmetic, for the exact-residual mode:
+// ComputeResidualImage (forcepho/src/common_kernel.cc:57-83) operation by
+// operation, each rounded once (no multiply-add contraction), the
+// exp-argument test before the exponential, H with its division by 24, and
+// exp evaluated in double and rounded once to float -- the correctly rounded
+// float exp wherever double exp's error does not straddle a float rounding
+// boundary.  Pixels of the pair are taken one at a time.
+template <int KP>
+__device__ __forceinline__ void residual_exact(const v2 (&X)[KP], const v2 (&Y)[KP], v2 (&R)[KP],
+                                               const float *rec) {
+    const float nxc = rec[R_NXC], nyc = rec[R_NYC];
+    const float fxx = rec[R_FXX], fxy = rec[R_FXY], fyy = rec[R_FYY], amp = rec[R_AMP];
+#pragma unroll
+    for (int j = 0; j < KP; ++j) {
+        float xs[2], ys[2], rs[2];
+        unpk(X[j], xs[0], xs[1]);
+        unpk(Y[j], ys[0], ys[1]);
+        unpk(R[j], rs[0], rs[1]);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const float dx = __fadd_rn(xs[h], nxc);  // xp - xcen (nxc = -xcen exactly)
+            const float dy = __fadd_rn(ys[h], nyc);
+            const float vx = __fadd_rn(__fmul_rn(fxx, dx), __fmul_rn(fxy, dy));
+            const float vy = __fadd_rn(__fmul_rn(fyy, dy), __fmul_rn(fxy, dx));
+            const float ea = __fadd_rn(__fmul_rn(dx, vx), __fmul_rn(dy, vy));
+            if (ea > FPHO_MAX_EXP_ARG) continue;
+            const float gp = (float)exp((double)__fmul_rn(-0.5f, ea));
+            const float t = __fsub_rn(__fsub_rn(__fadd_rn(__fmul_rn(vx, vx), __fmul_rn(vy, vy)),
+                                                fxx), fyy);
+            const float H = __fadd_rn(1.0f, __fdiv_rn(t, 24.0f));
+            rs[h] = __fsub_rn(rs[h], __fmul_rn(__fmul_rn(amp, gp), H));
+        }
+        R[j] = pk(rs[0], rs[1]);
+    }
+}
+
 // Pass 2 for one Gaussian over the thread's KP pixel pairs: the twelve sums
 // from which the model's derivatives w.r.t. (A, x, y, fxx, fyy, fxy) follow.
 struct GradSums {
@@ -459,8 +495,9 @@ __device__ __forceinline__ int scan_tile(const TileArgs &A, float4 bb, int g0, i
 
 // ------------------------------------------------------------ the tile body
 // GRAD = false runs the residual pass and chi2 only (no gradient pass, no
-// gradient partials written).
-template <int NT, int K, bool GRAD = true>
+// gradient partials written).  EXACT = true runs the residual pass in the
+// reference's float arithmetic (residual_exact) instead of the packed pass.
+template <int NT, int K, bool GRAD = true, bool EXACT = false>
 __device__ __forceinline__ void tile_body(const TileArgs &A, int tile, unsigned char *smem,
                                           uint64_t *mbar, uint32_t &phase) {
     static_assert(K % 2 == 0, "pixels per thread must be even (packed pairs)");
@@ -542,6 +579,10 @@ __device__ __forceinline__ void tile_body(const TileArgs &A, int tile, unsigned 
         const int c0 = c * cap, n = min(cap, n_live - c0);
         if (c > 0) __syncthreads();  // previous chunk fully consumed
         stage(c0, n);
+        if (EXACT) {
+            for (int i = 0; i < n; ++i) residual_exact<KP>(X, Y, R, recs + (size_t)i * GSTAGE);
+            continue;
+        }
         int i = 0;
         for (; i + 1 < n; i += 2)
             residual_pairs2<KP>(X, Y, R, recs + (size_t)i * GSTAGE, recs + (size_t)(i + 1) * GSTAGE,
@@ -621,7 +662,11 @@ __device__ __forceinline__ void tile_body(const TileArgs &A, int tile, unsigned 
                 P[6] = fmaf(j1.x, gA, P[6]);
                 // flush at a source boundary or at the end of the chunk
                 if ((flag & FLAG_LAST_SRC) || last) {
-                    const int src = __float_as_int(j3.w);
+                    // the index comes from the staged record: bounded, so that
+                    // a stage a timed-out wait left stale cannot write outside
+                    // the sums (the error word already marks the evaluation)
+                    const int src = min((unsigned)__float_as_int(j3.w),
+                                        (unsigned)(A.pv.n_sources - 1));
                     float v[8] = {P[0], P[1], P[2], P[3], P[4], P[5], P[6], 0.0f};
 #pragma unroll
                     for (int k = 0; k < 7; ++k) P[k] = 0.0f;
@@ -664,6 +709,263 @@ __device__ __forceinline__ void tile_body(const TileArgs &A, int tile, unsigned 
         for (int w = 0; w < NW; ++w) c += s_chi2[w];
         A.pchi2[tile] = c;
     }
+    for (int j = tid; GRAD && j < stride; j += NT) {
+        float v = 0.0f;
+#pragma unroll
+        for (int w = 0; w < NW; ++w) v += wacc[w * stride + j];
+        A.pgrad[(size_t)tile * stride + j] = v;
+    }
+    if (A.tile_cost && tid == 0) A.tile_cost[tile] = n_live * td.count;
+    if (A.pairs && tid == 0) atomicAdd(reinterpret_cast<unsigned long long *>(A.pairs),
+                                       (unsigned long long)((long long)n_live * td.count));
+}
+
+// ------------------------------------------------------------ split tile body
+// A tile of 32*K pixels evaluated by NW warps that share the tile's kept
+// Gaussians: every warp holds all of the tile's pixels (lane l holds pixels
+// l, l+32, ..., K per thread, as K/2 packed pairs) and takes a contiguous
+// 1/NW of each staged chunk of kept Gaussians.
+//   pass 1: each warp sums -model over its Gaussians; the NW partial models
+//           are added to the data in warp order through shared memory, so
+//           every warp holds the same residual bit for bit;
+//   chi2:   warp 0, in double, as tile_body;
+//   pass 2: each warp forms the gradient of its Gaussians (12 packed sums per
+//           Gaussian, Jacobian applied once per Gaussian per thread) and
+//           flushes per-source sums into its own shared-memory row; the rows
+//           are added in warp order at the end.
+// Against tile_body with NT = 32 NW threads and K' = K / NW pixels per thread
+// on the same tile, each thread does the per-Gaussian work (record loads,
+// exp-argument set-up, Jacobian epilogue) for NW times as many pixels, and a
+// CTA slot takes NW times fewer pixels per Gaussian, so tiles stay small (good
+// culling) while a launch has more tiles per resident CTA (a shorter tail).
+// Results are deterministic; the residual is summed in a different order from
+// tile_body's, so the two agree to rounding, not bit for bit.
+__host__ __device__ inline size_t split_smem_layout_bytes(int nw, int k, int live_cap, int idx_cap,
+                                                         int stride) {
+    return (size_t)live_cap * GSTAGE * 4 + (size_t)idx_cap * 4 + (size_t)nw * stride * 4 +
+           (size_t)nw * 32 * k * 4;
+}
+
+template <int NW, int K, bool GRAD = true>
+__device__ __forceinline__ void tile_body_split(const TileArgs &A, int tile, unsigned char *smem,
+                                                uint64_t *mbar, uint32_t &phase) {
+    static_assert(K % 2 == 0, "pixels per thread must be even (packed pairs)");
+    constexpr int NT = 32 * NW;
+    constexpr int KP = K / 2;
+    constexpr int TP = 32 * K;  // pixels per tile
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int cap = A.live_cap;
+    const int stride = A.pgrad_stride;
+
+    float *recs = reinterpret_cast<float *>(smem);
+    int *kept = reinterpret_cast<int *>(smem + (size_t)cap * GSTAGE * 4);
+    float *wacc = reinterpret_cast<float *>(kept + A.idx_cap);
+    float *part = wacc + (size_t)NW * stride;  // [NW][TP] partial models
+
+    __shared__ int s_cnt[NW];
+    __shared__ double s_chi2;
+    __shared__ int s_any_weight;
+
+    const TileDesc td = A.tiles[tile];
+    const float4 bb = A.want_residual ? A.tbox_all[tile] : A.tbox_w[tile];
+    const int g0 = A.pv.gauss_start[td.exposure];
+    const int g1 = A.pv.gauss_start[td.exposure + 1];
+    const int npsf = A.pv.exp_npsf[td.exposure];
+
+    for (int j = tid; j < NW * stride; j += NT) wacc[j] = 0.0f;
+
+    // ---- the tile's pixels, in every warp: pair j holds pixels lane + 64j, lane + 64j + 32
+    const float xmid = 0.5f * (bb.x + bb.y), ymid = 0.5f * (bb.z + bb.w);
+    v2 X[KP], Y[KP], R[KP];
+    int any_w = 0;
+#pragma unroll
+    for (int j = 0; j < KP; ++j) {
+        float xs[2], ys[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int li = lane + (2 * j + h) * 32;
+            const bool ok = li < td.count;
+            const int pix = td.pix_begin + (ok ? li : 0);
+            xs[h] = ok ? A.pv.xpix[pix] : xmid;
+            ys[h] = ok ? A.pv.ypix[pix] : ymid;
+            any_w |= ok && (A.pv.ierr[pix] != 0.0f);
+        }
+        X[j] = pk(xs[0], xs[1]);
+        Y[j] = pk(ys[0], ys[1]);
+        R[j] = 0ull;  // -model of this warp's Gaussians
+    }
+    if (tid == 0) s_any_weight = 0;
+
+    const int n_live = scan_tile<NT>(A, bb, g0, g1, npsf, kept, s_cnt);
+    if (any_w) s_any_weight = 1;
+    __syncthreads();
+    const bool tile_has_weight = s_any_weight != 0;
+
+    auto stage = [&](int c0, int n) {
+        fence_proxy_async_smem();
+        if (warp == 0) {
+            if (lane == 0)
+                mbar_arrive_expect_tx(mbar, (uint32_t)(n * GSTAGE * 4 + A.test_extra_tx));
+            __syncwarp();
+            for (int i = lane; i < n; i += 32)
+                bulk_g2s(recs + (size_t)i * GSTAGE,
+                         A.gtab + (size_t)(g0 + (kept[c0 + i] >> 2)) * GREC, GSTAGE * 4, mbar);
+        }
+        mbar_wait_bounded(mbar, phase, A.err);
+        phase ^= 1u;
+    };
+    // this warp's share [i0, i1) of a chunk of n records: contiguous, even
+    // lengths (two Gaussians per step)
+    auto share = [&](int n, int &i0, int &i1) {
+        const int per = 2 * ((n + 2 * NW - 1) / (2 * NW));
+        i0 = min(n, warp * per);
+        i1 = min(n, i0 + per);
+    };
+
+    const v2 KEXP2 = pk1(KEXP), KEXPLO2 = pk1(KEXP_LO);
+    const v2 CM24 = pk1(-1.0f / 24.0f), C24 = pk1(1.0f / 24.0f);
+    const int n_chunks = (n_live + cap - 1) / cap;
+
+    // ------------------------------------------------------------ pass 1
+    for (int c = 0; c < n_chunks; ++c) {
+        const int c0 = c * cap, n = min(cap, n_live - c0);
+        if (c > 0) __syncthreads();
+        stage(c0, n);
+        int i0, i1;
+        share(n, i0, i1);
+        int i = i0;
+        for (; i + 1 < i1; i += 2)
+            residual_pairs2<KP>(X, Y, R, recs + (size_t)i * GSTAGE, recs + (size_t)(i + 1) * GSTAGE,
+                                CM24, KEXP2, KEXPLO2);
+        for (; i < i1; ++i) {
+            const float *r = recs + (size_t)i * GSTAGE;
+            v2 NXC, NYC, FXX, FXY, FYY, AMP, HB, C0;
+            ld2(r + R_NXC, NXC, NYC);
+            ld2(r + R_FXX, FXX, FXY);
+            ld2(r + R_FYY, FYY, AMP);
+            ld2(r + R_HB, HB, C0);
+            const v2 HA = mul2(AMP, CM24);
+            if (kept[c0 + i] & FLAG_CUT)
+                residual_pairs<KP, true>(X, Y, R, NXC, NYC, FXX, FXY, FYY, HA, HB, KEXP2, KEXPLO2);
+            else
+                residual_pairs<KP, false>(X, Y, R, NXC, NYC, FXX, FXY, FYY, HA, HB, KEXP2, KEXPLO2);
+        }
+    }
+
+    // ---- the residual: data plus the warps' partial (negative) models, in warp order
+#pragma unroll
+    for (int j = 0; j < KP; ++j) {
+        float m0, m1;
+        unpk(R[j], m0, m1);
+        part[warp * TP + lane + 64 * j] = m0;
+        part[warp * TP + lane + 64 * j + 32] = m1;
+    }
+    __syncthreads();
+    v2 R2[KP];
+    double chi2 = 0.0;
+#pragma unroll
+    for (int j = 0; j < KP; ++j) {
+        float r2v[2];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int li = lane + (2 * j + h) * 32;
+            const bool ok = li < td.count;
+            const int pix = td.pix_begin + (ok ? li : 0);
+            const float d = ok ? A.pv.data[pix] : 0.0f;
+            const float ie = ok ? A.pv.ierr[pix] : 0.0f;
+            float r = d;
+#pragma unroll
+            for (int w = 0; w < NW; ++w) r += part[w * TP + li];
+            if (warp == 0) {
+                if (A.want_residual && ok) A.pv.residual[pix] = r;
+                const float rie = r * ie, die = d * ie;
+                double c = ((double)rie - (double)die);
+                c *= ((double)rie + (double)die);
+                chi2 += (ie != 0.0f) ? c : 0.0;
+            }
+            r2v[h] = (ie != 0.0f) ? -2.0f * ((r * ie) * ie) : 0.0f;
+        }
+        R2[j] = pk(r2v[0], r2v[1]);
+    }
+    if (warp == 0) {
+        chi2 = warp_sum_d(chi2);
+        if (lane == 0) s_chi2 = chi2;
+    }
+
+    // ------------------------------------------------------------ pass 2
+    if (GRAD && tile_has_weight) {
+        float P[7] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+        for (int c = n_chunks - 1; c >= 0; --c) {
+            const int c0 = c * cap, n = min(cap, n_live - c0);
+            if (c != n_chunks - 1) {
+                __syncthreads();
+                stage(c0, n);
+            }
+            int i0, i1;
+            share(n, i0, i1);
+            auto epilogue = [&](const float *r, int flag, const GradSums &s, bool last) {
+                const float4 *rj = reinterpret_cast<const float4 *>(r + R_JA_FLUX);
+                const float fxx = r[R_FXX], fxy = r[R_FXY], fyy = r[R_FYY];
+                const float sVx = lanesum(s.Vx), sVy = lanesum(s.Vy), sW = lanesum(s.W);
+                const float gA = lanesum(s.A);
+                const float gx = lanesum(s.HVx) - (fxx * sVx + fxy * sVy) * (1.0f / 12.0f);
+                const float gy = lanesum(s.HVy) - (fxy * sVx + fyy * sVy) * (1.0f / 12.0f);
+                const float gfxx = lanesum(s.T1) * (1.0f / 12.0f) - 0.5f * lanesum(s.HXX) -
+                                   sW * (1.0f / 24.0f);
+                const float gfyy = lanesum(s.T2) * (1.0f / 12.0f) - 0.5f * lanesum(s.HYY) -
+                                   sW * (1.0f / 24.0f);
+                const float gfxy = lanesum(s.T3) * (1.0f / 12.0f) - lanesum(s.HXY);
+                const float4 j0 = rj[0], j1 = rj[1], j2 = rj[2], j3 = rj[3];
+                P[0] = fmaf(j0.x, gA, P[0]);
+                P[1] = fmaf(j1.z, gy, fmaf(j1.y, gx, P[1]));
+                P[2] = fmaf(j2.x, gy, fmaf(j1.w, gx, P[2]));
+                P[3] = fmaf(j2.w, gfyy, fmaf(j2.z, gfxy, fmaf(j2.y, gfxx, fmaf(j0.y, gA, P[3]))));
+                P[4] = fmaf(j3.z, gfyy, fmaf(j3.y, gfxy, fmaf(j3.x, gfxx, fmaf(j0.z, gA, P[4]))));
+                P[5] = fmaf(j0.w, gA, P[5]);
+                P[6] = fmaf(j1.x, gA, P[6]);
+                if ((flag & FLAG_LAST_SRC) || last) {
+                    // the index comes from the staged record: bounded, so that
+                    // a stage a timed-out wait left stale cannot write outside
+                    // the sums (the error word already marks the evaluation)
+                    const int src = min((unsigned)__float_as_int(j3.w),
+                                        (unsigned)(A.pv.n_sources - 1));
+                    float v[8] = {P[0], P[1], P[2], P[3], P[4], P[5], P[6], 0.0f};
+#pragma unroll
+                    for (int k = 0; k < 7; ++k) P[k] = 0.0f;
+                    const float tot = warp_reduce7(v, lane);
+                    const int k = reduce7_index(lane);
+                    if ((lane & 3) == 0 && k < 7) wacc[warp * stride + src * 7 + k] += tot;
+                }
+            };
+            int i = i0;
+            for (; i + 1 < i1; i += 2) {
+                const float *ra = recs + (size_t)i * GSTAGE, *rb = ra + GSTAGE;
+                GradSums sa, sb;
+                gradient_pairs2<KP>(X, Y, R2, ra, rb, C24, KEXP2, sa, sb);
+                epilogue(ra, kept[c0 + i], sa, false);
+                epilogue(rb, kept[c0 + i + 1], sb, i + 1 == i1 - 1);
+            }
+            for (; i < i1; ++i) {
+                const float *r = recs + (size_t)i * GSTAGE;
+                v2 NXC, NYC, FXX, FXY, FYY, AMP, HB, C0;
+                ld2(r + R_NXC, NXC, NYC);
+                ld2(r + R_FXX, FXX, FXY);
+                ld2(r + R_FYY, FYY, AMP);
+                ld2(r + R_HB, HB, C0);
+                const int flag = kept[c0 + i];
+                GradSums s;
+                if (flag & FLAG_CUT)
+                    gradient_pairs<KP, true>(X, Y, R2, NXC, NYC, FXX, FXY, FYY, C0, C24, KEXP2, s);
+                else
+                    gradient_pairs<KP, false>(X, Y, R2, NXC, NYC, FXX, FXY, FYY, C0, C24, KEXP2, s);
+                epilogue(r, flag, s, i == i1 - 1);
+            }
+        }
+    }
+    __syncthreads();
+
+    // ---- tile partials (fixed-order sums)
+    if (tid == 0) A.pchi2[tile] = s_chi2;
     for (int j = tid; GRAD && j < stride; j += NT) {
         float v = 0.0f;
 #pragma unroll
@@ -749,7 +1051,8 @@ __device__ __forceinline__ void design_body(const TileArgs &A, int tile, unsigne
             else
                 residual_pairs<KP, false>(Xp, Yp, M, NXC, NYC, FXX, FXY, FYY, HA, UB, KEXP2, KEXPLO2);
             if ((flag & FLAG_LAST_SRC) || i == n - 1) {
-                const int src = __float_as_int(r[R_SRC]);
+                const int src = min((unsigned)__float_as_int(r[R_SRC]),
+                                    (unsigned)(A.pv.n_sources - 1));
                 float *row = X + (size_t)src * npix + td.pix_begin;
 #pragma unroll
                 for (int j = 0; j < KP; ++j) {

@@ -5,10 +5,12 @@ least squares for one band: Xp = X w, yp = (y - fixedX) w, ATA = Xp Xp^T,
 fluxes = solve(ATA, Xp yp)) and :func:`optimize_fluxes` (the maximum-
 likelihood fluxes and flux precision matrices of the active sources,
 conditional on their shapes, from ``patcher.design_matrix``).
-:func:`optimize_fluxes_device` does the same without leaving the GPU: the
-design matrix from one ``fpho_patch_design_matrix`` launch, the normal
-equations as FP64 matrix products (cuBLAS through torch), the solves by
-torch.linalg.
+:func:`optimize_fluxes_device` does the same without leaving the GPU and
+without forming the design matrix: ``fpho_patch_optimize_fluxes`` builds each
+tile's unit-flux models in shared memory, reduces the FP64 normal equations
+per band in a fixed order and solves them by Cholesky factorisation, on the
+patch's device data (after ``subtract_fixed``, the data less the fixed
+sources).
 
 :func:`run_hmc` and :func:`run_opt` keep the call shape and the result
 fields of forcepho's ``run_lmc`` and ``run_opt`` (fitting.py:255-342,
@@ -56,27 +58,30 @@ def optimize_fluxes(patcher, active, return_all=False):
     return fluxes, precisions
 
 
-def optimize_fluxes_device(patcher, active):
-    """As :func:`optimize_fluxes`, computed on the GPU: returns (fluxes
-    (n_bands, n_source), precisions (n_bands, n_source, n_source)) as float64
-    CUDA tensors."""
+def optimize_fluxes_device(patcher, active, stream=None, return_status=False):
+    """As :func:`optimize_fluxes`, computed on the GPU in one call of
+    ``fpho_patch_optimize_fluxes``: returns (fluxes (n_bands, n_source),
+    precisions (n_bands, n_source, n_source)) as float64 CUDA tensors, and
+    with `return_status` an int32 tensor (n_bands,) that is 1 where a band's
+    precision matrix is not positive definite (its fluxes are NaN).  Nothing
+    is synchronized or copied to the host."""
     import torch
+    from . import _lib
     scene = active if hasattr(active, "get_proposal") else patcher.set_scene(active)
     patcher.pack_meta(scene)
     patcher.replace_device_meta_ptrs()
-    X = patcher.design_matrix_device(scene.get_proposal()).to(torch.float64)
-    y = torch.as_tensor(patcher.retrieve_array("data"), device="cuda", dtype=torch.float64)
-    w = torch.as_tensor(patcher.ierr, device="cuda", dtype=torch.float64)
-    cuts = np.concatenate([[0], np.cumsum(patcher.band_N_pix)])
-    fl, pr = [], []
-    for b in range(patcher.n_bands):
-        sl = slice(int(cuts[b]), int(cuts[b + 1]))
-        Xp = X[:, sl] * w[sl]
-        yp = y[sl] * w[sl]
-        ata = Xp @ Xp.T
-        fl.append(torch.linalg.solve(ata, Xp @ yp))
-        pr.append(ata)
-    return torch.stack(fl), torch.stack(pr)
+    prop = np.ascontiguousarray(scene.get_proposal())
+    ns, nb = len(prop), int(patcher.n_bands)
+    dprop = torch.from_numpy(prop.view(np.uint8).copy()).cuda()
+    flux = torch.empty((nb, ns), dtype=torch.float64, device="cuda")
+    prec = torch.empty((nb, ns, ns), dtype=torch.float64, device="cuda")
+    status = torch.zeros(nb, dtype=torch.int32, device="cuda")
+    s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+    _lib.call("fpho_patch_optimize_fluxes", patcher.device_patch.handle, dprop.data_ptr(), ns,
+              flux.data_ptr(), prec.data_ptr(), status.data_ptr(), s)
+    if return_status:
+        return flux, prec, status
+    return flux, prec
 
 
 class Result:
@@ -127,13 +132,15 @@ class Result:
 
 
 def run_hmc(model, q, n_draws, warmup=(10,), n_chains=1, n_leapfrog=10, step_size=0.05,
-            target_accept=0.75, jitter=0.2, random_seed=0xDEADBEEF):
+            target_accept=0.75, jitter=0.2, random_seed=0xDEADBEEF, z_cov=None, full=False,
+            adapt=False):
     """HMC on the GPU with the call shape of forcepho's ``run_lmc``.
 
     Parameters
     ----------
     model : forcepho_b200.autograd.DevicePosterior (one patch; chains are
-        device copies of it) or BatchPosterior (one chain per patch)
+        device copies of it) or BatchPosterior (one chain per patch), or any
+        object with the BatchPosterior sampling interface
     q : starting position in the constrained space, one chain's (broadcast
         to every chain) or all chains' concatenated
     n_draws : samples kept per chain
@@ -141,6 +148,17 @@ def run_hmc(model, q, n_draws, warmup=(10,), n_chains=1, n_leapfrog=10, step_siz
         multiplied by exp(2 (acceptance - target_accept)), clipped to
         [1/4, 4] per round
     n_chains : chains of a DevicePosterior model (ignored for a batch)
+    z_cov : the inverse mass matrix in the unconstrained coordinates z, as
+        the reference's ``z_cov``: a vector of variances (one chain's, or all
+        chains'), or with `full` a (d, d) covariance for every chain;
+        default the identity
+    full : a dense inverse mass matrix per chain (chains of equal size)
+        instead of a diagonal
+    adapt : after each warm-up round of at least 10 iterations, set the
+        inverse mass matrix to the (co)variance of that round's samples,
+        pooled over the chains when they are copies of one patch,
+        regularised towards the identity (as the reference's adapting
+        potential does, forcepho/fitting.py:370-413)
 
     Returns
     -------
@@ -148,18 +166,22 @@ def run_hmc(model, q, n_draws, warmup=(10,), n_chains=1, n_leapfrog=10, step_siz
         (n_chains, n_draws, ndim), in the constrained space, ``n_call`` (one
         per chain per leapfrog step), ``wall_time``, ``accept`` (per chain,
         production iterations), ``step_size``
-    sampler : the MultiChainHMC
+    sampler : the MultiChainHMC (``scale`` / ``chol``: the inverse-mass factors)
     """
     import time
     import torch
     from .autograd import BatchPosterior, DevicePosterior
-    from .sampling import MultiChainHMC, chain_posterior
+    from .sampling import MultiChainHMC, chain_posterior, estimate_mass
+    pooled = False
     if isinstance(model, DevicePosterior):
         lo = model.tr.lower.cpu().numpy()
         hi = model.tr.upper.cpu().numpy()
         post = chain_posterior(model.ev.patch, int(n_chains), lo, hi)
-    elif isinstance(model, BatchPosterior):
+        pooled = True
+    elif isinstance(model, BatchPosterior) or all(
+            hasattr(model, a) for a in ("lnp_per_patch", "n_patches", "par_pad", "par_patch")):
         post, n_chains = model, model.n_patches
+        pooled = getattr(model, "copies", None) is not None
     else:
         raise TypeError("model must be a DevicePosterior or a BatchPosterior")
     q = np.asarray(q, dtype=np.float64).reshape(-1)
@@ -168,23 +190,44 @@ def run_hmc(model, q, n_draws, warmup=(10,), n_chains=1, n_leapfrog=10, step_siz
     if q.size != post.ndim:
         raise ValueError(f"q has {q.size} entries; the chains need {post.ndim}")
     z0 = post.inverse_transform(torch.as_tensor(q, device="cuda"))
-    hmc = MultiChainHMC(post, step_size, n_leapfrog, n_samples=int(n_draws),
-                        seed=int(random_seed) & 0x7FFFFFFF, jitter=jitter)
+    n_buf = max([int(n_draws)] + [int(w) for w in warmup])
+    hmc = MultiChainHMC(post, step_size, n_leapfrog, n_samples=n_buf,
+                        seed=int(random_seed) & 0x7FFFFFFF, jitter=jitter, full=full)
+    d = post.ndim // n_chains
+    if z_cov is not None:
+        zc = torch.as_tensor(np.asarray(z_cov, dtype=np.float64), device="cuda")
+        if full:
+            hmc.set_mass(chol=torch.linalg.cholesky(zc.reshape(d, d)))
+        else:
+            zc = zc.reshape(-1)
+            hmc.set_mass(scale=(zc.repeat(n_chains) if zc.numel() == d else zc).sqrt())
     hmc.set_state(z0)
     eps = float(step_size)
     t0 = time.time()
     for w in warmup:
         hmc.n_accept.zero_()
+        hmc.slot.zero_()
         hmc.run(int(w))
         acc = float(np.mean(hmc.acceptance(int(w))))
         eps *= float(np.clip(np.exp(2.0 * (acc - target_accept)), 0.25, 4.0))
+        if adapt and int(w) >= 10:
+            est = estimate_mass(hmc.samples[:int(w)], n_chains, full=full, pooled=pooled)
+            # the step size in whitened units: rescale by the change of the
+            # typical inverse-mass scale so the next round starts comparably
+            old = hmc.chol.diagonal(dim1=1, dim2=2) if full else hmc.scale
+            new = est.diagonal(dim1=1, dim2=2) if full else est
+            eps *= float(torch.exp(torch.log(old).mean() - torch.log(new).mean()))
+            if full:
+                hmc.set_mass(chol=est)
+            else:
+                hmc.set_mass(scale=est)
         hmc.set_eps(eps)
     hmc.n_accept.zero_()
     hmc.slot.zero_()
     hmc.run(int(n_draws))
     torch.cuda.synchronize()
     wall = time.time() - t0
-    zs = hmc.samples[:int(n_draws)]
+    zs = hmc.samples[:int(n_draws)]  # the ring buffer started at slot 0 for the draws
     qs = post.transform(zs).cpu().numpy().reshape(int(n_draws), n_chains, -1)
     chain = qs.transpose(1, 0, 2)
     return Result(ndim=chain.shape[-1], starting_position=q.copy(),

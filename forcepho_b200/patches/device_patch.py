@@ -57,6 +57,14 @@ class DevicePatch:
         """0: one CTA per tile; 1: persistent CTAs, costliest tiles first."""
         _lib.call("fpho_patch_set_schedule", self.handle, int(schedule))
 
+    def set_exact_residual(self, on=True, live_cap=160, stream=None):
+        """Residual pass in the reference's float arithmetic (a parity
+        diagnostic, see fpho_patch_set_exact_residual); switching it on
+        selects the 64 x 4 tile variant that compiles it."""
+        if on:
+            self.set_config(3, live_cap, stream)
+        _lib.call("fpho_patch_set_exact_residual", self.handle, int(bool(on)))
+
     def free(self):
         if getattr(self, "handle", None):
             _lib.lib.fpho_patch_free(self.handle)

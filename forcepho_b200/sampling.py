@@ -10,6 +10,17 @@ launch sequence evaluates every chain's leapfrog step.  One HMC iteration --
 momentum draw, ``n_leapfrog`` leapfrog steps, per-chain Metropolis test,
 selection of the accepted or the old state, recording of the sample -- is
 captured in one CUDA graph and replayed.
+
+Mass matrix.  The reference's NUTS takes the covariance of the
+unconstrained coordinates z as its inverse mass matrix (``z_cov``, diagonal
+or full, adapted during warm-up; forcepho/fitting.py:255-342, 370-413).
+Here the inverse mass of chain k is M_k^-1 = L_k L_k^T, given as a diagonal
+(``scale``: L = diag(scale), the per-coordinate standard deviations) or, when
+every chain has the same number of coordinates, as one lower-triangular
+factor per chain (``chol``).  The leapfrog runs in whitened momenta u = L^T p
+with unit kinetic energy: u += eps/2 L^T grad, z += eps L u, which is HMC with
+mass M = (L L^T)^-1 in z.  :func:`estimate_mass` turns warm-up samples into
+the factors (regularised towards the identity as Stan does).
 """
 
 import torch
@@ -18,7 +29,7 @@ from .autograd import BatchPosterior
 from .batch import PatchBatch
 from .patches.device_patch import DevicePatch
 
-__all__ = ["MultiChainHMC", "ChainCopy", "chain_posterior"]
+__all__ = ["MultiChainHMC", "ChainCopy", "chain_posterior", "estimate_mass"]
 
 
 class ChainCopy:
@@ -48,17 +59,47 @@ def _per_patch(post, v):
     return torch.cat([v, v.new_zeros(1)])[post.par_pad].sum(dim=1)
 
 
+def estimate_mass(samples, n_chains, full=False, pooled=False, shrink=5.0, floor=1e-3):
+    """Inverse-mass factors from samples of z (a (n, ndim) tensor, chains
+    concatenated along ndim): the per-coordinate standard deviations
+    (diagonal) or, with `full`, one Cholesky factor of the covariance per
+    chain (every chain must have ndim / n_chains coordinates).  `pooled`
+    averages the (co)variances over the chains (chains of one posterior).
+    The estimate over N samples is regularised towards `floor` times the
+    identity with weight shrink / (N + shrink)."""
+    x = samples.to(torch.float64)
+    n = x.shape[0]
+    w = n / (n + shrink)
+    reg = floor * shrink / (n + shrink)
+    if not full:
+        var = x.var(dim=0, unbiased=True)
+        if pooled:
+            var = var.view(n_chains, -1).mean(dim=0).repeat(n_chains)
+        return (w * var + reg).sqrt()
+    d = x.shape[1] // n_chains
+    xc = x.view(n, n_chains, d)
+    xc = xc - xc.mean(dim=0, keepdim=True)
+    cov = torch.einsum("nki,nkj->kij", xc, xc) / max(n - 1, 1)
+    if pooled:
+        cov = cov.mean(dim=0, keepdim=True).expand(n_chains, d, d)
+    eye = torch.eye(d, dtype=torch.float64, device=x.device)
+    return torch.linalg.cholesky(w * cov + reg * eye)
+
+
 class MultiChainHMC:
-    """Static-length HMC (unit mass) with a Metropolis test per chain.
+    """Static-length HMC with a Metropolis test per chain.
 
     posterior: a BatchPosterior (``lnprob_and_grad``, ``lnp_per_patch``,
     ``par_patch``, ``par_pad``, ``n_patches``, ``ndim``); each patch is one
     chain.  ``n_samples`` > 0 keeps the last that many states in
     ``samples`` (a ring buffer on the device).  Each iteration draws each
-    chain's step size uniformly in eps * (1 +- jitter).
+    chain's step size uniformly in eps * (1 +- jitter).  The inverse mass
+    matrix is the identity until :meth:`set_mass` (``full``: one dense
+    factor per chain, which needs chains of equal size).
     """
 
-    def __init__(self, posterior, eps, n_leapfrog, n_samples=0, seed=0, jitter=0.2):
+    def __init__(self, posterior, eps, n_leapfrog, n_samples=0, seed=0, jitter=0.2,
+                 full=False):
         self.post = posterior
         # the step size lives on the device, so a captured iteration reads the
         # current value (set_eps between replays tunes it)
@@ -73,8 +114,44 @@ class MultiChainHMC:
         self.n_samples = int(n_samples)
         self.samples = torch.zeros((max(self.n_samples, 1), n), **f64)
         self.slot = torch.zeros(1, dtype=torch.int64, device="cuda")
+        # inverse-mass factors, read by the captured graph: set_mass copies into them
+        self.scale = torch.ones(n, **f64)
+        self.full = bool(full)
+        self.chol = None
+        if self.full:
+            if n % k:
+                raise ValueError("a full mass matrix needs chains of equal size")
+            d = n // k
+            self.chol = torch.eye(d, **f64).repeat(k, 1, 1)
         self.graph = None
         torch.cuda.manual_seed(seed)
+
+    def set_mass(self, scale=None, chol=None):
+        """Inverse mass matrix: per-coordinate standard deviations `scale`
+        (ndim,) or, for a sampler made with ``full``, Cholesky factors `chol`
+        (n_chains, d, d) or (d, d) for every chain.  Takes effect in the next
+        iteration (graph replays included)."""
+        if scale is not None:
+            self.scale.copy_(torch.as_tensor(scale, dtype=torch.float64).reshape(-1))
+        if chol is not None:
+            if self.chol is None:
+                raise ValueError("the sampler was made without a full mass matrix")
+            c = torch.as_tensor(chol, dtype=torch.float64, device="cuda")
+            self.chol.copy_(c.expand_as(self.chol))
+
+    def _to_z(self, u):
+        """L u per chain: a whitened displacement in z."""
+        if self.chol is None:
+            return self.scale * u
+        k, d = self.chol.shape[0], self.chol.shape[1]
+        return torch.bmm(self.chol, u.view(k, d, 1)).view(-1)
+
+    def _to_u(self, g):
+        """L^T g per chain: a z-gradient in whitened coordinates."""
+        if self.chol is None:
+            return self.scale * g
+        k, d = self.chol.shape[0], self.chol.shape[1]
+        return torch.bmm(self.chol.transpose(1, 2), g.view(k, d, 1)).view(-1)
 
     @property
     def eps(self):
@@ -97,14 +174,16 @@ class MultiChainHMC:
         u = torch.rand(self.lnp.shape, dtype=torch.float64, device="cuda")
         eps = (self.eps_t * (1.0 + self.jitter * (2.0 * u - 1.0)))[post.par_patch]
         h = 0.5 * eps
-        p = torch.randn(self.z.shape, dtype=torch.float64, device="cuda")
+        p = torch.randn(self.z.shape, dtype=torch.float64, device="cuda")  # whitened momenta
         kin0 = _per_patch(post, p * p) * 0.5
         z, g = self.z.clone(), self.g.clone()
+        gu = self._to_u(g)
         for _ in range(self.L):
-            p = p + h * g
-            z = z + eps * p
+            p = p + h * gu
+            z = z + eps * self._to_z(p)
             _, g = post.lnprob_and_grad(z)
-            p = p + h * g
+            gu = self._to_u(g)
+            p = p + h * gu
         lnp1 = post.lnp_per_patch(z)
         kin1 = _per_patch(post, p * p) * 0.5
         log_ratio = (lnp1 - kin1) - (self.lnp - kin0)

@@ -247,11 +247,34 @@ FPHO_API int fpho_spline_points(const fpho_spline *s, const double *x, const dou
 /* Build a batch of patches evaluated together by one persistent launch (the
  * reference evaluates one patch per launch, forcepho/proposal.py:133-136, one
  * patch per MPI child, forcepho/dispatcher.py).  Every patch is switched to
- * the batched tile shape (64 threads x 8 pixels) with `live_cap`; rebuild the batch after
- * fpho_patch_replace_meta or fpho_patch_set_config on a member.  The patch
- * handles must outlive the batch. */
+ * the default batched tile shape (64 threads x 8 pixels) with `live_cap`;
+ * rebuild the batch after fpho_patch_replace_meta or fpho_patch_set_config on
+ * a member.  The patch handles must outlive the batch.  Equivalent to
+ * fpho_batch_create_config(patches, n, -1, live_cap, 0, stream, out). */
 FPHO_API int fpho_batch_create(fpho_patch *const *patches, int n, int live_cap, void *stream,
                                fpho_batch **out);
+
+/* As fpho_batch_create with the launch configuration chosen by the caller
+ * (the batch autotuner; no reference counterpart, whose launch shape is
+ * thread_block, shared_size and max_registers, forcepho/proposal.py:62-65,88-89):
+ *   variant      the patches' tile variant, one of fpho_batch_variants
+ *                (-1: the default, 64 threads x 8 pixels);
+ *   live_cap     image-Gaussian records per shared-memory stage;
+ *   ctas_per_sm  cap on resident CTAs per SM of the persistent grid, 0 for
+ *                as many as fit.
+ * FPHO_ERR_INVALID for a variant without a batched kernel. */
+FPHO_API int fpho_batch_create_config(fpho_patch *const *patches, int n, int variant,
+                                      int live_cap, int ctas_per_sm, void *stream,
+                                      fpho_batch **out);
+
+/* The tile variants that have a batched kernel: fills out[0..cap) and
+ * returns how many there are (an entry is -1 if its patch variant is not
+ * compiled). */
+FPHO_API int fpho_batch_variants(int *out, int cap);
+
+/* The configuration of a batch: out = (variant, live_cap, ctas_per_sm cap,
+ * persistent grid size). */
+FPHO_API int fpho_batch_config(const fpho_batch *b, int out[4]);
 
 /* out[0] patches, out[1] total sources, out[2] total bands, out[3] total dchi2
  * floats, out[4] work items (tiles), out[5] persistent grid, out[6] exposures. */
@@ -284,25 +307,35 @@ FPHO_API int fpho_batch_free(fpho_batch *b);
 #define FPHO_NOALLOC_SCRATCH_BYTES (32u * 1024u * 1024u)
 
 /* Same computation as fpho_evaluate_proposal, for callers that cannot
- * allocate device memory: code running while a CUDA graph is captured,
- * plugins whose host framework owns every device allocation, services that
- * must not grow or fragment device memory after start-up.  It calls no
+ * allocate device memory: plugins whose host framework owns every device
+ * allocation (its allocator alone may take device memory, so that its
+ * accounting and limits hold), and services that must not grow or fragment
+ * device memory after start-up.  It calls no
  * cudaMalloc/cudaFree and no allocating library routine; its scratch (tile
  * plan, image Gaussians, per-tile partial sums) lives in a file-scope device
  * array of FPHO_NOALLOC_SCRATCH_BYTES.
  *   patch         host struct whose array pointers are DEVICE pointers
  *                 (residual may be NULL; if set, data - model is written there)
  *   n_bands, n_exp  band and exposure counts of the index arrays
- *   total_pixels  upper bound on the sum of exposure_N
+ *   total_pixels  length of the pixel arrays (data, ierr, xpix, ypix and
+ *                 residual); every exposure's run [exposure_start,
+ *                 exposure_start + exposure_N) must lie inside it
  *   max_psf_per_source  upper bound on n_psf_per_source[]
  *   dev_proposal, dev_chi2, dev_dchi2  device fpho_source[n_sources],
  *                 double[n_bands], float[n_bands][dchi2_stride]
  *   dev_status    optional device int: 0, or error bits (1 a bounded wait gave
- *                 up, 2 inconsistent index arrays, 4 a size bound was
- *                 exceeded, 8 a PSF radius bin out of range)
+ *                 up, 2 inconsistent index arrays -- bands overlapping, an
+ *                 exposure's pixels outside total_pixels, a negative
+ *                 psfgauss_start --, 4 a size bound was exceeded, 8 a PSF
+ *                 radius bin out of range).  On any error every dev_chi2
+ *                 entry is NaN, with or without dev_status.
+ * The psfgauss rows the exposures index (psfgauss_start[e] + component) must
+ * exist: the device array's length is not passed, so it cannot be checked.
  * Sizes whose scratch exceeds FPHO_NOALLOC_SCRATCH_BYTES are rejected with
  * FPHO_ERR_LIMIT.  The first call on a device looks up the array's address
- * and sets a kernel attribute: make it before any stream capture.  All calls
+ * and sets a kernel attribute (once, to the shared-memory ceiling): make it
+ * before any stream capture.  The address is kept until the process exits, so
+ * a device reset is not supported.  All calls
  * share the array, which keeps the last call's contents; calls that overlap
  * on the GPU race and must be serialized.  The call is asynchronous. */
 FPHO_API int fpho_evaluate_proposal_noalloc(const fpho_patch_struct *patch, int n_bands,
@@ -319,8 +352,14 @@ FPHO_API int fpho_patch_error_word(fpho_patch *p, int *out);
 /* ---- tuning (no counterpart in the reference) --------------------------- */
 
 /* Number of compiled tile-kernel variants; out[0] threads per CTA and out[1]
- * pixels per thread of `variant`. */
+ * tile pixels per thread of `variant`. */
 FPHO_API int fpho_variant_info(int variant, int out[2]);
+
+/* Number of compiled tile-kernel variants; out[0] threads per CTA, out[1]
+ * pixels per tile, out[2] warps that share each tile's image Gaussians (0:
+ * every thread evaluates its own pixels over all of them; NW > 0: NW warps
+ * each hold all of the tile's pixels and take 1/NW of its Gaussians). */
+FPHO_API int fpho_variant_shape(int variant, int out[3]);
 
 /* Select the tile-kernel variant and the shared-memory stage size (image
  * Gaussians per chunk) used by this patch; re-plans the tiles if the tile
@@ -334,6 +373,16 @@ FPHO_API int fpho_patch_set_config(fpho_patch *p, int variant, int live_cap, voi
  * Results are identical either way.  No reference counterpart (the
  * reference launches one block per band). */
 FPHO_API int fpho_patch_set_schedule(fpho_patch *p, int schedule);
+
+/* Exact-residual mode (a parity diagnostic; no reference counterpart).  With
+ * `on` non-zero the residual pass of this patch's evaluations follows the
+ * reference's ComputeResidualImage (forcepho/src/common_kernel.cc:57-83) in
+ * float operation by operation, each operation rounded once, with exp
+ * evaluated in double and rounded once to float; the gradient pass is
+ * unchanged.  Residuals then equal the reference CPU kernel's wherever its
+ * float exp is correctly rounded.  Slower than the default pass; compiled for
+ * variant 3 (64 threads x 4 pixels) only: FPHO_ERR_STATE for other variants. */
+FPHO_API int fpho_patch_set_exact_residual(fpho_patch *p, int on);
 
 /* For tests of the error path only (no reference counterpart): with `on`
  * non-zero, every staging wait of this patch's tile kernel expects 16 bytes
@@ -351,6 +400,32 @@ FPHO_API int fpho_patch_set_test_stall(fpho_patch *p, int on);
  * survive the per-tile culling; *last_count receives the count of the last
  * evaluation (synchronizes).  last_count may be NULL. */
 FPHO_API int fpho_patch_count_pairs(fpho_patch *p, int enable, long long *last_count);
+
+/* ---- linear flux solve ------------------------------------------------- */
+
+/* The weighted normal equations of the flux fit of the patch's sources at
+ * the shapes of `dev_proposal` (device fpho_source[n_sources]), per band:
+ * dev_ata[n_bands][n_sources][n_sources] = sum_pix ierr^2 X_s X_t and
+ * dev_atb[n_bands][n_sources] = sum_pix ierr^2 X_s data, where X_s is source
+ * s's model at unit flux and data the patch's device data.  Replaces the
+ * reference's design matrix and normal-equation products
+ * (forcepho/patches/device_patch.py:185-238, forcepho/fitting.py:573-594);
+ * X is never stored: each tile forms FP64 partial sums, reduced per band in
+ * a fixed order.  Asynchronous on `stream`. */
+FPHO_API int fpho_patch_flux_normal_equations(fpho_patch *p, const void *dev_proposal,
+                                              int n_sources, double *dev_ata, double *dev_atb,
+                                              void *stream);
+
+/* forcepho's optimize_fluxes (forcepho/fitting.py:597-627) on the device:
+ * the normal equations above, then per band an FP64 Cholesky solve.
+ * dev_flux[n_bands][n_sources] = ATA^-1 ATb (the maximum-likelihood fluxes
+ * given the shapes), dev_precision[n_bands][n_sources][n_sources] = ATA (the
+ * flux precision matrix), dev_status[n_bands] (optional): 0, or 1 where ATA
+ * is not positive definite (that band's fluxes are NaN; the reference
+ * raises LinAlgError).  At most 64 sources.  Asynchronous on `stream`. */
+FPHO_API int fpho_patch_optimize_fluxes(fpho_patch *p, const void *dev_proposal, int n_sources,
+                                        double *dev_flux, double *dev_precision,
+                                        int *dev_status, void *stream);
 
 /* Copy the image-Gaussian records that the last evaluation built for one
  * exposure to host memory (32 floats each: -xcen, -ycen, fxx, fxy, fyy, amp,

@@ -164,6 +164,43 @@ def _worker_f32_res(payload, proposal, band):
     return band, c.value, g.reshape(ns, 7), lo, res[lo:hi].copy()
 
 
+def _worker_res_dexp(payload, proposal, band, rounded_trig=0):
+    """(band, first pixel, residual of the band's pixels) of
+    fpo_residual_band_f32_dexp, in a worker process."""
+    L = lib()
+    vp, ip = ctypes.c_void_p, ctypes.c_int
+    L.fpo_residual_band_f32_dexp.argtypes = [ip, vp, vp, vp, ip]
+    L.fpo_residual_band_f32_dexp.restype = ip
+    arrays, ns, nr = _resolve(payload)
+    st = _struct_from_arrays(arrays, ns, nr)
+    prop = np.ascontiguousarray(proposal)
+    e0 = int(arrays["band_start"][band])
+    e1 = e0 + int(arrays["band_N"][band])
+    lo = int(arrays["exposure_start"][e0])
+    hi = int(arrays["exposure_start"][e1 - 1] + arrays["exposure_N"][e1 - 1])
+    res = np.zeros(hi, dtype=np.float32)
+    if L.fpo_residual_band_f32_dexp(band, st.ctypes.data, prop.ctypes.data, res.ctypes.data,
+                                    int(rounded_trig)):
+        raise MemoryError("oracle allocation failed")
+    return band, lo, res[lo:hi].copy()
+
+
+def residual_dexp_many(patch, proposal, pool, bands=None, payload=None, rounded_trig=False):
+    """The reference CPU kernel's residual image with a correctly rounded
+    float exp in place of the C library's expf (fpo_residual_band_f32_dexp),
+    and with `rounded_trig` correctly rounded cos/sin of the position angle
+    in place of cosf/sinf; bands spread over `pool`; NaN outside the bands
+    evaluated."""
+    payload = payload or _patch_payload(patch)
+    bands = range(patch.n_bands) if bands is None else bands
+    res = np.full(patch.npix, np.nan, dtype=np.float32)
+    prop = np.ascontiguousarray(proposal)
+    jobs = [(payload, prop, b, int(rounded_trig)) for b in bands]
+    for b, lo, r in pool.starmap(_worker_res_dexp, jobs):
+        res[lo:lo + len(r)] = r
+    return res
+
+
 def f32_residual_many(patch, proposal, pool, bands=None, payload=None):
     """The f32 oracle (bit-identical to the reference CPU kernel) with its
     residual image, bands spread over `pool`: chi2 (n_bands,), dchi2

@@ -89,9 +89,20 @@ def test_create_rejects_bad_radius_bin():
 
 
 def test_variants_listed():
+    """Classic shapes: whole warps, an even number of pixels per thread.
+    Gaussian-split shapes: NW warps that each hold the whole tile, an even
+    number of pixels per thread (32 K pixels per tile)."""
     from forcepho_b200 import _lib
     v = _lib.variants()
-    assert len(v) >= 4 and all(nt % 32 == 0 and k % 2 == 0 for nt, k in v)
+    shapes = _lib.variant_shapes()
+    assert len(v) >= 4 and len(shapes) == len(v)
+    for (nt, k), (nt2, tile, split) in zip(v, shapes):
+        assert nt == nt2 and nt % 32 == 0 and tile == nt * k
+        if split == 0:
+            assert k % 2 == 0
+        else:
+            assert nt == 32 * split and tile % 64 == 0
+    assert any(s > 0 for _, _, s in shapes)
 
 
 def test_store_and_device_pixel_create_reject_bad_arguments():

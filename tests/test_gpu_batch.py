@@ -68,3 +68,40 @@ def test_batch_graph_replay():
     batch.free()
     for P in patches:
         P.free()
+
+
+def test_every_batch_candidate_matches_oracle():
+    """Every configuration the batch autotuner can pick (tile variant with a
+    batched kernel, stage size, persistent-grid cap) gives chi2 and gradients
+    of every patch of a small uneven batch within the parity bars of the
+    reference CPU kernel (restated by the oracle), with the per-component
+    gradient bar of test_gpu_parity.grad_ok."""
+    from forcepho_b200.autotune import batch_candidates, time_batch
+    from forcepho_b200.batch import PatchBatch
+    from test_gpu_parity import CHI2_RTOL, grad_ok
+    patches = small_batch(5, seed=11)
+    for P in patches:
+        P.return_residual = False
+        P.send_to_device()
+    props = [P.proposal() for P in patches]
+    refs = []
+    for P, q in zip(patches, props):
+        c, g = O.oracle_evaluate(P, q, precision="f32")
+        _, mixed, scale, _, rscale = O.oracle_mixed_abs(P, q, terms=True)
+        refs.append((c, g, mixed, scale, rscale))
+    cands = batch_candidates()
+    assert len({c[0] for c in cands}) >= 3
+    for v, lc, ctas in cands:
+        b = PatchBatch(patches, live_cap=lc, variant=v, ctas_per_sm=ctas)
+        assert b.config == {"variant": v, "live_cap": lc, "ctas_per_sm": ctas}
+        chi2_b, dchi2_b = b.evaluate(props)
+        assert b.error_word() == 0
+        for (c, g, mixed, scale, rscale), cb, gb in zip(refs, chi2_b, dchi2_b):
+            np.testing.assert_allclose(cb, c, rtol=CHI2_RTOL)
+            ok = grad_ok(gb, g, mixed, scale, rscale)
+            assert np.all(ok), ((v, lc, ctas), int((~ok).sum()))
+        b.free()
+    # the timing used by the tuner runs on the same batch
+    assert time_batch(patches, cands[0][0], cands[0][1], cands[0][2], reps=2) > 0
+    for P in patches:
+        P.free()

@@ -124,14 +124,16 @@ def test_residual_matches_oracle():
     assert np.max(np.abs(res - r)) <= 1e-5 * scale
 
 
-@pytest.mark.parametrize("variant", range(8))
-def test_variants_agree(variant):
+@pytest.mark.parametrize("variant", range(16))
+@pytest.mark.parametrize("live_cap", [32, 160])
+def test_variants_agree(variant, live_cap):
+    """Every compiled tile shape (classic and Gaussian-split) against the
+    reference; live_cap 32 forces several staged chunks per tile."""
     from forcepho_b200 import _lib
     if variant >= len(_lib.variants()):
         pytest.skip("variant not compiled")
     P, prop, d = load_golden("mini_3src_2band")
-    nt = _lib.variants()[variant][0]
-    chi2, dchi2 = gpu_eval(P, prop, variant=variant, live_cap=max(nt, 128))
+    chi2, dchi2 = gpu_eval(P, prop, variant=variant, live_cap=live_cap)
     c64, g64 = O.oracle_evaluate(P, prop, precision="f64")
     cm, gm = O.oracle_evaluate(P, prop, precision="mixed")
     np.testing.assert_allclose(chi2, c64, rtol=CHI2_RTOL)
@@ -256,7 +258,31 @@ def test_image_gaussians_bitexact(name):
     assert n_exact == n_total
 
 
-@pytest.mark.parametrize("variant", [3, 6, 0])
+def test_field20_every_shape():
+    """The 20-source patch at full size through every compiled tile shape
+    (classic and Gaussian-split), one CTA per tile and persistent, against
+    the reference kernel by the per-component bar."""
+    from forcepho_b200 import _lib, synth
+    from forcepho_b200.proposal import GPUProposer
+    P = synth.make_workload("field20", seed=0)
+    prop = P.proposal()
+    rc, rd = O.ref_evaluate(P, prop)
+    _, mixed, scale, _, rscale = O.oracle_mixed_abs(P, prop, terms=True)
+    P.return_residual = False
+    P.send_to_device()
+    for v in range(len(_lib.variants())):
+        for sched in (0, 1):
+            P.device_patch.set_config(v, 160)
+            P.device_patch.set_schedule(sched)
+            for _ in range(2):   # the second persistent evaluation follows the first's costs
+                chi2, dchi2 = GPUProposer().evaluate_proposal(prop, patch=P)
+            np.testing.assert_allclose(chi2, rc, rtol=CHI2_RTOL)
+            ok = grad_ok(dchi2, rd, mixed, scale, rscale)
+            assert np.all(ok), (v, sched, int((~ok).sum()))
+    P.free()
+
+
+@pytest.mark.parametrize("variant", [3, 6, 0, 8, 10])
 def test_persistent_schedule_identical(variant):
     """The persistent schedule (tiles taken by decreasing cost of the previous
     evaluation, through an atomic counter) gives bit-identical chi2 and
