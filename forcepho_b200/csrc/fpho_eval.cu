@@ -119,9 +119,11 @@ __global__ void __launch_bounds__(NT) design_kernel(TileArgs A, float *X, long l
 }
 
 // Split tiles (tile_body_split): NW warps share each tile's Gaussians, K
-// pixels per thread, 32 K pixels per tile.  MINB > 1 asks the compiler for at
-// least MINB resident CTAs per SM (a register cap of 64K / (32 NW MINB)).
-template <int NW, int K, bool GRAD, int MINB = 1>
+// pixels per thread, 32 K pixels per tile.  MINB asks the compiler for at
+// least MINB resident CTAs per SM, a register cap of 64K / (32 NW MINB); the
+// default, 16 / NW, caps at 128 registers a thread (left free, the compiler
+// takes up to 180 and halves the resident warps).
+template <int NW, int K, bool GRAD, int MINB = 16 / NW>
 __global__ void __launch_bounds__(32 * NW, MINB) split_kernel(TileArgs A) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ uint64_t mbar;
@@ -134,7 +136,7 @@ __global__ void __launch_bounds__(32 * NW, MINB) split_kernel(TileArgs A) {
     tile_body_split<NW, K, GRAD>(A, blockIdx.x, smem, &mbar, phase);
 }
 
-template <int NW, int K, bool GRAD, int MINB = 1>
+template <int NW, int K, bool GRAD, int MINB = 16 / NW>
 __global__ void __launch_bounds__(32 * NW, MINB) split_kernel_dyn(TileArgs A, const int *order,
                                                                   int n_tiles, int *counter) {
     extern __shared__ __align__(128) unsigned char smem[];

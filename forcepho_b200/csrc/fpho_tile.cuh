@@ -223,7 +223,9 @@ __device__ __forceinline__ void residual_pairs(const v2 (&X)[KP], const v2 (&Y)[
 // b's, exactly as two calls of residual_pairs in order would.  The
 // exp-argument cut is applied to both; for a Gaussian without FLAG_CUT no
 // weighted pixel of the tile reaches 36 (and with a residual output every
-// pixel is in the tile box), so the cut changes nothing there.
+// pixel is in the tile box), so the cut changes nothing there.  (Skipping the
+// cut for pairs without FLAG_CUT, as a compile-time branch, measured slower:
+// it raised the split kernel's registers from 128 to 180.)
 template <int KP>
 __device__ __forceinline__ void residual_pairs2(const v2 (&X)[KP], const v2 (&Y)[KP], v2 (&R)[KP],
                                                 const float *ra, const float *rb, v2 CM24,
@@ -304,9 +306,14 @@ __device__ __forceinline__ void residual_exact(const v2 (&X)[KP], const v2 (&Y)[
 }
 
 // Pass 2 for one Gaussian over the thread's KP pixel pairs: the twelve sums
-// from which the model's derivatives w.r.t. (A, x, y, fxx, fyy, fxy) follow.
+// from which the model's derivatives w.r.t. (A, x, y, fxx, fyy, fxy) follow
+// (W = -2 r ie^2 G, H the pixel-integral correction, d = pixel - centre,
+// v = F d): sum W H, sum W H v, sum W v, sum W H d d^T, sum W, and sum W d d^T.
+// The epilogue forms sum W d.v terms from sum W d d^T and F once per
+// Gaussian (d_x v_x = fxx dx^2 + fxy dx dy, and so on), which is one packed
+// instruction per pixel pair cheaper than summing them per pixel.
 struct GradSums {
-    v2 A, HVx, HVy, Vx, Vy, HXX, HXY, HYY, W, T1, T2, T3;
+    v2 A, HVx, HVy, Vx, Vy, HXX, HXY, HYY, W, WXX, WXY, WYY;
 };
 template <int KP, bool CUT>
 __device__ __forceinline__ void gradient_pairs(const v2 (&X)[KP], const v2 (&Y)[KP],
@@ -344,9 +351,10 @@ __device__ __forceinline__ void gradient_pairs(const v2 (&X)[KP], const v2 (&Y)[
         s.HXY = fma2(HDX, DY, s.HXY);
         s.HYY = fma2(mul2(WH, DY), DY, s.HYY);
         s.W = add2(s.W, W);
-        s.T1 = fma2(W, T1, s.T1);
-        s.T2 = fma2(W, mul2(DY, VY), s.T2);
-        s.T3 = fma2(W, fma2(DX, VY, mul2(DY, VX)), s.T3);
+        const v2 WDX = mul2(W, DX);
+        s.WXX = fma2(WDX, DX, s.WXX);
+        s.WXY = fma2(WDX, DY, s.WXY);
+        s.WYY = fma2(mul2(W, DY), DY, s.WYY);
     }
 }
 
@@ -412,12 +420,13 @@ __device__ __forceinline__ void gradient_pairs2(const v2 (&X)[KP], const v2 (&Y)
         sb.HYY = fma2(mul2(WHb, DYb), DYb, sb.HYY);
         sa.W = add2(sa.W, Wa);
         sb.W = add2(sb.W, Wb);
-        sa.T1 = fma2(Wa, T1a, sa.T1);
-        sb.T1 = fma2(Wb, T1b, sb.T1);
-        sa.T2 = fma2(Wa, mul2(DYa, VYa), sa.T2);
-        sb.T2 = fma2(Wb, mul2(DYb, VYb), sb.T2);
-        sa.T3 = fma2(Wa, fma2(DXa, VYa, mul2(DYa, VXa)), sa.T3);
-        sb.T3 = fma2(Wb, fma2(DXb, VYb, mul2(DYb, VXb)), sb.T3);
+        const v2 WDXa = mul2(Wa, DXa), WDXb = mul2(Wb, DXb);
+        sa.WXX = fma2(WDXa, DXa, sa.WXX);
+        sb.WXX = fma2(WDXb, DXb, sb.WXX);
+        sa.WXY = fma2(WDXa, DYa, sa.WXY);
+        sb.WXY = fma2(WDXb, DYb, sb.WXY);
+        sa.WYY = fma2(mul2(Wa, DYa), DYa, sa.WYY);
+        sb.WYY = fma2(mul2(Wb, DYb), DYb, sb.WYY);
     }
 }
 
@@ -647,11 +656,16 @@ __device__ __forceinline__ void tile_body(const TileArgs &A, int tile, unsigned 
                 const float gA = lanesum(s.A);
                 const float gx = lanesum(s.HVx) - (fxx * sVx + fxy * sVy) * (1.0f / 12.0f);
                 const float gy = lanesum(s.HVy) - (fxy * sVx + fyy * sVy) * (1.0f / 12.0f);
-                const float gfxx = lanesum(s.T1) * (1.0f / 12.0f) - 0.5f * lanesum(s.HXX) -
+                // sum W d.v terms from sum W d d^T: dx vx, dy vy, dx vy + dy vx
+                const float wxx = lanesum(s.WXX), wxy = lanesum(s.WXY), wyy = lanesum(s.WYY);
+                const float t1 = fxx * wxx + fxy * wxy;
+                const float t2 = fyy * wyy + fxy * wxy;
+                const float t3 = fxy * (wxx + wyy) + (fxx + fyy) * wxy;
+                const float gfxx = t1 * (1.0f / 12.0f) - 0.5f * lanesum(s.HXX) -
                                    sW * (1.0f / 24.0f);
-                const float gfyy = lanesum(s.T2) * (1.0f / 12.0f) - 0.5f * lanesum(s.HYY) -
+                const float gfyy = t2 * (1.0f / 12.0f) - 0.5f * lanesum(s.HYY) -
                                    sW * (1.0f / 24.0f);
-                const float gfxy = lanesum(s.T3) * (1.0f / 12.0f) - lanesum(s.HXY);
+                const float gfxy = t3 * (1.0f / 12.0f) - lanesum(s.HXY);
                 const float4 j0 = rj[0], j1 = rj[1], j2 = rj[2], j3 = rj[3];
                 P[0] = fmaf(j0.x, gA, P[0]);
                 P[1] = fmaf(j1.z, gy, fmaf(j1.y, gx, P[1]));
@@ -910,11 +924,16 @@ __device__ __forceinline__ void tile_body_split(const TileArgs &A, int tile, uns
                 const float gA = lanesum(s.A);
                 const float gx = lanesum(s.HVx) - (fxx * sVx + fxy * sVy) * (1.0f / 12.0f);
                 const float gy = lanesum(s.HVy) - (fxy * sVx + fyy * sVy) * (1.0f / 12.0f);
-                const float gfxx = lanesum(s.T1) * (1.0f / 12.0f) - 0.5f * lanesum(s.HXX) -
+                // sum W d.v terms from sum W d d^T: dx vx, dy vy, dx vy + dy vx
+                const float wxx = lanesum(s.WXX), wxy = lanesum(s.WXY), wyy = lanesum(s.WYY);
+                const float t1 = fxx * wxx + fxy * wxy;
+                const float t2 = fyy * wyy + fxy * wxy;
+                const float t3 = fxy * (wxx + wyy) + (fxx + fyy) * wxy;
+                const float gfxx = t1 * (1.0f / 12.0f) - 0.5f * lanesum(s.HXX) -
                                    sW * (1.0f / 24.0f);
-                const float gfyy = lanesum(s.T2) * (1.0f / 12.0f) - 0.5f * lanesum(s.HYY) -
+                const float gfyy = t2 * (1.0f / 12.0f) - 0.5f * lanesum(s.HYY) -
                                    sW * (1.0f / 24.0f);
-                const float gfxy = lanesum(s.T3) * (1.0f / 12.0f) - lanesum(s.HXY);
+                const float gfxy = t3 * (1.0f / 12.0f) - lanesum(s.HXY);
                 const float4 j0 = rj[0], j1 = rj[1], j2 = rj[2], j3 = rj[3];
                 P[0] = fmaf(j0.x, gA, P[0]);
                 P[1] = fmaf(j1.z, gy, fmaf(j1.y, gx, P[1]));

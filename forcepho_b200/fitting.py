@@ -144,9 +144,10 @@ def run_hmc(model, q, n_draws, warmup=(10,), n_chains=1, n_leapfrog=10, step_siz
     q : starting position in the constrained space, one chain's (broadcast
         to every chain) or all chains' concatenated
     n_draws : samples kept per chain
-    warmup : lengths of the tuning rounds; after each, the step size is
-        multiplied by exp(2 (acceptance - target_accept)), clipped to
-        [1/4, 4] per round
+    warmup : lengths of the tuning rounds; in each the step size adapts
+        every iteration by dual averaging towards `target_accept` (the
+        chains' mean acceptance probability), and the averaged value is kept
+        at the end of the round
     n_chains : chains of a DevicePosterior model (ignored for a batch)
     z_cov : the inverse mass matrix in the unconstrained coordinates z, as
         the reference's ``z_cov``: a vector of variances (one chain's, or all
@@ -202,26 +203,25 @@ def run_hmc(model, q, n_draws, warmup=(10,), n_chains=1, n_leapfrog=10, step_siz
             zc = zc.reshape(-1)
             hmc.set_mass(scale=(zc.repeat(n_chains) if zc.numel() == d else zc).sqrt())
     hmc.set_state(z0)
-    eps = float(step_size)
     t0 = time.time()
     for w in warmup:
         hmc.n_accept.zero_()
         hmc.slot.zero_()
+        hmc.start_adaptation(target_accept)
         hmc.run(int(w))
-        acc = float(np.mean(hmc.acceptance(int(w))))
-        eps *= float(np.clip(np.exp(2.0 * (acc - target_accept)), 0.25, 4.0))
+        hmc.stop_adaptation()
         if adapt and int(w) >= 10:
             est = estimate_mass(hmc.samples[:int(w)], n_chains, full=full, pooled=pooled)
-            # the step size in whitened units: rescale by the change of the
-            # typical inverse-mass scale so the next round starts comparably
+            # the step size is in whitened units: rescale it by the change of
+            # the typical inverse-mass scale so the next round starts comparably
             old = hmc.chol.diagonal(dim1=1, dim2=2) if full else hmc.scale
             new = est.diagonal(dim1=1, dim2=2) if full else est
-            eps *= float(torch.exp(torch.log(old).mean() - torch.log(new).mean()))
+            hmc.set_eps(hmc.eps * float(torch.exp(torch.log(old).mean() -
+                                                  torch.log(new).mean())))
             if full:
                 hmc.set_mass(chol=est)
             else:
                 hmc.set_mass(scale=est)
-        hmc.set_eps(eps)
     hmc.n_accept.zero_()
     hmc.slot.zero_()
     hmc.run(int(n_draws))

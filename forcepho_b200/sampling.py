@@ -21,6 +21,12 @@ factor per chain (``chol``).  The leapfrog runs in whitened momenta u = L^T p
 with unit kinetic energy: u += eps/2 L^T grad, z += eps L u, which is HMC with
 mass M = (L L^T)^-1 in z.  :func:`estimate_mass` turns warm-up samples into
 the factors (regularised towards the identity as Stan does).
+
+Step size.  During warm-up the step size adapts inside the captured
+iteration by dual averaging (Hoffman & Gelman 2014, the NUTS paper's
+Algorithm 5) towards a target mean acceptance probability over the chains;
+:meth:`MultiChainHMC.start_adaptation` / :meth:`stop_adaptation` switch it on
+and off without re-capturing, and stopping fixes the averaged step size.
 """
 
 import torch
@@ -123,8 +129,48 @@ class MultiChainHMC:
                 raise ValueError("a full mass matrix needs chains of equal size")
             d = n // k
             self.chol = torch.eye(d, **f64).repeat(k, 1, 1)
+        # dual-averaging state (device scalars, so the captured graph adapts)
+        self.da_on = torch.zeros((), **f64)        # 1 while adapting
+        self.da_m = torch.zeros((), **f64)         # adaptation iterations
+        self.da_hbar = torch.zeros((), **f64)
+        self.da_mu = torch.zeros((), **f64)
+        self.da_logbar = torch.zeros((), **f64)
+        self.da_target = torch.full((), 0.8, **f64)
+        self.mean_accept_prob = torch.zeros((), **f64)
         self.graph = None
         torch.cuda.manual_seed(seed)
+
+    # dual-averaging constants (gamma, t0, kappa of Hoffman & Gelman 2014)
+    DA_GAMMA, DA_T0, DA_KAPPA = 0.05, 10.0, 0.75
+
+    def start_adaptation(self, target_accept=0.8):
+        """Adapt the step size from the next iteration on, starting from the
+        current one (mu = log(10 eps))."""
+        self.da_on.fill_(1.0)
+        self.da_m.zero_()
+        self.da_hbar.zero_()
+        self.da_mu.copy_(torch.log(10.0 * self.eps_t))
+        self.da_logbar.copy_(torch.log(self.eps_t))
+        self.da_target.fill_(float(target_accept))
+
+    def stop_adaptation(self):
+        """Stop adapting and keep the averaged step size."""
+        self.da_on.zero_()
+        self.eps_t.copy_(torch.exp(self.da_logbar))
+
+    def _adapt(self, accept_prob):
+        """One dual-averaging update from this iteration's mean acceptance
+        probability (no effect while da_on is 0)."""
+        f = self.da_on
+        m = self.da_m + f
+        eta = 1.0 / (m + self.DA_T0)
+        self.da_hbar.copy_((1.0 - f * eta) * self.da_hbar + f * eta * (self.da_target - accept_prob))
+        log_eps = self.da_mu - torch.sqrt(m) / self.DA_GAMMA * self.da_hbar
+        w = torch.pow(torch.clamp(m, min=1.0), -self.DA_KAPPA)
+        self.da_logbar.copy_(f * (w * log_eps + (1.0 - w) * self.da_logbar) +
+                             (1.0 - f) * self.da_logbar)
+        self.eps_t.copy_(f * torch.exp(log_eps) + (1.0 - f) * self.eps_t)
+        self.da_m.copy_(m)
 
     def set_mass(self, scale=None, chol=None):
         """Inverse mass matrix: per-coordinate standard deviations `scale`
@@ -187,6 +233,11 @@ class MultiChainHMC:
         lnp1 = post.lnp_per_patch(z)
         kin1 = _per_patch(post, p * p) * 0.5
         log_ratio = (lnp1 - kin1) - (self.lnp - kin0)
+        ok = torch.isfinite(log_ratio)
+        prob = torch.where(ok, torch.exp(torch.clamp(torch.nan_to_num(log_ratio), max=0.0)),
+                           torch.zeros_like(log_ratio))
+        self.mean_accept_prob.copy_(prob.mean())
+        self._adapt(self.mean_accept_prob)
         u = torch.rand(self.lnp.shape, dtype=torch.float64, device="cuda")
         acc = (torch.log(u) < log_ratio) & torch.isfinite(lnp1)
         accp = acc[post.par_patch]

@@ -40,6 +40,6 @@ def test_stall_refused_where_unsafe():
     from forcepho_b200 import _lib, synth
     P = synth.make_workload("field20", seed=0)
     P.send_to_device()
-    with pytest.raises(_lib.FphoError):      # 900 Gaussians per exposure > 160 records
+    with pytest.raises(_lib.FphoError):      # 900 Gaussians per exposure > one stage
         _lib.call("fpho_patch_set_test_stall", P.device_patch.handle, 1)
     P.free()
