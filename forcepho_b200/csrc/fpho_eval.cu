@@ -207,6 +207,7 @@ static const Variant kVariants[] = {
     FPHO_VARIANT(256, 4), FPHO_VARIANT(128, 8), FPHO_VARIANT(64, 8), FPHO_VARIANT(32, 8),
     FPHO_SPLIT(4, 8, 64, 4), FPHO_SPLIT(2, 8, 64, 4), FPHO_SPLIT(8, 8, 64, 4),
     FPHO_SPLIT(4, 4, 32, 4), FPHO_SPLIT_MINB(4, 8, 5, 64, 4),
+    FPHO_SPLIT_MINB(4, 6, 5, 32, 6),  // 192-pixel tiles, 95 registers: 5 CTAs per SM
 };
 #undef FPHO_VARIANT
 #undef FPHO_VARIANT_EXACT

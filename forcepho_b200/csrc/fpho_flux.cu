@@ -249,13 +249,14 @@ struct NormalShape {
 };
 const NormalShape kNormalShapes[] = {
     {128, 32, (const void *)normal_tiles<32, 4>},
+    {192, 32, (const void *)normal_tiles<32, 6>},
     {256, 64, (const void *)normal_tiles<64, 4>},
     {512, 128, (const void *)normal_tiles<128, 4>},
     {1024, 256, (const void *)normal_tiles<256, 4>},
 };
 
 std::mutex g_norm_mu;
-size_t g_norm_attr[64][4];
+size_t g_norm_attr[64][8];
 
 }  // namespace
 }  // namespace fpho
@@ -276,8 +277,9 @@ static int enqueue_normal(fpho_patch *p, const fpho_source *d_prop, double *d_at
     const int ns = p->n_sources;
     const int n_terms = ns * (ns + 1) / 2 + ns;
     const int tile = variant_tile_pixels(p->variant);
+    constexpr int n_shapes = sizeof(kNormalShapes) / sizeof(kNormalShapes[0]);
     int shape = -1;
-    for (int i = 0; i < 4; ++i)
+    for (int i = 0; i < n_shapes; ++i)
         if (kNormalShapes[i].tile == tile) shape = i;
     if (shape < 0)
         return set_error(FPHO_ERR_STATE, "no normal-equation kernel for %d-pixel tiles", tile);

@@ -190,13 +190,15 @@ def run_hmc(model, q, n_draws, warmup=(10,), n_chains=1, n_leapfrog=10, step_siz
         q = np.tile(q, n_chains)
     if q.size != post.ndim:
         raise ValueError(f"q has {q.size} entries; the chains need {post.ndim}")
-    z0 = post.inverse_transform(torch.as_tensor(q, device="cuda"))
+    device = getattr(post, "device", "cuda")
+    z0 = post.inverse_transform(torch.as_tensor(q, device=device))
     n_buf = max([int(n_draws)] + [int(w) for w in warmup])
     hmc = MultiChainHMC(post, step_size, n_leapfrog, n_samples=n_buf,
-                        seed=int(random_seed) & 0x7FFFFFFF, jitter=jitter, full=full)
+                        seed=int(random_seed) & 0x7FFFFFFF, jitter=jitter, full=full,
+                        device=device)
     d = post.ndim // n_chains
     if z_cov is not None:
-        zc = torch.as_tensor(np.asarray(z_cov, dtype=np.float64), device="cuda")
+        zc = torch.as_tensor(np.asarray(z_cov, dtype=np.float64), device=device)
         if full:
             hmc.set_mass(chol=torch.linalg.cholesky(zc.reshape(d, d)))
         else:
@@ -225,7 +227,8 @@ def run_hmc(model, q, n_draws, warmup=(10,), n_chains=1, n_leapfrog=10, step_siz
     hmc.n_accept.zero_()
     hmc.slot.zero_()
     hmc.run(int(n_draws))
-    torch.cuda.synchronize()
+    if hmc.device.type == "cuda":
+        torch.cuda.synchronize()
     wall = time.time() - t0
     zs = hmc.samples[:int(n_draws)]  # the ring buffer started at slot 0 for the draws
     qs = post.transform(zs).cpu().numpy().reshape(int(n_draws), n_chains, -1)

@@ -105,21 +105,23 @@ class MultiChainHMC:
     """
 
     def __init__(self, posterior, eps, n_leapfrog, n_samples=0, seed=0, jitter=0.2,
-                 full=False):
+                 full=False, device="cuda"):
         self.post = posterior
+        self.device = torch.device(device)
+        dev = self.device
         # the step size lives on the device, so a captured iteration reads the
         # current value (set_eps between replays tunes it)
-        self.eps_t = torch.full((), float(eps), dtype=torch.float64, device="cuda")
+        self.eps_t = torch.full((), float(eps), dtype=torch.float64, device=dev)
         self.jitter = float(jitter)
         self.L = int(n_leapfrog)
         n, k = posterior.ndim, posterior.n_patches
-        f64 = dict(dtype=torch.float64, device="cuda")
+        f64 = dict(dtype=torch.float64, device=dev)
         self.z, self.g = torch.zeros(n, **f64), torch.zeros(n, **f64)
         self.lnp = torch.zeros(k, **f64)
-        self.n_accept = torch.zeros(k, dtype=torch.int64, device="cuda")
+        self.n_accept = torch.zeros(k, dtype=torch.int64, device=dev)
         self.n_samples = int(n_samples)
         self.samples = torch.zeros((max(self.n_samples, 1), n), **f64)
-        self.slot = torch.zeros(1, dtype=torch.int64, device="cuda")
+        self.slot = torch.zeros(1, dtype=torch.int64, device=dev)
         # inverse-mass factors, read by the captured graph: set_mass copies into them
         self.scale = torch.ones(n, **f64)
         self.full = bool(full)
@@ -138,7 +140,10 @@ class MultiChainHMC:
         self.da_target = torch.full((), 0.8, **f64)
         self.mean_accept_prob = torch.zeros((), **f64)
         self.graph = None
-        torch.cuda.manual_seed(seed)
+        if dev.type == "cuda":
+            torch.cuda.manual_seed(seed)
+        else:
+            torch.manual_seed(seed)
 
     # dual-averaging constants (gamma, t0, kappa of Hoffman & Gelman 2014)
     DA_GAMMA, DA_T0, DA_KAPPA = 0.05, 10.0, 0.75
@@ -182,7 +187,7 @@ class MultiChainHMC:
         if chol is not None:
             if self.chol is None:
                 raise ValueError("the sampler was made without a full mass matrix")
-            c = torch.as_tensor(chol, dtype=torch.float64, device="cuda")
+            c = torch.as_tensor(chol, dtype=torch.float64, device=self.device)
             self.chol.copy_(c.expand_as(self.chol))
 
     def _to_z(self, u):
@@ -217,10 +222,10 @@ class MultiChainHMC:
         post = self.post
         # a step size per chain, drawn uniformly within +-jitter of eps, so that
         # a fixed trajectory length cannot lock onto a period of the dynamics
-        u = torch.rand(self.lnp.shape, dtype=torch.float64, device="cuda")
+        u = torch.rand(self.lnp.shape, dtype=torch.float64, device=self.device)
         eps = (self.eps_t * (1.0 + self.jitter * (2.0 * u - 1.0)))[post.par_patch]
         h = 0.5 * eps
-        p = torch.randn(self.z.shape, dtype=torch.float64, device="cuda")  # whitened momenta
+        p = torch.randn(self.z.shape, dtype=torch.float64, device=self.device)  # whitened momenta
         kin0 = _per_patch(post, p * p) * 0.5
         z, g = self.z.clone(), self.g.clone()
         gu = self._to_u(g)
@@ -238,7 +243,7 @@ class MultiChainHMC:
                            torch.zeros_like(log_ratio))
         self.mean_accept_prob.copy_(prob.mean())
         self._adapt(self.mean_accept_prob)
-        u = torch.rand(self.lnp.shape, dtype=torch.float64, device="cuda")
+        u = torch.rand(self.lnp.shape, dtype=torch.float64, device=self.device)
         acc = (torch.log(u) < log_ratio) & torch.isfinite(lnp1)
         accp = acc[post.par_patch]
         self.z.copy_(torch.where(accp, z, self.z))
@@ -266,8 +271,9 @@ class MultiChainHMC:
 
     def run(self, n_iter, use_graph=True):
         """Advance every chain by `n_iter` HMC iterations (enqueued on the
-        current stream, not synchronized)."""
-        if not use_graph:
+        current stream, not synchronized; one CUDA graph replay per iteration
+        on a GPU, plain eager iterations on the CPU)."""
+        if not use_graph or self.device.type != "cuda":
             for _ in range(n_iter):
                 self._iteration()
             return

@@ -97,9 +97,9 @@ def test_variants_listed():
     shapes = _lib.variant_shapes()
     assert len(v) >= 4 and len(shapes) == len(v)
     for (nt, k), (nt2, tile, split) in zip(v, shapes):
-        assert nt == nt2 and nt % 32 == 0 and tile == nt * k
+        assert nt == nt2 and nt % 32 == 0 and k == tile // nt
         if split == 0:
-            assert k % 2 == 0
+            assert k % 2 == 0 and tile == nt * k
         else:
             assert nt == 32 * split and tile % 64 == 0
     assert any(s > 0 for _, _, s in shapes)
