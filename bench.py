@@ -47,9 +47,9 @@ METRIC = "chi2+grad evals/s & pixÂ·gauss/s: batched vs plain, 1 B200, rel err â‰
 FLOPS_PER_PAIR = 105          # 18 (model) + 87 (gradient) FP32 flops, FMA = 2
 WORKLOAD = "field20: 20 src, 8 bands x 4 exp x 128x128 px, 5-gauss PSF, 9 radii"
 # DRAM bytes (read + write) of one tile-kernel launch on this workload, from an
-# ncu capture of one launch: the 16 B per pixel of the pixel arrays plus the
-# image-Gaussian table, each read once.
-TILE_TRAFFIC_BYTES = 12673536
+# ncu capture of one launch of the split tile kernel: the 16 B per pixel of the
+# pixel arrays plus the image-Gaussian table, each read once.
+TILE_TRAFFIC_BYTES = 12675584
 # DRAM bytes of one store_copy launch packing a 471 k-pixel patch (ncu:
 # throughput x duration of one launch).
 STORE_COPY_TRAFFIC_BYTES = 3833600

@@ -78,7 +78,9 @@ def test_noalloc_matches_handle_path_twice(name):
         assert int(status.item()) == 0
         c = chi2.cpu().numpy()
         g = dchi2.cpu().numpy().reshape(nb, ns, 7)
-        np.testing.assert_allclose(c, chi2_a, rtol=1e-9)
+        # the handle path's default tile shape sums in a different order: the
+        # parity tolerances of the tests (chi2 1e-6, gradient 1e-5)
+        np.testing.assert_allclose(c, chi2_a, rtol=CHI2_RTOL)
         np.testing.assert_allclose(g, dchi2_a, rtol=1e-5,
                                    atol=1e-6 * float(np.abs(dchi2_a).max()))
         # against the reference CPU kernel's outputs (golden), by the parity bar
