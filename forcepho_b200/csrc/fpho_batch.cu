@@ -61,10 +61,11 @@ __global__ void batch_gaussians(const BatchPatch *bps, const int2 *expmap,
 }
 
 // SPLIT = 0: tile_body with NT threads x K pixels per tile; SPLIT = NW:
-// tile_body_split with NW warps (NT = 32 NW) and K pixels per thread.
-template <int NT, int K, int SPLIT>
-__global__ void __launch_bounds__(NT) batch_tiles(const TileArgs *args, const int2 *work,
-                                                  int n_work, int *counter) {
+// tile_body_split with NW warps (NT = 32 NW) and K pixels per thread.  MINB:
+// the minimum resident CTAs per SM asked of the compiler (a register cap).
+template <int NT, int K, int SPLIT, int MINB = 1>
+__global__ void __launch_bounds__(NT, MINB) batch_tiles(const TileArgs *args, const int2 *work,
+                                                        int n_work, int *counter) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ uint64_t mbar;
     __shared__ int s_item;
@@ -114,20 +115,30 @@ struct BatchShape {
     const void *fn;
 };
 const BatchShape kBatchShapes[] = {
-    {64, 512, 0, (const void *)batch_tiles<64, 8, 0>},    // default: 64 threads x 8 pixels
-    {64, 256, 0, (const void *)batch_tiles<64, 4, 0>},
-    {128, 512, 0, (const void *)batch_tiles<128, 4, 0>},
-    {128, 256, 4, (const void *)batch_tiles<128, 8, 4>},  // 4 warps share 256-pixel tiles
-    {64, 256, 2, (const void *)batch_tiles<64, 8, 2>},    // 2 warps share 256-pixel tiles
+    // registers capped at 128 a thread (MINB = 65536 / (128 NT))
+    {64, 512, 0, (const void *)batch_tiles<64, 8, 0, 8>},    // default: 64 threads x 8 pixels
+    {64, 256, 0, (const void *)batch_tiles<64, 4, 0, 8>},
+    {128, 512, 0, (const void *)batch_tiles<128, 4, 0, 4>},
+    // split tiles with the registers capped at 128 (left free, the compiler
+    // takes 156 and fewer CTAs fit), and at 96 for 5 CTAs per SM
+    {128, 256, 4, (const void *)batch_tiles<128, 8, 4, 4>},  // 4 warps share 256-pixel tiles
+    {64, 256, 2, (const void *)batch_tiles<64, 8, 2, 8>},    // 2 warps share 256-pixel tiles
+    {128, 256, 4, (const void *)batch_tiles<128, 8, 4, 5>},  // 4 warps, 5 CTAs per SM
 };
 constexpr int kNumBatchShapes = sizeof(kBatchShapes) / sizeof(kBatchShapes[0]);
 
-// the patch variant planned like batch shape `i`, or -1 if none is compiled
+// the patch variant planned like batch shape `i` (the k-th shape of a given
+// (threads, tile, split) maps to the k-th patch variant of it: the register
+// cap is the only difference between such shapes), or -1 if none is compiled
 int shape_variant(int i) {
     const BatchShape &B = kBatchShapes[i];
+    int rank = 0;
+    for (int j = 0; j < i; ++j)
+        rank += kBatchShapes[j].nt == B.nt && kBatchShapes[j].tile == B.tile &&
+                kBatchShapes[j].split == B.split;
     for (int v = 0; v < variant_count(); ++v)
         if (variant_threads(v) == B.nt && variant_tile_pixels(v) == B.tile &&
-            variant_split(v) == B.split)
+            variant_split(v) == B.split && rank-- == 0)
             return v;
     return -1;
 }

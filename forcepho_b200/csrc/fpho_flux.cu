@@ -242,17 +242,19 @@ __global__ void __launch_bounds__(64) normal_solve(const double *ata, const doub
         flux[(size_t)b * ns + i] = bad ? __longlong_as_double(0x7ff8000000000000ll) : z[i];
 }
 
-// the normal-equation kernel for a plan's tile size
+// the normal-equation kernel for a plan's tile size: two pixels per thread,
+// so that a tile has as many warps as fit (the per-pixel work is light and the
+// FP64 partial sums spread over all threads)
 struct NormalShape {
     int tile, nt;
     const void *fn;
 };
 const NormalShape kNormalShapes[] = {
-    {128, 32, (const void *)normal_tiles<32, 4>},
-    {192, 32, (const void *)normal_tiles<32, 6>},
-    {256, 64, (const void *)normal_tiles<64, 4>},
-    {512, 128, (const void *)normal_tiles<128, 4>},
-    {1024, 256, (const void *)normal_tiles<256, 4>},
+    {128, 64, (const void *)normal_tiles<64, 2>},
+    {192, 96, (const void *)normal_tiles<96, 2>},
+    {256, 128, (const void *)normal_tiles<128, 2>},
+    {512, 256, (const void *)normal_tiles<256, 2>},
+    {1024, 512, (const void *)normal_tiles<512, 2>},
 };
 
 std::mutex g_norm_mu;
