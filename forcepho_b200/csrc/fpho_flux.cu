@@ -122,19 +122,16 @@ __global__ void __launch_bounds__(NT) normal_tiles(TileArgs A, double *pnorm, in
         phase ^= 1u;
         for (int i = 0; i < n; ++i) {
             const float *r = recs + (size_t)i * GSTAGE;
-            v2 NXC, NYC, FXX, FXY, FYY, AMP, HB, C0;
-            ld2(r + R_NXC, NXC, NYC);
-            ld2(r + R_FXX, FXX, FXY);
-            ld2(r + R_FYY, FYY, AMP);
-            ld2(r + R_HB, HB, C0);
-            const v2 UA = pk1(r[R_JA_FLUX]);  // dA/dflux in place of amp
-            const v2 HA = mul2(UA, CM24);
-            const v2 UB = mul2(pk1(-1.0f), mul2(UA, C0));
-            const int flag = kept[c0 + i];
-            if (flag & FLAG_CUT)
-                residual_pairs<KP, true>(Xp, Yp, M, NXC, NYC, FXX, FXY, FYY, HA, UB, KEXP2, KEXPLO2);
-            else
-                residual_pairs<KP, false>(Xp, Yp, M, NXC, NYC, FXX, FXY, FYY, HA, UB, KEXP2, KEXPLO2);
+            int flag = kept[c0 + i];
+            if (!(flag & FLAG_LAST_SRC) && i + 1 < n) {
+                // two Gaussians of the same source: their exponentials interleave
+                design_pairs2<KP>(Xp, Yp, M, r, r + GSTAGE, CM24, KEXP2, KEXPLO2);
+                ++i;
+                r += GSTAGE;
+                flag = kept[c0 + i];
+            } else {
+                design_one<KP>(Xp, Yp, M, r, flag, CM24, KEXP2, KEXPLO2);
+            }
             if ((flag & FLAG_LAST_SRC) || i == n - 1) {
                 // a source's Gaussians are contiguous in the kept list; one
                 // that spans two chunks is flushed twice and added
@@ -242,20 +239,23 @@ __global__ void __launch_bounds__(64) normal_solve(const double *ata, const doub
         flux[(size_t)b * ns + i] = bad ? __longlong_as_double(0x7ff8000000000000ll) : z[i];
 }
 
-// the normal-equation kernel for a plan's tile size: two pixels per thread,
-// so that a tile has as many warps as fit (the per-pixel work is light and the
-// FP64 partial sums spread over all threads)
+// the normal-equation kernel for a plan's tile size: four pixels per thread
+// (two pixel pairs, two Gaussians interleaved: four independent exponential
+// chains); whole warps, so the 192-pixel tile takes six pixels per thread
 struct NormalShape {
     int tile, nt;
     const void *fn;
 };
 const NormalShape kNormalShapes[] = {
-    {128, 64, (const void *)normal_tiles<64, 2>},
-    {192, 96, (const void *)normal_tiles<96, 2>},
-    {256, 128, (const void *)normal_tiles<128, 2>},
-    {512, 256, (const void *)normal_tiles<256, 2>},
-    {1024, 512, (const void *)normal_tiles<512, 2>},
+    {128, 32, (const void *)normal_tiles<32, 4>},
+    {192, 32, (const void *)normal_tiles<32, 6>},
+    {256, 64, (const void *)normal_tiles<64, 4>},
+    {512, 128, (const void *)normal_tiles<128, 4>},
+    {1024, 256, (const void *)normal_tiles<256, 4>},
 };
+// records per shared-memory stage of the flux kernel: the design pass stages
+// each chunk once, so a small stage costs little and lets more CTAs reside
+constexpr int NORMAL_LIVE_CAP = 64;
 
 std::mutex g_norm_mu;
 size_t g_norm_attr[64][8];
@@ -287,7 +287,8 @@ static int enqueue_normal(fpho_patch *p, const fpho_source *d_prop, double *d_at
         return set_error(FPHO_ERR_STATE, "no normal-equation kernel for %d-pixel tiles", tile);
     const NormalShape &S = kNormalShapes[shape];
     const int idx_cap = std::max(p->max_g, 1);
-    const size_t smem = normal_smem_bytes(tile, p->live_cap, idx_cap, ns);
+    const int live_cap = std::min(p->live_cap, NORMAL_LIVE_CAP);
+    const size_t smem = normal_smem_bytes(tile, live_cap, idx_cap, ns);
     if (smem > 227 * 1024)
         return set_error(FPHO_ERR_LIMIT, "the normal equations of %d sources over %d-pixel tiles "
                          "need %zu bytes of shared memory (max 227 KB)", ns, tile, smem);
@@ -328,7 +329,7 @@ static int enqueue_normal(fpho_patch *p, const fpho_source *d_prop, double *d_at
     A.pgrad = p->d_pgrad;
     A.pgrad_stride = 7 * ns;
     A.want_residual = 1;
-    A.live_cap = p->live_cap;
+    A.live_cap = live_cap;
     A.idx_cap = idx_cap;
     A.err = p->d_err;
     A.pairs = nullptr;

@@ -265,7 +265,9 @@ constexpr float KEXP_LO = -9.629815167500055e-09f;
 __device__ __forceinline__ v2 exp2_unbiased(v2 E) {
     const float MAGIC = 12582912.0f;  // 1.5 * 2^23
     const v2 t = add2(E, pk1(MAGIC));
-    const v2 f = add2(E, add2(t, pk1(-MAGIC)) ^ 0x8000000080000000ull);  // E - n
+    // n = t - MAGIC is exact, so MAGIC - t (one FMA, no sign-bit operation) is
+    // -n, up to the sign of a zero, which the polynomial does not see (2^(+-0) = 1)
+    const v2 f = add2(E, fma2(t, pk1(-1.0f), pk1(MAGIC)));  // E - n
     v2 p = pk1(1.5370704932138324e-04f);
     p = fma2(p, f, pk1(1.3399848248809576e-03f));
     p = fma2(p, f, pk1(9.618373587727547e-03f));

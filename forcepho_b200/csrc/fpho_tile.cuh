@@ -997,6 +997,73 @@ __device__ __forceinline__ void tile_body_split(const TileArgs &A, int tile, uns
 }
 
 // ------------------------------------------------------------ design rows
+// The unit-flux model of one Gaussian (dA/dflux in place of the amplitude)
+// accumulated, negated, into M, as residual_pairs does for the model.
+template <int KP>
+__device__ __forceinline__ void design_one(const v2 (&Xp)[KP], const v2 (&Yp)[KP], v2 (&M)[KP],
+                                           const float *r, int flag, v2 CM24, v2 KEXP2,
+                                           v2 KEXPLO2) {
+    v2 NXC, NYC, FXX, FXY, FYY, AMP, HB, C0;
+    ld2(r + R_NXC, NXC, NYC);
+    ld2(r + R_FXX, FXX, FXY);
+    ld2(r + R_FYY, FYY, AMP);
+    ld2(r + R_HB, HB, C0);
+    const v2 UA = pk1(r[R_JA_FLUX]);
+    const v2 HA = mul2(UA, CM24);
+    const v2 UB = mul2(pk1(-1.0f), mul2(UA, C0));
+    if (flag & FLAG_CUT)
+        residual_pairs<KP, true>(Xp, Yp, M, NXC, NYC, FXX, FXY, FYY, HA, UB, KEXP2, KEXPLO2);
+    else
+        residual_pairs<KP, false>(Xp, Yp, M, NXC, NYC, FXX, FXY, FYY, HA, UB, KEXP2, KEXPLO2);
+}
+
+// The same for two consecutive Gaussians a, b of one source at once (their
+// exponentials interleave), M updated with a's term and then b's, the cut
+// applied to both (see residual_pairs2).
+template <int KP>
+__device__ __forceinline__ void design_pairs2(const v2 (&Xp)[KP], const v2 (&Yp)[KP],
+                                              v2 (&M)[KP], const float *ra, const float *rb,
+                                              v2 CM24, v2 KEXP2, v2 KEXPLO2) {
+    v2 NXa, NYa, FXXa, FXYa, FYYa, AMPa, HBa, C0a;
+    v2 NXb, NYb, FXXb, FXYb, FYYb, AMPb, HBb, C0b;
+    ld2(ra + R_NXC, NXa, NYa);
+    ld2(ra + R_FXX, FXXa, FXYa);
+    ld2(ra + R_FYY, FYYa, AMPa);
+    ld2(ra + R_HB, HBa, C0a);
+    ld2(rb + R_NXC, NXb, NYb);
+    ld2(rb + R_FXX, FXXb, FXYb);
+    ld2(rb + R_FYY, FYYb, AMPb);
+    ld2(rb + R_HB, HBb, C0b);
+    const v2 UAa = pk1(ra[R_JA_FLUX]), UAb = pk1(rb[R_JA_FLUX]);
+    const v2 HAa = mul2(UAa, CM24), HAb = mul2(UAb, CM24);
+    const v2 UBa = mul2(pk1(-1.0f), mul2(UAa, C0a)), UBb = mul2(pk1(-1.0f), mul2(UAb, C0b));
+#pragma unroll
+    for (int j = 0; j < KP; ++j) {
+        const v2 DXa = add2(Xp[j], NXa), DYa = add2(Yp[j], NYa);
+        const v2 DXb = add2(Xp[j], NXb), DYb = add2(Yp[j], NYb);
+        const v2 VXa = fma2(FXYa, DYa, mul2(FXXa, DXa));
+        const v2 VXb = fma2(FXYb, DYb, mul2(FXXb, DXb));
+        const v2 VYa = fma2(FXYa, DXa, mul2(FYYa, DYa));
+        const v2 VYb = fma2(FXYb, DXb, mul2(FYYb, DYb));
+        const v2 Qa = fma2(DYa, VYa, mul2(DXa, VXa));
+        const v2 Qb = fma2(DYb, VYb, mul2(DXb, VXb));
+        v2 Ga = exp2_unbiased(fma2(Qa, KEXP2, mul2(Qa, KEXPLO2)));
+        v2 Gb = exp2_unbiased(fma2(Qb, KEXP2, mul2(Qb, KEXPLO2)));
+        {
+            float g0, g1, q0, q1;
+            unpk(Ga, g0, g1);
+            unpk(Qa, q0, q1);
+            Ga = pk(q0 > FPHO_MAX_EXP_ARG ? 0.0f : g0, q1 > FPHO_MAX_EXP_ARG ? 0.0f : g1);
+            unpk(Gb, g0, g1);
+            unpk(Qb, q0, q1);
+            Gb = pk(q0 > FPHO_MAX_EXP_ARG ? 0.0f : g0, q1 > FPHO_MAX_EXP_ARG ? 0.0f : g1);
+        }
+        const v2 Sa = fma2(VYa, VYa, mul2(VXa, VXa));
+        const v2 Sb = fma2(VYb, VYb, mul2(VXb, VXb));
+        M[j] = fma2(fma2(Sa, HAa, UBa), Ga, M[j]);
+        M[j] = fma2(fma2(Sb, HAb, UBb), Gb, M[j]);
+    }
+}
 // The unit-flux model of every source at every pixel of the tile:
 // X[src][pix] = sum over the source's image Gaussians of dA/dflux * G * H
 // (dA/dflux = the record's R_JA_FLUX; with the source's flux this is its model
@@ -1056,19 +1123,16 @@ __device__ __forceinline__ void design_body(const TileArgs &A, int tile, unsigne
         phase ^= 1u;
         for (int i = 0; i < n; ++i) {
             const float *r = recs + (size_t)i * GSTAGE;
-            v2 NXC, NYC, FXX, FXY, FYY, AMP, HB, C0;
-            ld2(r + R_NXC, NXC, NYC);
-            ld2(r + R_FXX, FXX, FXY);
-            ld2(r + R_FYY, FYY, AMP);
-            ld2(r + R_HB, HB, C0);
-            const v2 UA = pk1(r[R_JA_FLUX]);  // dA/dflux in place of amp
-            const v2 HA = mul2(UA, CM24);
-            const v2 UB = mul2(pk1(-1.0f), mul2(UA, C0));
-            const int flag = kept[c0 + i];
-            if (flag & FLAG_CUT)
-                residual_pairs<KP, true>(Xp, Yp, M, NXC, NYC, FXX, FXY, FYY, HA, UB, KEXP2, KEXPLO2);
-            else
-                residual_pairs<KP, false>(Xp, Yp, M, NXC, NYC, FXX, FXY, FYY, HA, UB, KEXP2, KEXPLO2);
+            int flag = kept[c0 + i];
+            if (!(flag & FLAG_LAST_SRC) && i + 1 < n) {
+                // two Gaussians of the same source: their exponentials interleave
+                design_pairs2<KP>(Xp, Yp, M, r, r + GSTAGE, CM24, KEXP2, KEXPLO2);
+                ++i;
+                r += GSTAGE;
+                flag = kept[c0 + i];
+            } else {
+                design_one<KP>(Xp, Yp, M, r, flag, CM24, KEXP2, KEXPLO2);
+            }
             if ((flag & FLAG_LAST_SRC) || i == n - 1) {
                 const int src = min((unsigned)__float_as_int(r[R_SRC]),
                                     (unsigned)(A.pv.n_sources - 1));
