@@ -90,19 +90,20 @@ __global__ void __launch_bounds__(NT, MINB) batch_tiles(const TileArgs *args, co
     }
 }
 
+// grid (n_jobs, ceil(max_stride / REDUCE_WARPS)), block 32 REDUCE_WARPS: the
+// same per-component warp sums as reduce_bands, so a patch's batched result
+// equals its single-patch one bit for bit
 __global__ void batch_reduce(const BandJob *jobs, double *chi2, float *dchi2, int *counter) {
     const BandJob jb = jobs[blockIdx.x];
-    const int j = blockIdx.y * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int j = blockIdx.y * REDUCE_WARPS + w;
     if (j < jb.stride) {
-        double acc = 0.0;
-        for (int t = jb.t0; t < jb.t1; ++t) acc += (double)jb.pgrad[(size_t)t * jb.stride + j];
-        dchi2[jb.dchi2_off + j] = (float)acc;
+        const double acc = warp_column_sum(jb.pgrad + j, jb.stride, jb.t0, jb.t1, lane);
+        if (lane == 0) dchi2[jb.dchi2_off + j] = (float)acc;
     }
-    if (blockIdx.y == 0 && threadIdx.x < 32) {
-        double c = 0.0;
-        for (int t = jb.t0 + threadIdx.x; t < jb.t1; t += 32) c += jb.pchi2[t];
-        for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-        if (threadIdx.x == 0) chi2[jb.chi2_index] = c;
+    if (blockIdx.y == 0 && w == 0) {
+        const double c = warp_column_sum(jb.pchi2, 1, jb.t0, jb.t1, lane);
+        if (lane == 0) chi2[jb.chi2_index] = c;
     }
     if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) *counter = 0;
 }
@@ -474,7 +475,8 @@ static int batch_enqueue(fpho_batch *b, const fpho_source *d_props, double *d_ch
     }
     if (b->ev1) CUDA_TRY(cudaEventRecord(b->ev1, s));
     if (b->n_jobs > 0) {
-        batch_reduce<<<dim3(b->n_jobs, (b->max_stride + 127) / 128), 128, 0, s>>>(
+        batch_reduce<<<dim3(b->n_jobs, (b->max_stride + REDUCE_WARPS - 1) / REDUCE_WARPS),
+                       32 * REDUCE_WARPS, 0, s>>>(
             b->d_jobs, d_chi2, d_dchi2, b->d_counter);
         CUDA_TRY(cudaGetLastError());
     }

@@ -874,8 +874,8 @@ int enqueue_evaluate(fpho_patch *p, const fpho_source *d_prop, double *d_chi2, f
     }
     if (rc) return rc;
     if (p->ev_tile1) CUDA_TRY(cudaEventRecord(p->ev_tile1, s));
-    dim3 rg(p->n_bands, grad ? (out_stride + 127) / 128 : 1);
-    reduce_bands<<<rg, 128, 0, s>>>(p->d_tile_band_start, p->d_pchi2, p->d_pgrad,
+    dim3 rg(p->n_bands, grad ? (out_stride + REDUCE_WARPS - 1) / REDUCE_WARPS : 1);
+    reduce_bands<<<rg, 32 * REDUCE_WARPS, 0, s>>>(p->d_tile_band_start, p->d_pchi2, p->d_pgrad,
                                     7 * p->n_sources, d_chi2, grad ? d_dchi2 : nullptr,
                                     out_stride);
     CUDA_TRY(cudaGetLastError());

@@ -96,24 +96,39 @@ static __global__ void __launch_bounds__(1024) order_tiles(const int *cost, int 
         order[atomicAdd(&hist[NB - 1 - (int)((long long)cost[i] * NB / span)], 1)] = i;
 }
 
-// Sum tile partials per band in double.  grid (n_bands, ceil(out_stride/128)).
+// Sum of a tile range [t0, t1) of one column (FP64): lane l adds tiles
+// t0 + l, t0 + l + 32, ... in order, then the lanes combine by a fixed
+// butterfly -- deterministic, and 32 loads in flight instead of one chain.
+template <typename T>
+__device__ __forceinline__ double warp_column_sum(const T *col, size_t step, int t0, int t1,
+                                                  int lane) {
+    double acc = 0.0;
+    for (int t = t0 + lane; t < t1; t += 32) acc += (double)col[(size_t)t * step];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    return acc;
+}
+
+// Warps per block of reduce_bands and batch_reduce: one gradient component each.
+constexpr int REDUCE_WARPS = 4;
+
+// Sum tile partials per band in double.  grid (n_bands, ceil(out_stride /
+// REDUCE_WARPS)), block 32 REDUCE_WARPS: warp w of block y sums component
+// y REDUCE_WARPS + w; block y = 0, warp 0 also sums chi2.
 static __global__ void reduce_bands(const int *tile_band_start, const double *pchi2,
                                     const float *pgrad, int stride, double *chi2_out,
                                     float *dchi2_out, int out_stride) {
     const int b = blockIdx.x;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int t0 = tile_band_start[b], t1 = tile_band_start[b + 1];
-    const int j = blockIdx.y * blockDim.x + threadIdx.x;
+    const int j = blockIdx.y * REDUCE_WARPS + w;
     if (dchi2_out && j < out_stride) {
-        double acc = 0.0;
-        if (j < stride)
-            for (int t = t0; t < t1; ++t) acc += (double)pgrad[(size_t)t * stride + j];
-        dchi2_out[(size_t)b * out_stride + j] = (float)acc;
+        const double acc = j < stride ? warp_column_sum(pgrad + j, stride, t0, t1, lane) : 0.0;
+        if (lane == 0) dchi2_out[(size_t)b * out_stride + j] = (float)acc;
     }
-    if (blockIdx.y == 0 && threadIdx.x < 32) {
-        double c = 0.0;
-        for (int t = t0 + threadIdx.x; t < t1; t += 32) c += pchi2[t];
-        for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
-        if (threadIdx.x == 0) chi2_out[b] = c;
+    if (blockIdx.y == 0 && w == 0) {
+        const double c = warp_column_sum(pchi2, 1, t0, t1, lane);
+        if (lane == 0) chi2_out[b] = c;
     }
 }
 

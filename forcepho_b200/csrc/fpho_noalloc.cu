@@ -363,7 +363,8 @@ extern "C" int fpho_evaluate_proposal_noalloc(const fpho_patch_struct *patch, in
     A.err = &hdr->err;
     A.pairs = nullptr;
     noalloc_tiles<<<(unsigned)n_tiles_max, NA_THREADS, smem, s>>>(A, hdr);
-    reduce_bands<<<dim3(n_bands, (dchi2_stride + 127) / 128), 128, 0, s>>>(
+    reduce_bands<<<dim3(n_bands, (dchi2_stride + REDUCE_WARPS - 1) / REDUCE_WARPS),
+                   32 * REDUCE_WARPS, 0, s>>>(
         tile_band_start, pchi2, pgrad, stride, dev_chi2, dev_dchi2, dchi2_stride);
     noalloc_finish<<<1, 32, 0, s>>>(hdr, dev_status, dev_chi2, n_bands);
     ce = cudaGetLastError();
