@@ -292,10 +292,12 @@ int launch_tile_kernel(int variant, const TileArgs &A, int n_tiles, cudaStream_t
 static std::mutex g_design_mu;
 static size_t g_design_set[64][kNumVariants];
 
-int launch_design_kernel(int variant, const TileArgs &A, int n_tiles, float *X, long long npix,
+int launch_design_kernel(int variant, const TileArgs &A_in, int n_tiles, float *X, long long npix,
                          cudaStream_t stream) {
     if (n_tiles <= 0) return FPHO_OK;
     const Variant &V = kVariants[variant];
+    TileArgs A = A_in;
+    A.live_cap = std::min(A.live_cap, DESIGN_LIVE_CAP);
     const size_t smem =
         tile_smem_layout_bytes(V.design_nt / 32, A.live_cap, A.idx_cap, A.pgrad_stride);
     int dev = 0;

@@ -253,9 +253,7 @@ const NormalShape kNormalShapes[] = {
     {512, 128, (const void *)normal_tiles<128, 4>},
     {1024, 256, (const void *)normal_tiles<256, 4>},
 };
-// records per shared-memory stage of the flux kernel: the design pass stages
-// each chunk once, so a small stage costs little and lets more CTAs reside
-constexpr int NORMAL_LIVE_CAP = 64;
+
 
 std::mutex g_norm_mu;
 size_t g_norm_attr[64][8];
@@ -287,7 +285,7 @@ static int enqueue_normal(fpho_patch *p, const fpho_source *d_prop, double *d_at
         return set_error(FPHO_ERR_STATE, "no normal-equation kernel for %d-pixel tiles", tile);
     const NormalShape &S = kNormalShapes[shape];
     const int idx_cap = std::max(p->max_g, 1);
-    const int live_cap = std::min(p->live_cap, NORMAL_LIVE_CAP);
+    const int live_cap = std::min(p->live_cap, DESIGN_LIVE_CAP);
     const size_t smem = normal_smem_bytes(tile, live_cap, idx_cap, ns);
     if (smem > 227 * 1024)
         return set_error(FPHO_ERR_LIMIT, "the normal equations of %d sources over %d-pixel tiles "

@@ -997,6 +997,12 @@ __device__ __forceinline__ void tile_body_split(const TileArgs &A, int tile, uns
 }
 
 // ------------------------------------------------------------ design rows
+// Records per shared-memory stage of the design passes (the design matrix and
+// the flux solve's normal equations): each chunk is staged once, so a small
+// stage costs little and lets more CTAs reside.  Both passes use it, so their
+// unit-flux rows -- flushed at source boundaries and chunk ends -- are the
+// same floats.
+constexpr int DESIGN_LIVE_CAP = 64;
 // The unit-flux model of one Gaussian (dA/dflux in place of the amplitude)
 // accumulated, negated, into M, as residual_pairs does for the model.
 template <int KP>
