@@ -122,3 +122,32 @@ def test_store_and_device_pixel_create_reject_bad_arguments():
     assert L.fpho_store_free(None) == 0
     rc = L.fpho_patch_create_device_pixels(None, 1, 0, None, ctypes.byref(h))
     assert rc == 1 and "NULL" in _lib.last_error() and not h.value
+
+
+def test_new_entry_points_reject_bad_arguments():
+    """Host-side checks of the batch configuration, flux-solve, exact-residual
+    and variant-shape entry points, made before any CUDA call."""
+    from forcepho_b200 import _lib
+    L = _lib.lib
+    h = ctypes.c_void_p()
+    one = (ctypes.c_void_p * 1)(None)
+    assert L.fpho_batch_create_config(None, 1, -1, 128, 0, None, ctypes.byref(h)) == 1
+    assert L.fpho_batch_create_config(one, 1, -1, 8, 0, None, ctypes.byref(h)) == 1
+    assert "live_cap" in _lib.last_error()
+    assert L.fpho_batch_create_config(one, 1, -1, 128, 99, None, ctypes.byref(h)) == 1
+    assert "ctas_per_sm" in _lib.last_error()
+    out = (ctypes.c_int * 16)()
+    n = L.fpho_batch_variants(out, 16)
+    no_batch = [v for v in range(len(_lib.variants())) if v not in list(out)[:n]][0]
+    assert L.fpho_batch_create_config(one, 1, no_batch, 128, 0, None, ctypes.byref(h)) == 1
+    assert "no batched tile kernel" in _lib.last_error()
+    assert L.fpho_batch_create_config(one, 1, -1, 128, 0, None, ctypes.byref(h)) == 1
+    assert "NULL" in _lib.last_error() and not h.value           # the patch itself
+    assert n >= 5 and all(out[i] >= 0 for i in range(n))
+    assert L.fpho_batch_config(None, out) == 1
+    assert L.fpho_patch_optimize_fluxes(None, None, 1, None, None, None, None) == 1
+    assert L.fpho_patch_flux_normal_equations(None, None, 1, None, None, None) == 1
+    assert L.fpho_patch_set_exact_residual(None, 1) == 1
+    shape = (ctypes.c_int * 3)()
+    assert L.fpho_variant_shape(-1, shape) == 1 and L.fpho_variant_shape(999, shape) == 1
+    assert L.fpho_variant_shape(0, shape) == len(_lib.variants())
