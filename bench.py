@@ -899,17 +899,19 @@ def run_ours(args):
     achieved = evaluated_pairs * FLOPS_PER_PAIR / tile_s / 1e12
     sfu = evaluated_pairs * 2 / tile_s / 1e9
 
+    # the further legs run in single-GPU runs only (a multi-GPU run measures
+    # the patch-parallel evaluation and holds every GPU while it runs)
     differentiable = None
-    if not args.no_differentiable:
+    if world == 1 and not args.no_differentiable:
         differentiable = differentiable_leg(args, torch, P, cfg, steps=max(3, min(args.steps, 50)))
 
     multichain = None
-    if args.chains > 0:
+    if world == 1 and args.chains > 0:
         multichain = multichain_leg(args, torch, steps=max(3, min(args.steps, 50)),
                                     n_chains=args.chains)
 
     batched = None
-    if args.batch_patches > 0:
+    if world == 1 and args.batch_patches > 0:
         batched = batched_leg(args, torch, _lib, steps=max(3, min(args.steps, 50)))
         rb = batched["roofline"]
         rb.update({"peak": fp32_tflops, "frac": rb["achieved"] / fp32_tflops,
