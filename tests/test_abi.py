@@ -95,7 +95,7 @@ def test_variants_listed():
     from forcepho_b200 import _lib
     v = _lib.variants()
     shapes = _lib.variant_shapes()
-    assert len(v) >= 4 and len(shapes) == len(v)
+    assert len(v) == 14 and len(shapes) == len(v)
     for (nt, k), (nt2, tile, split) in zip(v, shapes):
         assert nt == nt2 and nt % 32 == 0 and k == tile // nt
         if split == 0:
