@@ -54,13 +54,11 @@ __device__ __forceinline__ void upper_pair(int p, int ns, int &s, int &t) {
 template <int NT, int K>
 __global__ void __launch_bounds__(NT) normal_tiles(TileArgs A, double *pnorm, int n_terms) {
     static_assert(K % 2 == 0, "pixels per thread must be even (packed pairs)");
-    constexpr int NW = NT / 32;
     constexpr int KP = K / 2;
     constexpr int TP = NT * K;
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ uint64_t mbar;
-    __shared__ int s_cnt[NW];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x;
     if (tid == 0) {
         mbar_init(&mbar, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -105,21 +103,12 @@ __global__ void __launch_bounds__(NT) normal_tiles(TileArgs A, double *pnorm, in
         Yp[j] = pk(yv[0], yv[1]);
         M[j] = 0ull;
     }
-    const int n_live = scan_tile<NT>(A, bb, g0, g1, npsf, kept, s_cnt);
+    const int n_live = scan_tile<NT>(A, bb, g0, g1, npsf, kept);
     const v2 KEXP2 = pk1(KEXP), KEXPLO2 = pk1(KEXP_LO), CM24 = pk1(-1.0f / 24.0f);
     for (int c0 = 0; c0 < n_live; c0 += cap) {
         const int n = min(cap, n_live - c0);
         if (c0 > 0) __syncthreads();
-        fence_proxy_async_smem();
-        if (warp == 0) {
-            if (lane == 0) mbar_arrive_expect_tx(&mbar, (uint32_t)n * GSTAGE * 4);
-            __syncwarp();
-            for (int i = lane; i < n; i += 32)
-                bulk_g2s(recs + (size_t)i * GSTAGE,
-                         A.gtab + (size_t)(g0 + (kept[c0 + i] >> 2)) * GREC, GSTAGE * 4, &mbar);
-        }
-        mbar_wait_bounded(&mbar, phase, A.err);
-        phase ^= 1u;
+        stage_records<NT>(recs, A.gtab + (size_t)g0 * GREC, kept, c0, n, 0, &mbar, phase, A.err);
         for (int i = 0; i < n; ++i) {
             const float *r = recs + (size_t)i * GSTAGE;
             int flag = kept[c0 + i];

@@ -149,6 +149,27 @@ __host__ __device__ inline size_t tile_smem_layout_bytes(int nw, int live_cap, i
     return (size_t)live_cap * GSTAGE * 4 + (size_t)idx_cap * 4 + (size_t)nw * stride * 4;
 }
 
+// Stage the records of kept entries [c0, c0 + n) of an exposure (first record
+// `gexp`) into `recs`, in list order, and wait for them.  Every thread of the
+// CTA issues the bulk copies of its records (one 128-byte copy each); issued
+// by one warp, the copies of a stage queued behind each other and the CTA
+// spent about a fifth of each tile waiting for them.  Callers have finished
+// reading `recs` (a barrier) before the call.
+template <int NT>
+__device__ __forceinline__ void stage_records(float *recs, const float *gexp, const int *kept,
+                                              int c0, int n, int extra_tx, uint64_t *mbar,
+                                              uint32_t &phase, int *err) {
+    fence_proxy_async_smem();
+    if (threadIdx.x == 0)
+        mbar_arrive_expect_tx(mbar, (uint32_t)(n * GSTAGE * 4 + extra_tx));
+    __syncthreads();  // the expected bytes are set before any copy can complete
+    for (int i = threadIdx.x; i < n; i += NT)
+        bulk_g2s(recs + (size_t)i * GSTAGE, gexp + (size_t)(kept[c0 + i] >> 2) * GREC,
+                 GSTAGE * 4, mbar);
+    mbar_wait_bounded(mbar, phase, err);
+    phase ^= 1u;
+}
+
 // ------------------------------------------------------------ culling
 // Minimum over the rectangle [x0,x1] x [y0,y1] of the exp-argument
 // q(p) = (p-c)^T F (p-c): 0 if the centre is inside, else the smallest of the
@@ -173,13 +194,11 @@ __device__ __forceinline__ float rect_min_q(float4 bb, float xc, float yc, float
     return best;
 }
 
-// Is image Gaussian `rec` (in global memory) possibly within exp-argument 36
-// of some point of the tile box?  Conservative: cull only when the exact
-// minimum, less a 2e-3 relative + 2e-3 margin for float rounding, exceeds 36.
-__device__ __forceinline__ bool keeps_tile(const float *rec, float4 bb) {
-    const float4 a = *reinterpret_cast<const float4 *>(rec);      // -xc -xc -yc -yc
-    const float4 b = *reinterpret_cast<const float4 *>(rec + 4);  // fxx fxx fxy fxy
-    const float fyy = rec[R_FYY];
+// Is an image Gaussian possibly within exp-argument 36 of some point of the
+// tile box?  Conservative: cull only when the exact minimum, less a 2e-3
+// relative + 2e-3 margin for float rounding, exceeds 36.  `a` and `b` are the
+// record's first two float4 (-xc -xc -yc -yc, fxx fxx fxy fxy).
+__device__ __forceinline__ bool keeps_tile(float4 a, float4 b, float fyy, float4 bb) {
     const float fxx = b.x, fxy = b.z;
     if (!(fxx > 0.0f && fyy > 0.0f)) return true;
     const float q = rect_min_q(bb, -a.x, -a.z, fxx, fxy, fyy);
@@ -450,8 +469,9 @@ constexpr int FLAG_LAST_SRC = 2;   // last kept Gaussian of its source in the ch
 // visible to the whole CTA.
 template <int NT>
 __device__ __forceinline__ int scan_tile(const TileArgs &A, float4 bb, int g0, int g1, int npsf,
-                                         int *kept, int *s_cnt) {
+                                         int *kept) {
     constexpr int NW = NT / 32;
+    __shared__ int s_cnt[NW];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     int n_live = 0;
     for (int base = g0; base < g1; base += NT) {
@@ -463,7 +483,9 @@ __device__ __forceinline__ int scan_tile(const TileArgs &A, float4 bb, int g0, i
             live = !(gb.y < bb.x || gb.x > bb.y || gb.w < bb.z || gb.z > bb.w);
             if (live) {
                 const float *r = A.gtab + (size_t)idx * GREC;
-                live = keeps_tile(r, bb);
+                const float4 ra = *reinterpret_cast<const float4 *>(r);
+                const float4 rb = *reinterpret_cast<const float4 *>(r + 4);
+                live = keeps_tile(ra, rb, r[R_FYY], bb);
                 const float nxc = r[R_NXC], nyc = r[R_NYC];
                 const float fxx = r[R_FXX], fxy = r[R_FXY], fyy = r[R_FYY];
                 float qmax = 0.0f;
@@ -521,7 +543,6 @@ __device__ __forceinline__ void tile_body(const TileArgs &A, int tile, unsigned 
     int *kept = reinterpret_cast<int *>(smem + (size_t)cap * GSTAGE * 4);
     float *wacc = reinterpret_cast<float *>(kept + A.idx_cap);
 
-    __shared__ int s_cnt[NW];
     __shared__ double s_chi2[NW];
     __shared__ int s_any_weight;
 
@@ -559,24 +580,15 @@ __device__ __forceinline__ void tile_body(const TileArgs &A, int tile, unsigned 
     if (tid == 0) s_any_weight = 0;
 
     // ---- the ordered list of kept image Gaussians
-    const int n_live = scan_tile<NT>(A, bb, g0, g1, npsf, kept, s_cnt);
+    const int n_live = scan_tile<NT>(A, bb, g0, g1, npsf, kept);
     if (any_w) s_any_weight = 1;
     __syncthreads();
     const bool tile_has_weight = s_any_weight != 0;
 
     // ---- stage kept records [c0, c0 + n) into shared memory with bulk copies
     auto stage = [&](int c0, int n) {
-        fence_proxy_async_smem();
-        if (warp == 0) {
-            if (lane == 0)
-                mbar_arrive_expect_tx(mbar, (uint32_t)(n * GSTAGE * 4 + A.test_extra_tx));
-            __syncwarp();
-            for (int i = lane; i < n; i += 32)
-                bulk_g2s(recs + (size_t)i * GSTAGE,
-                         A.gtab + (size_t)(g0 + (kept[c0 + i] >> 2)) * GREC, GSTAGE * 4, mbar);
-        }
-        mbar_wait_bounded(mbar, phase, A.err);
-        phase ^= 1u;
+        stage_records<NT>(recs, A.gtab + (size_t)g0 * GREC, kept, c0, n, A.test_extra_tx, mbar,
+                          phase, A.err);
     };
 
     const v2 KEXP2 = pk1(KEXP), KEXPLO2 = pk1(KEXP_LO);
@@ -776,7 +788,6 @@ __device__ __forceinline__ void tile_body_split(const TileArgs &A, int tile, uns
     float *wacc = reinterpret_cast<float *>(kept + A.idx_cap);
     float *part = wacc + (size_t)NW * stride;  // [NW][TP] partial models
 
-    __shared__ int s_cnt[NW];
     __shared__ double s_chi2;
     __shared__ int s_any_weight;
 
@@ -810,23 +821,14 @@ __device__ __forceinline__ void tile_body_split(const TileArgs &A, int tile, uns
     }
     if (tid == 0) s_any_weight = 0;
 
-    const int n_live = scan_tile<NT>(A, bb, g0, g1, npsf, kept, s_cnt);
+    const int n_live = scan_tile<NT>(A, bb, g0, g1, npsf, kept);
     if (any_w) s_any_weight = 1;
     __syncthreads();
     const bool tile_has_weight = s_any_weight != 0;
 
     auto stage = [&](int c0, int n) {
-        fence_proxy_async_smem();
-        if (warp == 0) {
-            if (lane == 0)
-                mbar_arrive_expect_tx(mbar, (uint32_t)(n * GSTAGE * 4 + A.test_extra_tx));
-            __syncwarp();
-            for (int i = lane; i < n; i += 32)
-                bulk_g2s(recs + (size_t)i * GSTAGE,
-                         A.gtab + (size_t)(g0 + (kept[c0 + i] >> 2)) * GREC, GSTAGE * 4, mbar);
-        }
-        mbar_wait_bounded(mbar, phase, A.err);
-        phase ^= 1u;
+        stage_records<NT>(recs, A.gtab + (size_t)g0 * GREC, kept, c0, n, A.test_extra_tx, mbar,
+                          phase, A.err);
     };
     // this warp's share [i0, i1) of a chunk of n records: contiguous, even
     // lengths (two Gaussians per step)
@@ -1082,13 +1084,11 @@ __device__ __forceinline__ void design_body(const TileArgs &A, int tile, unsigne
                                             uint64_t *mbar, uint32_t &phase, float *X,
                                             long long npix) {
     static_assert(K % 2 == 0, "pixels per thread must be even (packed pairs)");
-    constexpr int NW = NT / 32;
     constexpr int KP = K / 2;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x;
     const int cap = A.live_cap;
     float *recs = reinterpret_cast<float *>(smem);
     int *kept = reinterpret_cast<int *>(smem + (size_t)cap * GSTAGE * 4);
-    __shared__ int s_cnt[NW];
 
     const TileDesc td = A.tiles[tile];
     const float4 bb = A.tbox_all[tile];
@@ -1112,21 +1112,12 @@ __device__ __forceinline__ void design_body(const TileArgs &A, int tile, unsigne
         Yp[j] = pk(ys[0], ys[1]);
         M[j] = 0ull;
     }
-    const int n_live = scan_tile<NT>(A, bb, g0, g1, npsf, kept, s_cnt);
+    const int n_live = scan_tile<NT>(A, bb, g0, g1, npsf, kept);
     const v2 KEXP2 = pk1(KEXP), KEXPLO2 = pk1(KEXP_LO), CM24 = pk1(-1.0f / 24.0f);
     for (int c0 = 0; c0 < n_live; c0 += cap) {
         const int n = min(cap, n_live - c0);
         if (c0 > 0) __syncthreads();
-        fence_proxy_async_smem();
-        if (warp == 0) {
-            if (lane == 0) mbar_arrive_expect_tx(mbar, (uint32_t)n * GSTAGE * 4);
-            __syncwarp();
-            for (int i = lane; i < n; i += 32)
-                bulk_g2s(recs + (size_t)i * GSTAGE,
-                         A.gtab + (size_t)(g0 + (kept[c0 + i] >> 2)) * GREC, GSTAGE * 4, mbar);
-        }
-        mbar_wait_bounded(mbar, phase, A.err);
-        phase ^= 1u;
+        stage_records<NT>(recs, A.gtab + (size_t)g0 * GREC, kept, c0, n, 0, mbar, phase, A.err);
         for (int i = 0; i < n; ++i) {
             const float *r = recs + (size_t)i * GSTAGE;
             int flag = kept[c0 + i];
