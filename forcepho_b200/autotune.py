@@ -31,7 +31,7 @@ from . import _lib
 CACHE = os.environ.get("FPHO_AUTOTUNE_CACHE",
                        os.path.join(os.path.expanduser("~"), ".cache", "forcepho_b200",
                                     "autotune.json"))
-DEFAULT = {"variant": 12, "live_cap": 256, "schedule": 1}  # 4 warps share 256-pixel tiles
+DEFAULT = {"variant": 8, "live_cap": 256, "schedule": 1}  # 4 warps share 256-pixel tiles
 BATCH_DEFAULT = {"variant": 6, "live_cap": 128, "ctas_per_sm": 0}   # 64 threads x 8 pixels
 LIVE_CAPS = (96, 128, 160, 192, 256, 384)
 SCHEDULES = (0, 1)

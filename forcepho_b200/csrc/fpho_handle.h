@@ -33,11 +33,11 @@ struct fpho_patch {
     int *d_exp_band = nullptr, *d_exp_npsf = nullptr, *d_gauss_start = nullptr;
     fpho_patch_struct *d_struct = nullptr;
     // tile plan (host copy of the tile list kept for batching); the default
-    // configuration is variant 12 (4 warps sharing each 256-pixel tile's
-    // Gaussians, 8 pixels per thread, registers capped for 5 CTAs per SM),
-    // 256 records per shared-memory stage, persistent schedule -- the fastest
-    // measured on the 20-source, 8-band x 4-exposure, 128x128 px patch
-    int variant = 12, live_cap = 256, n_tiles = 0;
+    // configuration is variant 8 (4 warps sharing each 256-pixel tile's
+    // Gaussians, 8 pixels per thread, 4 CTAs per SM), 256 records per
+    // shared-memory stage, persistent schedule -- the fastest measured on the
+    // 20-source, 8-band x 4-exposure, 128x128 px patch
+    int variant = 8, live_cap = 256, n_tiles = 0;
     std::vector<fpho::TileDesc> h_tiles;
     std::vector<int> tile_band_start;
     fpho::TileDesc *d_tiles = nullptr;

@@ -363,9 +363,8 @@ FPHO_API int fpho_variant_shape(int variant, int out[3]);
 
 /* Select the tile-kernel variant and the shared-memory stage size (image
  * Gaussians per chunk) used by this patch; re-plans the tiles if the tile
- * size changes.  Default: variant 12 (128 threads: 4 warps sharing each
- * 256-pixel tile's Gaussians, 8 pixels per thread, 5 CTAs per SM), live_cap
- * 256. */
+ * size changes.  Default: variant 8 (128 threads: 4 warps sharing each
+ * 256-pixel tile's Gaussians, 8 pixels per thread), live_cap 256. */
 FPHO_API int fpho_patch_set_config(fpho_patch *p, int variant, int live_cap, void *stream);
 
 /* Tile scheduling of this patch: 0 = one CTA per tile; 1 (default) = as many
