@@ -243,31 +243,36 @@ __device__ __forceinline__ float ex2f(float x) {
 }
 
 // -0.5 * log2(e): exp(-Q/2) = 2^(Q * KEXP).  KEXP_LO carries the rounding of
-// KEXP (relative 1.3e-8), so that fma(Q, KEXP, Q * KEXP_LO) is the exponent
+// KEXP (relative 1.3e-8), so that Q * KEXP + Q * KEXP_LO is the exponent
 // without the systematic error a rounded constant would add.
 constexpr float KEXP = -0.72134752044448170368f;
 constexpr float KEXP_LO = -9.629815167500055e-09f;
 
-// Unbiased 2^E for packed E in [-126, 0].
+// Unbiased exp(-Q/2) for packed exp-arguments Q in [0, 174].
 //
 // MUFU.EX2 (ex2.approx) is accurate to a few 1e-7 but its error has a mean of
 // about -3e-8 over the exponents seen here.  In the residual r = data - model
 // that bias does not average out: the gradient of chi2 near a fit measures a
 // ~1% parameter offset, and a relative model bias b shows up in it amplified
-// ~1e3 times.  So the residual pass evaluates 2^E with Cody and Waite's range
-// reduction E = n + f, n = rint(E), f in [-1/2, 1/2] (the rounding done by
-// adding 1.5*2^23), a degree-6 polynomial for 2^f (coefficients fitted here by
-// relative least squares with the constant term pinned to 1: mean relative
-// error 6e-10, max 8e-8 in float), and scaling by 2^n through the exponent
-// field.  Inputs below -126 give garbage that callers discard (they select 0
-// for exp-arguments above the cutoff, and never use the value at pixels
-// outside the culling box).
-__device__ __forceinline__ v2 exp2_unbiased(v2 E) {
+// ~1e3 times.  So the residual pass evaluates 2^E, E = Q * (KEXP + KEXP_LO),
+// with Cody and Waite's range reduction E = n + f:
+//   n = rint(Q * KEXP), the rounding done by one FMA with 1.5*2^23, whose
+//       low mantissa bits then hold n;
+//   f = (Q * KEXP - n) + Q * KEXP_LO, two FMAs, the first forming the product
+//       exactly, so that f (|f| <= 1/2 + 4e-7) carries one rounding of a
+//       number below 1/2 rather than the rounding of E itself (up to 1e-6
+//       absolute at E = -26);
+// then a degree-6 polynomial for 2^f (coefficients fitted here by relative
+// least squares with the constant term pinned to 1: mean relative error
+// 6e-10, max 8e-8 in float) and scaling by 2^n through the exponent field.
+// Arguments above 174 give garbage that callers discard (they select 0 for
+// exp-arguments above the cutoff, and never use the value at pixels outside
+// the culling box).
+__device__ __forceinline__ v2 exp_neg_half(v2 Q, v2 KEXP2, v2 KEXPLO2) {
     const float MAGIC = 12582912.0f;  // 1.5 * 2^23
-    const v2 t = add2(E, pk1(MAGIC));
-    // n = t - MAGIC is exact, so MAGIC - t (one FMA, no sign-bit operation) is
-    // -n, up to the sign of a zero, which the polynomial does not see (2^(+-0) = 1)
-    const v2 f = add2(E, fma2(t, pk1(-1.0f), pk1(MAGIC)));  // E - n
+    const v2 t = fma2(Q, KEXP2, pk1(MAGIC));
+    // MAGIC - t (one FMA, no sign-bit operation) is -n exactly
+    const v2 f = fma2(Q, KEXPLO2, fma2(Q, KEXP2, fma2(t, pk1(-1.0f), pk1(MAGIC))));
     v2 p = pk1(1.5370704932138324e-04f);
     p = fma2(p, f, pk1(1.3399848248809576e-03f));
     p = fma2(p, f, pk1(9.618373587727547e-03f));

@@ -224,8 +224,8 @@ __device__ __forceinline__ void residual_pairs(const v2 (&X)[KP], const v2 (&Y)[
         const v2 VX = fma2(FXY, DY, mul2(FXX, DX));
         const v2 VY = fma2(FXY, DX, mul2(FYY, DY));
         const v2 Q = fma2(DY, VY, mul2(DX, VX));
-        // the residual needs an unbiased exponential (see exp2_unbiased)
-        v2 Gp = exp2_unbiased(fma2(Q, KEXP2, mul2(Q, KEXPLO2)));
+        // the residual needs an unbiased exponential (see exp_neg_half)
+        v2 Gp = exp_neg_half(Q, KEXP2, KEXPLO2);
         if (CUT) {
             float g0, g1, q0, q1;
             unpk(Gp, g0, g1);
@@ -270,8 +270,8 @@ __device__ __forceinline__ void residual_pairs2(const v2 (&X)[KP], const v2 (&Y)
         const v2 VYb = fma2(FXYb, DXb, mul2(FYYb, DYb));
         const v2 Qa = fma2(DYa, VYa, mul2(DXa, VXa));
         const v2 Qb = fma2(DYb, VYb, mul2(DXb, VXb));
-        v2 Ga = exp2_unbiased(fma2(Qa, KEXP2, mul2(Qa, KEXPLO2)));
-        v2 Gb = exp2_unbiased(fma2(Qb, KEXP2, mul2(Qb, KEXPLO2)));
+        v2 Ga = exp_neg_half(Qa, KEXP2, KEXPLO2);
+        v2 Gb = exp_neg_half(Qb, KEXP2, KEXPLO2);
         {
             float g0, g1, q0, q1;
             unpk(Ga, g0, g1);
@@ -1055,8 +1055,8 @@ __device__ __forceinline__ void design_pairs2(const v2 (&Xp)[KP], const v2 (&Yp)
         const v2 VYb = fma2(FXYb, DXb, mul2(FYYb, DYb));
         const v2 Qa = fma2(DYa, VYa, mul2(DXa, VXa));
         const v2 Qb = fma2(DYb, VYb, mul2(DXb, VXb));
-        v2 Ga = exp2_unbiased(fma2(Qa, KEXP2, mul2(Qa, KEXPLO2)));
-        v2 Gb = exp2_unbiased(fma2(Qb, KEXP2, mul2(Qb, KEXPLO2)));
+        v2 Ga = exp_neg_half(Qa, KEXP2, KEXPLO2);
+        v2 Gb = exp_neg_half(Qb, KEXP2, KEXPLO2);
         {
             float g0, g1, q0, q1;
             unpk(Ga, g0, g1);
