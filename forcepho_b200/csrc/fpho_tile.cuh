@@ -330,7 +330,8 @@ __device__ __forceinline__ void residual_exact(const v2 (&X)[KP], const v2 (&Y)[
 // v = F d): sum W H, sum W H v, sum W v, sum W H d d^T, sum W, and sum W d d^T.
 // The epilogue forms sum W d.v terms from sum W d d^T and F once per
 // Gaussian (d_x v_x = fxx dx^2 + fxy dx dy, and so on), which is one packed
-// instruction per pixel pair cheaper than summing them per pixel.
+// instruction per pixel pair cheaper than summing them per pixel; the
+// products dx^2, dx dy, dy^2 are formed once and weighted by both W H and W.
 struct GradSums {
     v2 A, HVx, HVy, Vx, Vy, HXX, HXY, HYY, W, WXX, WXY, WYY;
 };
@@ -365,15 +366,14 @@ __device__ __forceinline__ void gradient_pairs(const v2 (&X)[KP], const v2 (&Y)[
         s.HVy = fma2(WH, VY, s.HVy);
         s.Vx = fma2(W, VX, s.Vx);
         s.Vy = fma2(W, VY, s.Vy);
-        const v2 HDX = mul2(WH, DX);
-        s.HXX = fma2(HDX, DX, s.HXX);
-        s.HXY = fma2(HDX, DY, s.HXY);
-        s.HYY = fma2(mul2(WH, DY), DY, s.HYY);
+        const v2 DXX = mul2(DX, DX), DXY = mul2(DX, DY), DYY = mul2(DY, DY);
+        s.HXX = fma2(WH, DXX, s.HXX);
+        s.HXY = fma2(WH, DXY, s.HXY);
+        s.HYY = fma2(WH, DYY, s.HYY);
         s.W = add2(s.W, W);
-        const v2 WDX = mul2(W, DX);
-        s.WXX = fma2(WDX, DX, s.WXX);
-        s.WXY = fma2(WDX, DY, s.WXY);
-        s.WYY = fma2(mul2(W, DY), DY, s.WYY);
+        s.WXX = fma2(W, DXX, s.WXX);
+        s.WXY = fma2(W, DXY, s.WXY);
+        s.WYY = fma2(W, DYY, s.WYY);
     }
 }
 
@@ -430,22 +430,22 @@ __device__ __forceinline__ void gradient_pairs2(const v2 (&X)[KP], const v2 (&Y)
         sb.Vx = fma2(Wb, VXb, sb.Vx);
         sa.Vy = fma2(Wa, VYa, sa.Vy);
         sb.Vy = fma2(Wb, VYb, sb.Vy);
-        const v2 HDXa = mul2(WHa, DXa), HDXb = mul2(WHb, DXb);
-        sa.HXX = fma2(HDXa, DXa, sa.HXX);
-        sb.HXX = fma2(HDXb, DXb, sb.HXX);
-        sa.HXY = fma2(HDXa, DYa, sa.HXY);
-        sb.HXY = fma2(HDXb, DYb, sb.HXY);
-        sa.HYY = fma2(mul2(WHa, DYa), DYa, sa.HYY);
-        sb.HYY = fma2(mul2(WHb, DYb), DYb, sb.HYY);
+        const v2 DXXa = mul2(DXa, DXa), DXYa = mul2(DXa, DYa), DYYa = mul2(DYa, DYa);
+        const v2 DXXb = mul2(DXb, DXb), DXYb = mul2(DXb, DYb), DYYb = mul2(DYb, DYb);
+        sa.HXX = fma2(WHa, DXXa, sa.HXX);
+        sb.HXX = fma2(WHb, DXXb, sb.HXX);
+        sa.HXY = fma2(WHa, DXYa, sa.HXY);
+        sb.HXY = fma2(WHb, DXYb, sb.HXY);
+        sa.HYY = fma2(WHa, DYYa, sa.HYY);
+        sb.HYY = fma2(WHb, DYYb, sb.HYY);
         sa.W = add2(sa.W, Wa);
         sb.W = add2(sb.W, Wb);
-        const v2 WDXa = mul2(Wa, DXa), WDXb = mul2(Wb, DXb);
-        sa.WXX = fma2(WDXa, DXa, sa.WXX);
-        sb.WXX = fma2(WDXb, DXb, sb.WXX);
-        sa.WXY = fma2(WDXa, DYa, sa.WXY);
-        sb.WXY = fma2(WDXb, DYb, sb.WXY);
-        sa.WYY = fma2(mul2(Wa, DYa), DYa, sa.WYY);
-        sb.WYY = fma2(mul2(Wb, DYb), DYb, sb.WYY);
+        sa.WXX = fma2(Wa, DXXa, sa.WXX);
+        sb.WXX = fma2(Wb, DXXb, sb.WXX);
+        sa.WXY = fma2(Wa, DXYa, sa.WXY);
+        sb.WXY = fma2(Wb, DXYb, sb.WXY);
+        sa.WYY = fma2(Wa, DYYa, sa.WYY);
+        sb.WYY = fma2(Wb, DYYb, sb.WYY);
     }
 }
 
