@@ -7,7 +7,8 @@
 //      reference's per-pixel `exparg > 36` skip, which is still applied to
 //      every Gaussian that can cross the threshold inside the tile);
 //   2. stage the kept 128-byte records into shared memory with cp.async.bulk
-//      (one bulk copy per record, completion on an mbarrier);
+//      (one bulk copy per record, issued by every thread of the CTA,
+//      completion on an mbarrier);
 //   3. residual pass: r = data - sum_g amp G H over kept Gaussians, in the
 //      reference's Gaussian order (ComputeResidualImage, common_kernel.cc:57-83);
 //   4. chi2 per pixel in double, exactly as compute_gaussians_kernel.cc:286-293;
