@@ -51,6 +51,35 @@ __device__ __forceinline__ void upper_pair(int p, int ns, int &s, int &t) {
     t = s + p;
 }
 
+// A tile's partial normal equations from its unit-flux rows (ns rows of
+// TP + 1 floats), weights ws and data ys: the upper triangle of
+// sum w^2 X_s X_t, then sum w^2 X_s y, each term summed in FP64 over the
+// tile's pixels in order.  Every thread of the CTA takes terms.
+template <int NT, int TP>
+__device__ __forceinline__ void tile_normal_partials(const float *rows, const float *ws,
+                                                     const float *ys, int ns, int count,
+                                                     int n_terms, double *out) {
+    const int n_pairs = ns * (ns + 1) / 2;
+    for (int p = threadIdx.x; p < n_terms; p += NT) {
+        int s, t;
+        const float *other;
+        if (p < n_pairs) {
+            upper_pair(p, ns, s, t);
+            other = rows + (size_t)t * (TP + 1);
+        } else {
+            s = p - n_pairs;
+            other = ys;
+        }
+        const float *xs_ = rows + (size_t)s * (TP + 1);
+        double acc = 0.0;
+        for (int li = 0; li < count; ++li) {
+            const double w = (double)ws[li];
+            acc = fma(w * w * (double)xs_[li], (double)other[li], acc);
+        }
+        out[p] = acc;
+    }
+}
+
 template <int NT, int K>
 __global__ void __launch_bounds__(NT) normal_tiles(TileArgs A, double *pnorm, int n_terms) {
     static_assert(K % 2 == 0, "pixels per thread must be even (packed pairs)");
@@ -138,26 +167,8 @@ __global__ void __launch_bounds__(NT) normal_tiles(TileArgs A, double *pnorm, in
         }
     }
     __syncthreads();
-    // tile partials: the upper triangle of sum w^2 X_s X_t, then sum w^2 X_s y
-    const int n_pairs = ns * (ns + 1) / 2;
-    for (int p = tid; p < n_terms; p += NT) {
-        int s, t;
-        const float *other;
-        if (p < n_pairs) {
-            upper_pair(p, ns, s, t);
-            other = rows + (size_t)t * (TP + 1);
-        } else {
-            s = p - n_pairs;
-            other = ys;
-        }
-        const float *xs_ = rows + (size_t)s * (TP + 1);
-        double acc = 0.0;
-        for (int li = 0; li < td.count; ++li) {
-            const double w = (double)ws[li];
-            acc = fma(w * w * (double)xs_[li], (double)other[li], acc);
-        }
-        pnorm[(size_t)tile * n_terms + p] = acc;
-    }
+    tile_normal_partials<NT, TP>(rows, ws, ys, ns, td.count, n_terms,
+                                 pnorm + (size_t)tile * n_terms);
 }
 
 // grid (n_bands, ceil(n_terms / 128)): ATA[b] (both triangles) and ATb[b]
@@ -230,7 +241,10 @@ __global__ void __launch_bounds__(64) normal_solve(const double *ata, const doub
 
 // the normal-equation kernel for a plan's tile size: four pixels per thread
 // (two pixel pairs, two Gaussians interleaved: four independent exponential
-// chains); whole warps, so the 192-pixel tile takes six pixels per thread
+// chains); whole warps, so the 192-pixel tile takes six pixels per thread.
+// (A form with 4 warps of 8 pixels per thread sharing each 256-pixel tile's
+// Gaussians, as the split tile kernels do, measured no faster: 0.430 against
+// 0.427 ms for the 20-source patch.)
 struct NormalShape {
     int tile, nt;
     const void *fn;
