@@ -74,6 +74,9 @@ def parse():
                     help="0: one CTA per tile; 1: persistent CTAs, costliest tiles first")
     ap.add_argument("--batch-patches", type=int, default=256,
                     help="patches of the batched leg (uneven patches); 0 skips it")
+    ap.add_argument("--batch-config", default=None, metavar="VARIANT,LIVE_CAP,CTAS_PER_SM",
+                    help="launch configuration of the batched leg (default: the batch "
+                         "autotuner's choice)")
     ap.add_argument("--chains", type=int, default=256,
                     help="HMC chains of the multi-chain leg (single-source patch); 0 skips it")
     ap.add_argument("--no-differentiable", action="store_true",
@@ -270,7 +273,11 @@ def batched_leg(args, torch, lib, steps):
     # the batch autotuner: tile variant, stage size and persistent-grid cap,
     # timed on this batch (cached by the batch's signature)
     from forcepho_b200.autotune import choose_batch_config
-    bcfg = choose_batch_config(patches)
+    if args.batch_config:
+        v, lc, c = (int(x) for x in args.batch_config.split(","))
+        bcfg = {"variant": v, "live_cap": lc, "ctas_per_sm": c}
+    else:
+        bcfg = choose_batch_config(patches)
     batch = PatchBatch(patches, config=bcfg)
     dprop, chi2, dchi2 = batch.device_buffers()
     s = torch.cuda.current_stream()
