@@ -108,6 +108,11 @@ _SIGS = {
     "fpho_build_proposal_batch": (c_int, [c_void_p, c_void_p, c_int, c_void_p, c_void_p,
                                           c_void_p, c_void_p]),
     "fpho_spline_points": (c_int, [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p]),
+    "fpho_build_proposal_bounded": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int,
+                                            c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "fpho_bounded_lnp_grad": (c_int, [c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
+                                      c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_void_p,
+                                      c_int, c_void_p, c_void_p]),
     "fpho_patch_time_tiles": (c_int, [c_void_p, c_int]),
     "fpho_patch_image_gaussians": (c_int, [c_void_p, c_int, c_void_p, c_int,
                                            ctypes.POINTER(c_int)]),

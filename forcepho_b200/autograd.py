@@ -82,6 +82,14 @@ class PatchEvaluator:
                   NPARAMS * self.n_sources, flags, _stream())
         self.generation += 1
 
+    def evaluate(self, grad=True):
+        """Enqueue one evaluation of the proposal already in ``self.prop``."""
+        flags = 0 if grad else _lib.FPHO_CHI2_ONLY
+        _lib.call("fpho_evaluate_proposal", self.handle, self.prop.data_ptr(), self.n_sources,
+                  self.chi2.data_ptr(), self.dchi2.data_ptr() if grad else None,
+                  NPARAMS * self.n_sources, flags, _stream())
+        self.generation += 1
+
     def stacked(self):
         """d chi2 / d theta of the last gradient run, (n_sources, n_bands + 6)."""
         return stack_grad(self.dchi2, self.n_bands, self.n_sources)
@@ -141,6 +149,44 @@ def default_bounds(params, n_bands, pixscale=0.03, n_pix=2.0, flux_frac=0.25,
     return lo.reshape(-1), hi.reshape(-1)
 
 
+def _param_maps(n_params, dst, src):
+    """CSR form (offsets int32 [n_params + 1], indices int64) of the dchi2
+    entries of each parameter, from pairs (dst[k], src[k]) grouped by
+    parameter in their given order."""
+    dst = np.asarray(dst, dtype=np.int64)
+    src = np.asarray(src, dtype=np.int64)
+    order = np.argsort(dst, kind="stable")
+    counts = np.bincount(dst, minlength=n_params)
+    off = np.concatenate([[0], np.cumsum(counts)]).astype(np.int32)
+    return off, src[order]
+
+
+class _LnpGrad:
+    """lnp(z) and d lnp / dz in one launch (fpho_bounded_lnp_grad) from an
+    evaluation's chi2 and dchi2, for a bounded transform `tr` and the
+    parameters' dchi2 maps."""
+
+    def __init__(self, tr, n_params, dst, src):
+        off, idx = _param_maps(n_params, dst, src)
+        self.tr, self.n = tr, int(n_params)
+        self.off = torch.as_tensor(off, device="cuda")
+        self.idx = torch.as_tensor(idx, device="cuda")
+        self.work = torch.zeros((self.n + 255) // 256, dtype=torch.float64, device="cuda")
+        self.counter = torch.zeros(1, dtype=torch.int32, device="cuda")
+
+    def __call__(self, z, dchi2, chi2):
+        if z.dtype != torch.float64 or not z.is_cuda or not z.is_contiguous():
+            raise TypeError("z must be a contiguous float64 CUDA tensor")
+        g = torch.empty(self.n, dtype=torch.float64, device="cuda")
+        lnp = torch.empty((), dtype=torch.float64, device="cuda")
+        _lib.call("fpho_bounded_lnp_grad", self.n, z.data_ptr(), self.tr.lower.data_ptr(),
+                  self.tr.range.data_ptr(), dchi2.data_ptr(), self.off.data_ptr(),
+                  self.idx.data_ptr(), chi2.data_ptr(), chi2.numel(), g.data_ptr(),
+                  lnp.data_ptr(), self.work.data_ptr(), self.work.numel(),
+                  self.counter.data_ptr(), _stream())
+        return lnp, g
+
+
 class _Bounded:
     """BoundedTransform on the device: q = lower + range * sigmoid(z)."""
 
@@ -173,6 +219,20 @@ class DevicePosterior:
             raise ValueError(f"bounds have {self.tr.lower.numel()} entries, the patch has "
                              f"{self.ev.n_params} parameters")
         self.ndim = self.ev.n_params
+        # parameter (s, j) of Scene order <- dchi2 entries (band b, source s, k)
+        nb, ns = self.ev.n_bands, self.ev.n_sources
+        dst, src = [], []
+        for s in range(ns):
+            for j in range(nb + 6):
+                i = s * (nb + 6) + j
+                if j < nb:
+                    dst.append(i)
+                    src.append((j * ns + s) * NPARAMS)
+                else:
+                    for b in range(nb):
+                        dst.append(i)
+                        src.append((b * ns + s) * NPARAMS + j - nb + 1)
+        self._lnpg = _LnpGrad(self.tr, self.ndim, dst, src)
 
     def transform(self, z):
         return self.tr.transform(z)
@@ -186,6 +246,18 @@ class DevicePosterior:
         return LnLike.apply(q, self.ev) + torch.log(self.tr.range * s * (1.0 - s)).sum()
 
     def lnprob_and_grad(self, z):
+        """(lnp, d lnp / dz) at z: the transform and the proposal build in one
+        launch, the evaluation, and lnp with its gradient in one launch."""
+        z = z.contiguous()
+        ev = self.ev
+        _lib.call("fpho_build_proposal_bounded", ev.table.handle, z.data_ptr(),
+                  self.tr.lower.data_ptr(), self.tr.range.data_ptr(), ev.n_sources, ev.n_bands,
+                  None, None, None, ev.prop.data_ptr(), _stream())
+        ev.evaluate(grad=True)
+        return self._lnpg(z, ev.dchi2, ev.chi2)
+
+    def _lnprob_and_grad_torch(self, z):
+        """The same from torch elementwise operations (the unfused form)."""
         s = torch.sigmoid(z)
         q = self.tr.lower + self.tr.range * s
         jac = self.tr.range * s * (1.0 - s)
@@ -239,6 +311,7 @@ class BatchPosterior:
                         shape_src.append(src + j)
             g0 += b_ * s_ * NPARAMS
         cuda = lambda a: torch.as_tensor(np.asarray(a, dtype=np.int64), device="cuda")
+        self._lnpg = _LnpGrad(self.tr, self.ndim, flux_dst + shape_dst, flux_src + shape_src)
         self.flux_dst, self.flux_src = cuda(flux_dst), cuda(flux_src)
         # shape gradients: each parameter sums its patch's bands; a padded
         # gather (index n_dchi2 points at an appended zero) keeps the sum
@@ -272,6 +345,18 @@ class BatchPosterior:
         return self.tr.inverse_transform(q)
 
     def lnprob_and_grad(self, z):
+        """(lnp, d lnp / dz) at z in four launches: transform and proposals,
+        image Gaussians + tiles + reductions of the batch, lnp and gradient."""
+        z = z.contiguous()
+        _lib.call("fpho_build_proposal_bounded", self.table.handle, z.data_ptr(),
+                  self.tr.lower.data_ptr(), self.tr.range.data_ptr(), self.src_bands.numel(), 0,
+                  self.src_bands.data_ptr(), self.src_off.data_ptr(), None, self.prop.data_ptr(),
+                  _stream())
+        self.batch.evaluate_device(self.prop, self.chi2, self.dchi2, _stream())
+        return self._lnpg(z, self.dchi2, self.chi2)
+
+    def _lnprob_and_grad_torch(self, z):
+        """The same from torch elementwise operations (the unfused form)."""
         s = torch.sigmoid(z)
         q = self.tr.lower + self.tr.range * s
         jac = self.tr.range * s * (1.0 - s)

@@ -81,12 +81,22 @@ struct SplineView {
     double sersic_min;
 };
 
-// value, d/dx (sersic), d/dy (rh) of spline `k` at (x, y)
-__device__ void spline_eval(const SplineView &S, int k, double x, double y, double out[3]) {
+// The B-spline bases at (x, y), shared by every radius's spline (all the
+// mixture radii's splines have the same knots).
+struct SplineBasis {
     int lx, ly;
     double Bx[4], dBx[4], By[4], dBy[4];
-    cubic_basis(S.tx, S.ntx, x, lx, Bx, dBx);
-    cubic_basis(S.ty, S.nty, y, ly, By, dBy);
+};
+__device__ void spline_basis(const SplineView &S, double x, double y, SplineBasis &b) {
+    cubic_basis(S.tx, S.ntx, x, b.lx, b.Bx, b.dBx);
+    cubic_basis(S.ty, S.nty, y, b.ly, b.By, b.dBy);
+}
+
+// value, d/dx (sersic), d/dy (rh) of spline `k` from the bases at (x, y)
+__device__ void spline_combine(const SplineView &S, int k, const SplineBasis &sb,
+                               double out[3]) {
+    const int lx = sb.lx, ly = sb.ly;
+    const double *Bx = sb.Bx, *dBx = sb.dBx, *By = sb.By, *dBy = sb.dBy;
     const int ncy = S.nty - 4;
     const double *c = S.coef + (size_t)k * (S.ntx - 4) * ncy;
     double v = 0.0, vx = 0.0, vy = 0.0;
@@ -106,18 +116,21 @@ __device__ void spline_eval(const SplineView &S, int k, double x, double y, doub
     out[2] = vy;
 }
 
+// value, d/dx (sersic), d/dy (rh) of spline `k` at (x, y)
+__device__ void spline_eval(const SplineView &S, int k, double x, double y, double out[3]) {
+    SplineBasis sb;
+    spline_basis(S, x, y, sb);
+    spline_combine(S, k, sb, out);
+}
+
 // One thread per source: parameters in the reference's Scene order
 // [flux_1..flux_B, ra, dec, q, pa, sersic, rhalf] -> fpho_source.
 // With `src_bands` / `src_off` (batched form) source s has src_bands[s] bands
 // and its parameters start at theta[src_off[s]]; otherwise every source has
 // `n_bands` bands and a stride of n_bands + 6.
-__global__ void build_proposal_kernel(SplineView S, const double *theta, int n_src, int n_bands,
-                                      const int *src_bands, const long long *src_off,
-                                      fpho_source *out) {
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= n_src) return;
-    if (src_bands) n_bands = src_bands[s];
-    const double *p = theta + (src_off ? (size_t)src_off[s] : (size_t)s * (n_bands + 6));
+// One source from its parameters p[n_bands + 6] (Scene order).
+__device__ void build_source(const SplineView &S, const double *p, int n_bands,
+                             fpho_source *dst) {
     fpho_source src;
     memset(&src, 0, sizeof(src));
     for (int b = 0; b < n_bands; ++b) src.fluxes[b] = (float)p[b];
@@ -139,15 +152,128 @@ __global__ void build_proposal_kernel(SplineView S, const double *theta, int n_s
     } else if (rh < 0.0) {      // sources.py:661-663
         src.mixture_amplitudes[0] = 1.0f;
     } else {
+        // one basis for all radii: the knot searches are dependent global
+        // loads, so evaluating them once per source instead of once per
+        // radius is what the kernel's time is made of
+        SplineBasis sb;
+        spline_basis(S, nser, rh, sb);
         for (int k = 0; k < S.n_radii; ++k) {
             double v[3];
-            spline_eval(S, k, nser, rh, v);
+            spline_combine(S, k, sb, v);
             src.mixture_amplitudes[k] = (float)v[0];
             src.damplitude_dnsersic[k] = (float)v[1];
             src.damplitude_drh[k] = (float)v[2];
         }
     }
-    out[s] = src;
+    *dst = src;
+}
+
+// The knot vectors in shared memory: the binary searches of the bases then
+// wait on shared-memory loads instead of dependent global ones.  Every thread
+// of the block calls it (a barrier).
+__device__ __forceinline__ SplineView knots_to_shared(const SplineView &S, double *s_tx,
+                                                      double *s_ty) {
+    for (int i = threadIdx.x; i < S.ntx; i += blockDim.x) s_tx[i] = S.tx[i];
+    for (int i = threadIdx.x; i < S.nty; i += blockDim.x) s_ty[i] = S.ty[i];
+    __syncthreads();
+    SplineView L = S;
+    L.tx = s_tx;
+    L.ty = s_ty;
+    return L;
+}
+
+__global__ void build_proposal_kernel(SplineView S, const double *theta, int n_src, int n_bands,
+                                      const int *src_bands, const long long *src_off,
+                                      fpho_source *out) {
+    __shared__ double s_tx[SPL_MAX_KNOTS], s_ty[SPL_MAX_KNOTS];
+    const SplineView L = knots_to_shared(S, s_tx, s_ty);
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n_src) return;
+    if (src_bands) n_bands = src_bands[s];
+    const double *p = theta + (src_off ? (size_t)src_off[s] : (size_t)s * (n_bands + 6));
+    build_source(L, p, n_bands, out + s);
+}
+
+// sigmoid in double, as torch.sigmoid evaluates it
+__device__ __forceinline__ double sigmoid_d(double z) { return 1.0 / (1.0 + exp(-z)); }
+
+// The same from unconstrained parameters z through the bounded transform
+// q = lower + range * sigmoid(z) (BoundedTransform.transform,
+// forcepho/model.py:596-637), one thread per source; q is also stored when
+// q_out is not NULL.
+__global__ void build_proposal_bounded_kernel(SplineView S, const double *z, const double *lower,
+                                              const double *range, int n_src, int n_bands,
+                                              const int *src_bands, const long long *src_off,
+                                              double *q_out, fpho_source *out) {
+    __shared__ double s_tx[SPL_MAX_KNOTS], s_ty[SPL_MAX_KNOTS];
+    const SplineView L = knots_to_shared(S, s_tx, s_ty);
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= n_src) return;
+    if (src_bands) n_bands = src_bands[s];
+    const size_t o = src_off ? (size_t)src_off[s] : (size_t)s * (n_bands + 6);
+    double q[FPHO_MAXBANDS + 6];
+    for (int i = 0; i < n_bands + 6; ++i) {
+        q[i] = lower[o + i] + range[o + i] * sigmoid_d(z[o + i]);
+        if (q_out) q_out[o + i] = q[i];
+    }
+    build_source(L, q, n_bands, out + s);
+}
+
+// lnp(z) = -chi2/2 + sum_i log jac_i and its gradient w.r.t. z, with
+// jac_i = range_i s_i (1 - s_i), s_i = sigmoid(z_i) (FastPosterior.evaluate
+// and BoundedTransform, forcepho/model.py:323-387, 596-637):
+//   grad_i = -jac_i / 2 * sum_{k in map[i]} dchi2[k] + (1 - 2 s_i),
+// the map of parameter i listing its dchi2 entries (a flux: one band; a shape
+// parameter: every band of its patch, in band order), summed in double.  Each
+// block writes the sum of its log jac terms; the last block to finish (a
+// counter, reset for the next call) adds the partials and the chi2 in order.
+constexpr int LNP_THREADS = 256;
+__global__ void __launch_bounds__(LNP_THREADS) bounded_lnp_grad_kernel(
+    int n, const double *z, const double *lower, const double *range, const float *dchi2,
+    const int *map_off, const long long *map_idx, const double *chi2, int n_chi2, double *grad,
+    double *lnp, double *partial, unsigned *counter) {
+    __shared__ double red[LNP_THREADS];
+    __shared__ bool last;
+    const int i = blockIdx.x * LNP_THREADS + threadIdx.x;
+    double lj = 0.0;
+    if (i < n) {
+        double gq = 0.0;
+        for (int k = map_off[i]; k < map_off[i + 1]; ++k) gq += (double)dchi2[map_idx[k]];
+        const double sg = sigmoid_d(z[i]);
+        const double jac = range[i] * sg * (1.0 - sg);
+        grad[i] = gq * (-0.5 * jac) + (1.0 - 2.0 * sg);
+        lj = log(jac);
+    }
+    red[threadIdx.x] = lj;
+    __syncthreads();
+    for (int w = LNP_THREADS / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        partial[blockIdx.x] = red[0];
+        __threadfence();
+        last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    // the last block: -chi2/2 + the partials, each thread a strided share in
+    // order, then the same tree as above
+    __threadfence();
+    double c = 0.0, l = 0.0;
+    for (int b = threadIdx.x; b < n_chi2; b += LNP_THREADS) c += chi2[b];
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += LNP_THREADS)
+        l += ((volatile double *)partial)[b];
+    red[threadIdx.x] = -0.5 * c + l;
+    __syncthreads();
+    for (int w = LNP_THREADS / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        *lnp = red[0];
+        *counter = 0u;
+    }
 }
 
 // Spline values and derivatives at arbitrary points (for validation).
@@ -256,6 +382,47 @@ extern "C" int fpho_spline_points(const fpho_spline *s, const double *x, const d
     if (n > 0)
         spline_points_kernel<<<(n + 127) / 128, 128, 0, (cudaStream_t)stream>>>(s->view, x, y, m,
                                                                                out);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return set_error(FPHO_ERR_CUDA, "launch: %s", cudaGetErrorString(e));
+    return FPHO_OK;
+}
+
+extern "C" int fpho_build_proposal_bounded(const fpho_spline *s, const double *z,
+                                           const double *lower, const double *range,
+                                           int n_sources, int n_bands, const int *src_bands,
+                                           const long long *src_offset, double *q_out,
+                                           fpho_source *out, void *stream) {
+    clear_error();
+    if (!s || !z || !lower || !range || !out) return set_error(FPHO_ERR_INVALID, "NULL argument");
+    if (n_sources < 1) return set_error(FPHO_ERR_INVALID, "n_sources=%d < 1", n_sources);
+    if (!src_bands != !src_offset)
+        return set_error(FPHO_ERR_INVALID, "src_bands and src_offset go together");
+    if (!src_bands && (n_bands < 1 || n_bands > FPHO_MAXBANDS))
+        return set_error(FPHO_ERR_LIMIT, "n_bands=%d outside [1, %d]", n_bands, FPHO_MAXBANDS);
+    build_proposal_bounded_kernel<<<(n_sources + 63) / 64, 64, 0, (cudaStream_t)stream>>>(
+        s->view, z, lower, range, n_sources, n_bands, src_bands, src_offset, q_out, out);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return set_error(FPHO_ERR_CUDA, "launch: %s", cudaGetErrorString(e));
+    return FPHO_OK;
+}
+
+extern "C" int fpho_bounded_lnp_grad(int n_params, const double *z, const double *lower,
+                                     const double *range, const float *dchi2,
+                                     const int *map_offset, const long long *map_index,
+                                     const double *chi2, int n_chi2, double *grad_out,
+                                     double *lnp_out, double *work, int n_work,
+                                     unsigned *counter, void *stream) {
+    clear_error();
+    if (n_params < 1 || n_chi2 < 0) return set_error(FPHO_ERR_INVALID, "bad sizes");
+    if (!z || !lower || !range || !dchi2 || !map_offset || !map_index || (n_chi2 && !chi2) ||
+        !grad_out || !lnp_out || !work || !counter)
+        return set_error(FPHO_ERR_INVALID, "NULL argument");
+    const int blocks = (n_params + LNP_THREADS - 1) / LNP_THREADS;
+    if (n_work < blocks)
+        return set_error(FPHO_ERR_LIMIT, "work holds %d partials, %d needed", n_work, blocks);
+    bounded_lnp_grad_kernel<<<blocks, LNP_THREADS, 0, (cudaStream_t)stream>>>(
+        n_params, z, lower, range, dchi2, map_offset, map_index, chi2, n_chi2, grad_out, lnp_out,
+        work, counter);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return set_error(FPHO_ERR_CUDA, "launch: %s", cudaGetErrorString(e));
     return FPHO_OK;

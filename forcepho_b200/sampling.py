@@ -50,11 +50,20 @@ class ChainCopy:
         self.device_patch.free()
 
 
-def chain_posterior(patch, n_chains, lower, upper, live_cap=128):
+def chain_posterior(patch, n_chains, lower, upper, live_cap=128, config=None):
     """A BatchPosterior over `n_chains` device copies of `patch` with the
-    same bounds: chain k's parameters are the k-th block of z."""
+    same bounds: chain k's parameters are the k-th block of z.  `config`: the
+    batched launch configuration (a dict as from
+    :func:`forcepho_b200.autotune.choose_batch_config`, or "tune" to have the
+    batch autotuner choose it for these copies); None keeps the batch default
+    with `live_cap` records per stage."""
     copies = [ChainCopy(patch) for _ in range(n_chains)]
-    batch = PatchBatch(copies, live_cap=live_cap)
+    if isinstance(config, str):
+        if config != "tune":
+            raise ValueError(f"config must be a dict, 'tune' or None, not {config!r}")
+        from .autotune import choose_batch_config
+        config = choose_batch_config(copies)
+    batch = PatchBatch(copies, live_cap=live_cap, config=config)
     post = BatchPosterior(batch, [lower] * n_chains, [upper] * n_chains)
     post.copies = copies
     return post

@@ -237,6 +237,39 @@ FPHO_API int fpho_build_proposal_batch(const fpho_spline *s, const double *theta
                                        const int *src_bands, const long long *src_offset,
                                        fpho_source *out, void *stream);
 
+/* The proposal from unconstrained parameters: q = lower + range *
+ * sigmoid(z) per parameter (BoundedTransform.transform,
+ * forcepho/model.py:596-637), then as fpho_build_proposal (src_bands and
+ * src_offset NULL: every source has n_bands bands, stride n_bands + 6) or
+ * fpho_build_proposal_batch (both given; n_bands ignored).  z, lower, range
+ * (= upper - lower) and the optional q_out are device arrays in the
+ * parameters' Scene order.  One launch replaces the transform and the
+ * proposal build of a sampler step. */
+FPHO_API int fpho_build_proposal_bounded(const fpho_spline *s, const double *z,
+                                         const double *lower, const double *range,
+                                         int n_sources, int n_bands, const int *src_bands,
+                                         const long long *src_offset, double *q_out,
+                                         fpho_source *out, void *stream);
+
+/* lnp(z) = -sum(chi2)/2 + sum_i log jac_i and d lnp / dz_i
+ *   = -jac_i / 2 * sum_{k = map_offset[i]}^{map_offset[i+1]-1} dchi2[map_index[k]]
+ *     + (1 - 2 s_i),
+ * s_i = sigmoid(z_i), jac_i = range_i s_i (1 - s_i) (FastPosterior.evaluate
+ * with BoundedTransform, forcepho/model.py:323-387, 596-637).  The map lists
+ * each parameter's entries of the evaluation's dchi2 (a flux: its band; a
+ * shape parameter: every band, in band order; summed in double), so that it
+ * also stacks the per-band gradient as stack_grad (forcepho/model.py:387-405)
+ * does.  work[n_work] holds one partial per 256 parameters; *counter
+ * (device, zero before the first call) is reset by every call.  The lnp sum
+ * is in a fixed order.  One launch, in place of the transform's and the
+ * stacking's elementwise steps. */
+FPHO_API int fpho_bounded_lnp_grad(int n_params, const double *z, const double *lower,
+                                   const double *range, const float *dchi2,
+                                   const int *map_offset, const long long *map_index,
+                                   const double *chi2, int n_chi2, double *grad_out,
+                                   double *lnp_out, double *work, int n_work,
+                                   unsigned *counter, void *stream);
+
 /* Spline values and derivatives at m device points (x = sersic, y = rh):
  * out[m][n_radii][3] = (value, d/dsersic, d/drh). */
 FPHO_API int fpho_spline_points(const fpho_spline *s, const double *x, const double *y, int m,

@@ -278,7 +278,9 @@ def test_lnprob_and_grad_equals_autograd():
     zz = z.clone().requires_grad_(True)
     lnp2 = post.lnprob(zz)
     (g2,) = torch.autograd.grad(lnp2, zz)
-    assert float(lnp) == float(lnp2)
+    # lnprob_and_grad sums lnp in its own fixed order (fpho_bounded_lnp_grad),
+    # torch's autograd path in torch's: equal to rounding
+    assert abs(float(lnp) - float(lnp2)) <= 1e-14 * abs(float(lnp2))
     np.testing.assert_allclose(g.cpu().numpy(), g2.cpu().numpy(), rtol=1e-13, atol=0)
     P.free()
 

@@ -115,3 +115,14 @@ def test_run_hmc_adapts_mass(full):
     v = chain.transpose(1, 0, 2).reshape(300, -1).var(axis=0).reshape(T.k, T.d).mean(axis=0)
     np.testing.assert_allclose(v / np.diag(C), 1.0, atol=0.2)
     assert res.accept.mean() > 0.5
+
+
+def test_param_maps_group_in_order():
+    """The CSR maps of the fused gradient keep each parameter's entries in the
+    order given (band order for the shape parameters)."""
+    from forcepho_b200.autograd import _param_maps
+    dst = [2, 0, 2, 1, 2, 0]
+    src = [10, 11, 12, 13, 14, 15]
+    off, idx = _param_maps(4, dst, src)
+    assert off.tolist() == [0, 2, 3, 6, 6]
+    assert idx.tolist() == [11, 15, 13, 10, 12, 14]
