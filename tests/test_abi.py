@@ -151,3 +151,23 @@ def test_new_entry_points_reject_bad_arguments():
     shape = (ctypes.c_int * 3)()
     assert L.fpho_variant_shape(-1, shape) == 1 and L.fpho_variant_shape(999, shape) == 1
     assert L.fpho_variant_shape(0, shape) == len(_lib.variants())
+
+
+def test_fused_posterior_entry_points_reject_bad_arguments():
+    """Host-side checks of fpho_build_proposal_bounded and
+    fpho_bounded_lnp_grad, made before any CUDA call."""
+    from forcepho_b200 import _lib
+    L = _lib.get()
+    p = ctypes.c_void_p(16)  # never dereferenced: every call below fails its checks first
+    assert L.fpho_build_proposal_bounded(None, p, p, p, 1, 1, None, None, None, p, None) == 1
+    assert "NULL" in _lib.last_error()
+    assert L.fpho_build_proposal_bounded(p, p, p, p, 0, 1, None, None, None, p, None) == 1
+    assert L.fpho_build_proposal_bounded(p, p, p, p, 1, 1, p, None, None, p, None) == 1
+    assert "together" in _lib.last_error()
+    assert L.fpho_build_proposal_bounded(p, p, p, p, 1, 0, None, None, None, p, None) != 0
+    assert "n_bands" in _lib.last_error()
+    assert L.fpho_bounded_lnp_grad(0, p, p, p, p, p, p, p, 1, p, p, p, 1, p, None) == 1
+    assert L.fpho_bounded_lnp_grad(10, None, p, p, p, p, p, p, 1, p, p, p, 1, p, None) == 1
+    assert "NULL" in _lib.last_error()
+    assert L.fpho_bounded_lnp_grad(600, p, p, p, p, p, p, p, 1, p, p, p, 2, p, None) != 0
+    assert "partials" in _lib.last_error()
