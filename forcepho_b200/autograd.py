@@ -174,11 +174,18 @@ class _LnpGrad:
         self.work = torch.zeros((self.n + 255) // 256, dtype=torch.float64, device="cuda")
         self.counter = torch.zeros(1, dtype=torch.int32, device="cuda")
 
-    def __call__(self, z, dchi2, chi2):
+    def __call__(self, z, dchi2, chi2, out=None):
         if z.dtype != torch.float64 or not z.is_cuda or not z.is_contiguous():
             raise TypeError("z must be a contiguous float64 CUDA tensor")
-        g = torch.empty(self.n, dtype=torch.float64, device="cuda")
-        lnp = torch.empty((), dtype=torch.float64, device="cuda")
+        if out is None:
+            lnp = torch.empty((), dtype=torch.float64, device="cuda")
+            g = torch.empty(self.n, dtype=torch.float64, device="cuda")
+        else:
+            lnp, g = out
+            if (lnp.dtype != torch.float64 or g.dtype != torch.float64 or lnp.numel() != 1
+                    or g.numel() != self.n or not g.is_contiguous()):
+                raise ValueError("out must be a float64 scalar and a contiguous float64 "
+                                 f"vector of {self.n}")
         _lib.call("fpho_bounded_lnp_grad", self.n, z.data_ptr(), self.tr.lower.data_ptr(),
                   self.tr.range.data_ptr(), dchi2.data_ptr(), self.off.data_ptr(),
                   self.idx.data_ptr(), chi2.data_ptr(), chi2.numel(), g.data_ptr(),
@@ -245,16 +252,17 @@ class DevicePosterior:
         q = self.tr.lower + self.tr.range * s
         return LnLike.apply(q, self.ev) + torch.log(self.tr.range * s * (1.0 - s)).sum()
 
-    def lnprob_and_grad(self, z):
+    def lnprob_and_grad(self, z, out=None):
         """(lnp, d lnp / dz) at z: the transform and the proposal build in one
-        launch, the evaluation, and lnp with its gradient in one launch."""
+        launch, the evaluation, and lnp with its gradient in one launch
+        (written into ``out`` = (lnp, grad) tensors when given)."""
         z = z.contiguous()
         ev = self.ev
         _lib.call("fpho_build_proposal_bounded", ev.table.handle, z.data_ptr(),
                   self.tr.lower.data_ptr(), self.tr.range.data_ptr(), ev.n_sources, ev.n_bands,
                   None, None, None, ev.prop.data_ptr(), _stream())
         ev.evaluate(grad=True)
-        return self._lnpg(z, ev.dchi2, ev.chi2)
+        return self._lnpg(z, ev.dchi2, ev.chi2, out)
 
     def _lnprob_and_grad_torch(self, z):
         """The same from torch elementwise operations (the unfused form)."""
@@ -344,16 +352,17 @@ class BatchPosterior:
     def inverse_transform(self, q):
         return self.tr.inverse_transform(q)
 
-    def lnprob_and_grad(self, z):
-        """(lnp, d lnp / dz) at z in four launches: transform and proposals,
-        image Gaussians + tiles + reductions of the batch, lnp and gradient."""
+    def lnprob_and_grad(self, z, out=None):
+        """(lnp, d lnp / dz) at z in five launches: transform and proposals,
+        image Gaussians + tiles + reductions of the batch, lnp and gradient
+        (written into ``out`` = (lnp, grad) tensors when given)."""
         z = z.contiguous()
         _lib.call("fpho_build_proposal_bounded", self.table.handle, z.data_ptr(),
                   self.tr.lower.data_ptr(), self.tr.range.data_ptr(), self.src_bands.numel(), 0,
                   self.src_bands.data_ptr(), self.src_off.data_ptr(), None, self.prop.data_ptr(),
                   _stream())
         self.batch.evaluate_device(self.prop, self.chi2, self.dchi2, _stream())
-        return self._lnpg(z, self.dchi2, self.chi2)
+        return self._lnpg(z, self.dchi2, self.chi2, out)
 
     def _lnprob_and_grad_torch(self, z):
         """The same from torch elementwise operations (the unfused form)."""
@@ -411,6 +420,9 @@ class Leapfrog:
         return self.post.lnprob_and_grad(z)
 
     def _refresh(self):
+        if not self.use_autograd and isinstance(self.post, (DevicePosterior, BatchPosterior)):
+            self.post.lnprob_and_grad(self.z, out=(self.lnp, self.g))
+            return
         lnp, g = self._grad(self.z)
         self.lnp.copy_(lnp)
         self.g.copy_(g)

@@ -237,13 +237,23 @@ class MultiChainHMC:
         p = torch.randn(self.z.shape, dtype=torch.float64, device=self.device)  # whitened momenta
         kin0 = _per_patch(post, p * p) * 0.5
         z, g = self.z.clone(), self.g.clone()
-        gu = self._to_u(g)
-        for _ in range(self.L):
-            p = p + h * gu
-            z = z + eps * self._to_z(p)
-            _, g = post.lnprob_and_grad(z)
+        if self.chol is None:
+            # diagonal mass: kick p += (h scale) g, drift z += (eps scale) p,
+            # one launch each
+            hs, es = h * self.scale, eps * self.scale
+            for _ in range(self.L):
+                p.addcmul_(hs, g)
+                z.addcmul_(es, p)
+                _, g = post.lnprob_and_grad(z)
+                p.addcmul_(hs, g)
+        else:
             gu = self._to_u(g)
-            p = p + h * gu
+            for _ in range(self.L):
+                p = p + h * gu
+                z = z + eps * self._to_z(p)
+                _, g = post.lnprob_and_grad(z)
+                gu = self._to_u(g)
+                p = p + h * gu
         lnp1 = post.lnp_per_patch(z)
         kin1 = _per_patch(post, p * p) * 0.5
         log_ratio = (lnp1 - kin1) - (self.lnp - kin0)
