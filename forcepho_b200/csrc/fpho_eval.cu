@@ -635,7 +635,6 @@ static int create_patch(const fpho_patch_struct *host, int n_bands, int return_r
         }
     }
     if (!rc) rc = upload_meta(p, host, s);
-    if (!rc) rc = dalloc(&p->d_chi2_out, (size_t)p->n_bands);
     if (!rc) rc = dalloc(&p->d_err, 1);
     if (!rc && cudaMemsetAsync(p->d_err, 0, sizeof(int), s) != cudaSuccess)
         rc = set_error(FPHO_ERR_CUDA, "cudaMemsetAsync failed");
@@ -725,7 +724,8 @@ static void destroy_patch(fpho_patch *p) {
     free_plan(p);
     dfree(p->d_data); dfree(p->d_ierr); dfree(p->d_xpix); dfree(p->d_ypix); dfree(p->d_residual);
     dfree(p->d_exposure_start); dfree(p->d_exposure_N); dfree(p->d_band_start);
-    dfree(p->d_band_N); dfree(p->d_struct); dfree(p->d_chi2_out); dfree(p->d_dchi2_out);
+    dfree(p->d_band_N); dfree(p->d_struct); dfree(p->d_io);
+    if (p->h_io) cudaFreeHost(p->h_io);
     dfree(p->d_err); dfree(p->d_pairs); dfree(p->d_pnorm); dfree(p->d_atb);
     if (p->ev_tile0) cudaEventDestroy(p->ev_tile0);
     if (p->ev_tile1) cudaEventDestroy(p->ev_tile1);
@@ -906,26 +906,39 @@ extern "C" int fpho_evaluate_proposal(fpho_patch *p, const fpho_source *proposal
     if (!host_io)
         return enqueue_evaluate(p, proposal, chi2, dchi2, dchi2_stride, want_res, s, grad);
 
-    const size_t gbytes = (size_t)p->n_bands * dchi2_stride;
-    if (p->d_dchi2_cap < (int)gbytes) {
-        dfree(p->d_dchi2_out);
-        int rc = dalloc(&p->d_dchi2_out, gbytes);
+    const size_t gfloats = (size_t)p->n_bands * dchi2_stride;
+    const size_t chi2_bytes = sizeof(double) * p->n_bands;
+    const size_t io_bytes = chi2_bytes + sizeof(float) * gfloats;  // a multiple of 4
+    if (p->d_io_cap < io_bytes) {
+        dfree(p->d_io);
+        p->d_io_cap = 0;
+        int rc = dalloc(&p->d_io, io_bytes);
         if (rc) return rc;
-        p->d_dchi2_cap = (int)gbytes;
+        p->d_io_cap = io_bytes;
     }
+    if (p->h_io_cap < io_bytes + sizeof(int)) {
+        if (p->h_io) cudaFreeHost(p->h_io);
+        p->h_io = nullptr;
+        p->h_io_cap = 0;
+        CUDA_TRY(cudaHostAlloc((void **)&p->h_io, io_bytes + sizeof(int), cudaHostAllocDefault));
+        p->h_io_cap = io_bytes + sizeof(int);
+    }
+    double *d_chi2 = reinterpret_cast<double *>(p->d_io);
+    float *d_dchi2 = reinterpret_cast<float *>(p->d_io + chi2_bytes);
     CUDA_TRY(cudaMemcpyAsync(p->d_prop, proposal, sizeof(fpho_source) * n_sources,
                              cudaMemcpyHostToDevice, s));
-    int rc = enqueue_evaluate(p, p->d_prop, p->d_chi2_out, p->d_dchi2_out, dchi2_stride,
-                              want_res, s, grad);
+    int rc = enqueue_evaluate(p, p->d_prop, d_chi2, d_dchi2, dchi2_stride, want_res, s, grad);
     if (rc) return rc;
-    int err = 0;
-    CUDA_TRY(cudaMemcpyAsync(chi2, p->d_chi2_out, sizeof(double) * p->n_bands,
+    // the results in one transfer, the error word in a second, both pinned
+    CUDA_TRY(cudaMemcpyAsync(p->h_io, p->d_io, grad ? io_bytes : chi2_bytes,
                              cudaMemcpyDeviceToHost, s));
-    if (grad)
-        CUDA_TRY(cudaMemcpyAsync(dchi2, p->d_dchi2_out, sizeof(float) * gbytes,
-                                 cudaMemcpyDeviceToHost, s));
-    CUDA_TRY(cudaMemcpyAsync(&err, p->d_err, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CUDA_TRY(cudaMemcpyAsync(p->h_io + io_bytes, p->d_err, sizeof(int), cudaMemcpyDeviceToHost,
+                             s));
     CUDA_TRY(cudaStreamSynchronize(s));
+    std::memcpy(chi2, p->h_io, chi2_bytes);
+    if (grad) std::memcpy(dchi2, p->h_io + chi2_bytes, sizeof(float) * gfloats);
+    int err = 0;
+    std::memcpy(&err, p->h_io + io_bytes, sizeof(int));
     if (err) return set_error(FPHO_ERR_KERNEL, "tile kernel reported error word 0x%x", err);
     return FPHO_OK;
 }

@@ -57,9 +57,14 @@ struct fpho_patch {
     double *d_pchi2 = nullptr;
     float *d_pgrad = nullptr;
     fpho_source *d_prop = nullptr;
-    double *d_chi2_out = nullptr;
-    float *d_dchi2_out = nullptr;
-    int d_dchi2_cap = 0;
+    // host-I/O evaluations: the results on the device, [chi2 (n_bands
+    // doubles)][dchi2], copied back in one transfer into a pinned staging
+    // buffer (followed by the error word) and from there to the caller's
+    // arrays
+    unsigned char *d_io = nullptr;
+    size_t d_io_cap = 0;
+    unsigned char *h_io = nullptr;
+    size_t h_io_cap = 0;
     int *d_err = nullptr;
     long long *d_pairs = nullptr;
     // flux solve (fpho_flux.cu): per-tile normal-equation partials and ATb
