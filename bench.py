@@ -965,7 +965,9 @@ def run_ours(args):
             "e2e": {"value": e2e_value, "unit": "evals/s",
                     "h2d_bytes_per_step": int(prop.nbytes),
                     "d2h_bytes_per_step": int(nb * 8 + nb * ns * 7 * 4 + 4)},
-            "gpu_launches": (4 if cfg.get("schedule", 0) == 1 else 3) * args.steps,
+            # per evaluation: prepare_evaluation (image Gaussians, tile order,
+            # error word), the tile kernel and reduce_bands
+            "gpu_launches": 3 * args.steps,
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_tflops,
                          "unit": "TFLOP/s", "frac": achieved / fp32_tflops,
                          "traffic": TILE_TRAFFIC_BYTES,

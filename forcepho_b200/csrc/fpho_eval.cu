@@ -79,7 +79,7 @@ __global__ void __launch_bounds__(NT) tile_kernel(TileArgs A) {
 }
 
 // Persistent form: each CTA takes tiles from `order` through an atomic counter
-// (reset by order_tiles) until the list is exhausted, so the most expensive
+// (reset with the ordering, order_tiles_body) until the list is exhausted, so the most expensive
 // tiles start first and the cheap ones fill the gaps at the end.  The counter
 // only hands out indices; no CTA waits on another.
 template <int NT, int K, bool GRAD, bool EXACT = false>
@@ -835,13 +835,17 @@ int enqueue_evaluate(fpho_patch *p, const fpho_source *d_prop, double *d_chi2, f
     if (want_residual && !p->d_residual)
         return set_error(FPHO_ERR_STATE,
                          "residual requested but the patch was created without one");
-    CUDA_TRY(cudaMemsetAsync(p->d_err, 0, sizeof(int), s));
     if (p->count_pairs) CUDA_TRY(cudaMemsetAsync(p->d_pairs, 0, sizeof(long long), s));
     const PatchView pv = make_view(p);
-    const int max_g = p->max_g;
-    if (max_g > 0) {
-        dim3 grid((max_g + 127) / 128, p->n_exp);
-        build_image_gaussians<<<grid, 128, 0, s>>>(pv, d_prop, p->d_gtab, p->d_gbox);
+    // the order only matters when the tiles outnumber what runs at once
+    const bool ordered = p->schedule == 1 && p->n_tiles > 4 * device_sms();
+    {
+        // image Gaussians, the tile order and the error word in one launch
+        dim3 grid(std::max((p->max_g + 127) / 128, 1), p->n_exp + (ordered ? 1 : 0));
+        prepare_evaluation<<<grid, 128, 0, s>>>(pv, d_prop, p->d_gtab, p->d_gbox,
+                                                p->d_tile_cost, p->n_tiles,
+                                                ordered ? p->d_tile_order : nullptr,
+                                                p->d_tile_counter, p->d_err);
         CUDA_TRY(cudaGetLastError());
     }
     TileArgs A;
@@ -862,12 +866,8 @@ int enqueue_evaluate(fpho_patch *p, const fpho_source *d_prop, double *d_chi2, f
     A.test_extra_tx = p->test_extra_tx;
     if (p->ev_tile0) CUDA_TRY(cudaEventRecord(p->ev_tile0, s));
     int rc;
-    // the order only matters when the tiles outnumber what runs at once
-    if (p->schedule == 1 && p->n_tiles > 4 * device_sms()) {
+    if (ordered) {
         A.tile_cost = p->d_tile_cost;
-        order_tiles<<<1, 1024, 0, s>>>(p->d_tile_cost, p->n_tiles, p->d_tile_order,
-                                       p->d_tile_counter);
-        CUDA_TRY(cudaGetLastError());
         rc = launch_tile_kernel(p->variant, A, p->n_tiles, s, grad, p->d_tile_order,
                                 p->d_tile_counter, p->exact_residual != 0);
     } else {

@@ -61,9 +61,9 @@ static __global__ void tile_bboxes(PatchView pv, const TileDesc *tiles, float4 *
 // [0, max cost]; within a bucket the order is whatever the shared-memory
 // atomics give.  The result does not depend on the order, since every tile
 // writes its own partials and reduce_bands sums them in tile-index order.
-// One CTA of 1024 threads.  Also resets the work counter.
-static __global__ void __launch_bounds__(1024) order_tiles(const int *cost, int n_tiles, int *order,
-                                                           int *counter) {
+// One CTA (at least 64 threads).  Also resets the work counter.
+__device__ __forceinline__ void order_tiles_body(const int *cost, int n_tiles, int *order,
+                                                 int *counter) {
     constexpr int NB = 64;
     __shared__ int hist[NB];
     __shared__ int smax;
@@ -94,6 +94,29 @@ static __global__ void __launch_bounds__(1024) order_tiles(const int *cost, int 
     __syncthreads();
     for (int i = tid; i < n_tiles; i += blockDim.x)
         order[atomicAdd(&hist[NB - 1 - (int)((long long)cost[i] * NB / span)], 1)] = i;
+}
+
+// The launch before the tile kernel of an evaluation: blocks (x, e < n_exp)
+// build exposure e's image Gaussians (as build_image_gaussians); with
+// `order`, the block (0, n_exp) orders the tiles by the previous
+// evaluation's costs (as order_tiles) at the same time; and block (0, 0)
+// clears the error word.  One launch instead of a memset and two kernels.
+static __global__ void __launch_bounds__(128) prepare_evaluation(
+    PatchView pv, const fpho_source *src, float *gtab, float4 *gbox, const int *cost, int n_tiles,
+    int *order, int *counter, int *err) {
+    if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) *err = 0;
+    const int e = blockIdx.y;
+    if (e == pv.n_exp) {
+        if (blockIdx.x == 0 && order) order_tiles_body(cost, n_tiles, order, counter);
+        return;
+    }
+    const int g0 = pv.gauss_start[e];
+    const int n = pv.gauss_start[e + 1] - g0;
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int npsf = pv.exp_npsf[e];
+    const int s = i / npsf, p = i - s * npsf;
+    build_one_gaussian(pv, src, e, s, p, gtab + (size_t)(g0 + i) * GREC, gbox + g0 + i);
 }
 
 // Sum of a tile range [t0, t1) of one column (FP64): lane l adds tiles
