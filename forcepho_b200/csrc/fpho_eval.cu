@@ -841,8 +841,9 @@ int enqueue_evaluate(fpho_patch *p, const fpho_source *d_prop, double *d_chi2, f
     const bool ordered = p->schedule == 1 && p->n_tiles > 4 * device_sms();
     {
         // image Gaussians, the tile order and the error word in one launch
-        dim3 grid(std::max((p->max_g + 127) / 128, 1), p->n_exp + (ordered ? 1 : 0));
-        prepare_evaluation<<<grid, 128, 0, s>>>(pv, d_prop, p->d_gtab, p->d_gbox,
+        dim3 grid(std::max((p->max_g + PREP_THREADS - 1) / PREP_THREADS, 1),
+                  p->n_exp + (ordered ? 1 : 0));
+        prepare_evaluation<<<grid, PREP_THREADS, 0, s>>>(pv, d_prop, p->d_gtab, p->d_gbox,
                                                 p->d_tile_cost, p->n_tiles,
                                                 ordered ? p->d_tile_order : nullptr,
                                                 p->d_tile_counter, p->d_err);

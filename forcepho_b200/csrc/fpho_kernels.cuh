@@ -101,7 +101,11 @@ __device__ __forceinline__ void order_tiles_body(const int *cost, int n_tiles, i
 // `order`, the block (0, n_exp) orders the tiles by the previous
 // evaluation's costs (as order_tiles) at the same time; and block (0, 0)
 // clears the error word.  One launch instead of a memset and two kernels.
-static __global__ void __launch_bounds__(128) prepare_evaluation(
+// Launched with PREP_THREADS threads per block: the ordering block is then
+// as wide as a standalone sort would be (its passes over the costs are
+// latency-bound), and one block covers an exposure's image Gaussians.
+constexpr int PREP_THREADS = 1024;
+static __global__ void __launch_bounds__(PREP_THREADS) prepare_evaluation(
     PatchView pv, const fpho_source *src, float *gtab, float4 *gbox, const int *cost, int n_tiles,
     int *order, int *counter, int *err) {
     if (blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) *err = 0;
