@@ -831,7 +831,8 @@ namespace fpho {
 
 // Enqueue one evaluation with device-resident proposal and outputs.
 int enqueue_evaluate(fpho_patch *p, const fpho_source *d_prop, double *d_chi2, float *d_dchi2,
-                     int out_stride, bool want_residual, cudaStream_t s, bool grad) {
+                     int out_stride, bool want_residual, cudaStream_t s, bool grad,
+                     int *d_err_out = nullptr) {
     if (want_residual && !p->d_residual)
         return set_error(FPHO_ERR_STATE,
                          "residual requested but the patch was created without one");
@@ -880,7 +881,7 @@ int enqueue_evaluate(fpho_patch *p, const fpho_source *d_prop, double *d_chi2, f
     dim3 rg(p->n_bands, grad ? (out_stride + REDUCE_WARPS - 1) / REDUCE_WARPS : 1);
     reduce_bands<<<rg, 32 * REDUCE_WARPS, 0, s>>>(p->d_tile_band_start, p->d_pchi2, p->d_pgrad,
                                     7 * p->n_sources, d_chi2, grad ? d_dchi2 : nullptr,
-                                    out_stride);
+                                    out_stride, p->d_err, d_err_out);
     CUDA_TRY(cudaGetLastError());
     return FPHO_OK;
 }
@@ -907,9 +908,11 @@ extern "C" int fpho_evaluate_proposal(fpho_patch *p, const fpho_source *proposal
     if (!host_io)
         return enqueue_evaluate(p, proposal, chi2, dchi2, dchi2_stride, want_res, s, grad);
 
+    // [chi2 (n_bands doubles)][error word, 8 bytes][dchi2]
     const size_t gfloats = (size_t)p->n_bands * dchi2_stride;
     const size_t chi2_bytes = sizeof(double) * p->n_bands;
-    const size_t io_bytes = chi2_bytes + sizeof(float) * gfloats;  // a multiple of 4
+    const size_t head_bytes = chi2_bytes + 8;
+    const size_t io_bytes = head_bytes + sizeof(float) * gfloats;
     if (p->d_io_cap < io_bytes) {
         dfree(p->d_io);
         p->d_io_cap = 0;
@@ -917,29 +920,29 @@ extern "C" int fpho_evaluate_proposal(fpho_patch *p, const fpho_source *proposal
         if (rc) return rc;
         p->d_io_cap = io_bytes;
     }
-    if (p->h_io_cap < io_bytes + sizeof(int)) {
+    if (p->h_io_cap < io_bytes) {
         if (p->h_io) cudaFreeHost(p->h_io);
         p->h_io = nullptr;
         p->h_io_cap = 0;
-        CUDA_TRY(cudaHostAlloc((void **)&p->h_io, io_bytes + sizeof(int), cudaHostAllocDefault));
-        p->h_io_cap = io_bytes + sizeof(int);
+        CUDA_TRY(cudaHostAlloc((void **)&p->h_io, io_bytes, cudaHostAllocDefault));
+        p->h_io_cap = io_bytes;
     }
     double *d_chi2 = reinterpret_cast<double *>(p->d_io);
-    float *d_dchi2 = reinterpret_cast<float *>(p->d_io + chi2_bytes);
+    int *d_err_out = reinterpret_cast<int *>(p->d_io + chi2_bytes);
+    float *d_dchi2 = reinterpret_cast<float *>(p->d_io + head_bytes);
     CUDA_TRY(cudaMemcpyAsync(p->d_prop, proposal, sizeof(fpho_source) * n_sources,
                              cudaMemcpyHostToDevice, s));
-    int rc = enqueue_evaluate(p, p->d_prop, d_chi2, d_dchi2, dchi2_stride, want_res, s, grad);
+    int rc = enqueue_evaluate(p, p->d_prop, d_chi2, d_dchi2, dchi2_stride, want_res, s, grad,
+                              d_err_out);
     if (rc) return rc;
-    // the results in one transfer, the error word in a second, both pinned
-    CUDA_TRY(cudaMemcpyAsync(p->h_io, p->d_io, grad ? io_bytes : chi2_bytes,
+    // results and error word in one transfer into pinned memory
+    CUDA_TRY(cudaMemcpyAsync(p->h_io, p->d_io, grad ? io_bytes : head_bytes,
                              cudaMemcpyDeviceToHost, s));
-    CUDA_TRY(cudaMemcpyAsync(p->h_io + io_bytes, p->d_err, sizeof(int), cudaMemcpyDeviceToHost,
-                             s));
     CUDA_TRY(cudaStreamSynchronize(s));
     std::memcpy(chi2, p->h_io, chi2_bytes);
-    if (grad) std::memcpy(dchi2, p->h_io + chi2_bytes, sizeof(float) * gfloats);
+    if (grad) std::memcpy(dchi2, p->h_io + head_bytes, sizeof(float) * gfloats);
     int err = 0;
-    std::memcpy(&err, p->h_io + io_bytes, sizeof(int));
+    std::memcpy(&err, p->h_io + chi2_bytes, sizeof(int));
     if (err) return set_error(FPHO_ERR_KERNEL, "tile kernel reported error word 0x%x", err);
     return FPHO_OK;
 }

@@ -58,9 +58,8 @@ struct fpho_patch {
     float *d_pgrad = nullptr;
     fpho_source *d_prop = nullptr;
     // host-I/O evaluations: the results on the device, [chi2 (n_bands
-    // doubles)][dchi2], copied back in one transfer into a pinned staging
-    // buffer (followed by the error word) and from there to the caller's
-    // arrays
+    // doubles)][error word, 8 bytes][dchi2], copied back in one transfer into
+    // a pinned staging buffer and from there to the caller's arrays
     unsigned char *d_io = nullptr;
     size_t d_io_cap = 0;
     unsigned char *h_io = nullptr;

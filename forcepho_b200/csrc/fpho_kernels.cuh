@@ -142,10 +142,14 @@ constexpr int REDUCE_WARPS = 4;
 // Sum tile partials per band in double.  grid (n_bands, ceil(out_stride /
 // REDUCE_WARPS)), block 32 REDUCE_WARPS: warp w of block y sums component
 // y REDUCE_WARPS + w; block y = 0, warp 0 also sums chi2.
+// With err_out, block (0, 0) also copies the evaluation's error word there
+// (beside the results, so that one transfer brings both to the host).
 static __global__ void reduce_bands(const int *tile_band_start, const double *pchi2,
                                     const float *pgrad, int stride, double *chi2_out,
-                                    float *dchi2_out, int out_stride) {
+                                    float *dchi2_out, int out_stride, const int *err = nullptr,
+                                    int *err_out = nullptr) {
     const int b = blockIdx.x;
+    if (err_out && blockIdx.x == 0 && blockIdx.y == 0 && threadIdx.x == 0) *err_out = *err;
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int t0 = tile_band_start[b], t1 = tile_band_start[b + 1];
     const int j = blockIdx.y * REDUCE_WARPS + w;
