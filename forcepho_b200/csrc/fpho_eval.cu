@@ -79,8 +79,9 @@ __global__ void __launch_bounds__(NT) tile_kernel(TileArgs A) {
 }
 
 // Persistent form: each CTA takes tiles from `order` through an atomic counter
-// (reset with the ordering, order_tiles_body) until the list is exhausted, so the most expensive
-// tiles start first and the cheap ones fill the gaps at the end.  The counter
+// (reset with the ordering, order_tiles_body) until the list is exhausted, so
+// the most expensive tiles start first and the cheap ones fill the gaps at
+// the end.  The counter
 // only hands out indices; no CTA waits on another.
 template <int NT, int K, bool GRAD, bool EXACT = false>
 __global__ void __launch_bounds__(NT) tile_kernel_dyn(TileArgs A, const int *order, int n_tiles,
@@ -843,7 +844,7 @@ int enqueue_evaluate(fpho_patch *p, const fpho_source *d_prop, double *d_chi2, f
     {
         // image Gaussians, the tile order and the error word in one launch
         dim3 grid(std::max((p->max_g + PREP_THREADS - 1) / PREP_THREADS, 1),
-                  p->n_exp + (ordered ? 1 : 0));
+                  std::max(p->n_exp + (ordered ? 1 : 0), 1));
         prepare_evaluation<<<grid, PREP_THREADS, 0, s>>>(pv, d_prop, p->d_gtab, p->d_gbox,
                                                 p->d_tile_cost, p->n_tiles,
                                                 ordered ? p->d_tile_order : nullptr,
