@@ -128,46 +128,6 @@ __device__ void spline_eval(const SplineView &S, int k, double x, double y, doub
 // With `src_bands` / `src_off` (batched form) source s has src_bands[s] bands
 // and its parameters start at theta[src_off[s]]; otherwise every source has
 // `n_bands` bands and a stride of n_bands + 6.
-// One source from its parameters p[n_bands + 6] (Scene order).
-__device__ void build_source(const SplineView &S, const double *p, int n_bands,
-                             fpho_source *dst) {
-    fpho_source src;
-    memset(&src, 0, sizeof(src));
-    for (int b = 0; b < n_bands; ++b) src.fluxes[b] = (float)p[b];
-    src.ra = (float)p[n_bands];
-    src.dec = (float)p[n_bands + 1];
-    src.q = (float)p[n_bands + 2];
-    src.pa = (float)p[n_bands + 3];
-    const double nser = p[n_bands + 4], rh = p[n_bands + 5];
-    src.nsersic = (float)nser;
-    src.rh = (float)rh;
-    if (nser < S.sersic_min) {  // sources.py:656-660: all weight on the radius nearest rh
-        int best = 0;
-        double bd = fabs(rh - S.radii[0]);
-        for (int k = 1; k < S.n_radii; ++k) {
-            const double d = fabs(rh - S.radii[k]);
-            if (d < bd) { bd = d; best = k; }
-        }
-        src.mixture_amplitudes[best] = 1.0f;
-    } else if (rh < 0.0) {      // sources.py:661-663
-        src.mixture_amplitudes[0] = 1.0f;
-    } else {
-        // one basis for all radii: the knot searches are dependent global
-        // loads, so evaluating them once per source instead of once per
-        // radius is what the kernel's time is made of
-        SplineBasis sb;
-        spline_basis(S, nser, rh, sb);
-        for (int k = 0; k < S.n_radii; ++k) {
-            double v[3];
-            spline_combine(S, k, sb, v);
-            src.mixture_amplitudes[k] = (float)v[0];
-            src.damplitude_dnsersic[k] = (float)v[1];
-            src.damplitude_drh[k] = (float)v[2];
-        }
-    }
-    *dst = src;
-}
-
 // The knot vectors in shared memory: the binary searches of the bases then
 // wait on shared-memory loads instead of dependent global ones.  Every thread
 // of the block calls it (a barrier).
@@ -182,41 +142,79 @@ __device__ __forceinline__ SplineView knots_to_shared(const SplineView &S, doubl
     return L;
 }
 
-__global__ void build_proposal_kernel(SplineView S, const double *theta, int n_src, int n_bands,
-                                      const int *src_bands, const long long *src_off,
-                                      fpho_source *out) {
-    __shared__ double s_tx[SPL_MAX_KNOTS], s_ty[SPL_MAX_KNOTS];
-    const SplineView L = knots_to_shared(S, s_tx, s_ty);
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= n_src) return;
-    if (src_bands) n_bands = src_bands[s];
-    const double *p = theta + (src_off ? (size_t)src_off[s] : (size_t)s * (n_bands + 6));
-    build_source(L, p, n_bands, out + s);
-}
-
 // sigmoid in double, as torch.sigmoid evaluates it
 __device__ __forceinline__ double sigmoid_d(double z) { return 1.0 / (1.0 + exp(-z)); }
 
-// The same from unconstrained parameters z through the bounded transform
-// q = lower + range * sigmoid(z) (BoundedTransform.transform,
-// forcepho/model.py:596-637), one thread per source; q is also stored when
-// q_out is not NULL.
-__global__ void build_proposal_bounded_kernel(SplineView S, const double *z, const double *lower,
-                                              const double *range, int n_src, int n_bands,
-                                              const int *src_bands, const long long *src_off,
-                                              double *q_out, fpho_source *out) {
+// One warp per source: parameters in the reference's Scene order
+// [flux_1..flux_B, ra, dec, q, pa, sersic, rhalf] -> fpho_source.  Lane i
+// holds parameters i and i + 32 (with BOUNDED, mapped from unconstrained z
+// through q = lower + range * sigmoid(z), BoundedTransform.transform,
+// forcepho/model.py:596-637, and stored to q_out when given) and writes the
+// fields they fill; lane k < n_radii evaluates mixture radius k's spline
+// (value, d/dsersic, d/drh) with the reference's branches for sersic below
+// the table and rh < 0 (forcepho/sources.py:656-663); every other field is
+// zero.  Each field is rounded to float exactly as a per-source loop would.
+// With `src_bands` / `src_off` (batched form) source s has src_bands[s]
+// bands and its parameters start at par[src_off[s]]; otherwise every source
+// has `n_bands` bands and a stride of n_bands + 6.
+constexpr int PROP_THREADS = 128;
+template <bool BOUNDED>
+__global__ void __launch_bounds__(PROP_THREADS) proposal_kernel(
+    SplineView S, const double *par, const double *lower, const double *range, int n_src,
+    int n_bands, const int *src_bands, const long long *src_off, double *q_out,
+    fpho_source *out) {
     __shared__ double s_tx[SPL_MAX_KNOTS], s_ty[SPL_MAX_KNOTS];
     const SplineView L = knots_to_shared(S, s_tx, s_ty);
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= n_src) return;
-    if (src_bands) n_bands = src_bands[s];
-    const size_t o = src_off ? (size_t)src_off[s] : (size_t)s * (n_bands + 6);
-    double q[FPHO_MAXBANDS + 6];
-    for (int i = 0; i < n_bands + 6; ++i) {
-        q[i] = lower[o + i] + range[o + i] * sigmoid_d(z[o + i]);
-        if (q_out) q_out[o + i] = q[i];
+    const int lane = threadIdx.x & 31;
+    const int s = blockIdx.x * (PROP_THREADS / 32) + (threadIdx.x >> 5);
+    if (s >= n_src) return;  // whole warps
+    const int nb = src_bands ? src_bands[s] : n_bands;
+    const size_t o = src_off ? (size_t)src_off[s] : (size_t)s * (nb + 6);
+    const int np = nb + 6;
+    float *f = reinterpret_cast<float *>(out + s);
+    // field offsets (floats) in fpho_source
+    constexpr int F_SHAPE = 0, F_FLUX = 6, F_AMP = F_FLUX + FPHO_MAXBANDS;
+    constexpr int F_DRH = F_AMP + FPHO_MAXRADII, F_DN = F_DRH + FPHO_MAXRADII;
+    double v[2] = {0.0, 0.0};
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int i = lane + 32 * h;
+        if (i >= np) continue;
+        double x = par[o + i];
+        if (BOUNDED) {
+            x = lower[o + i] + range[o + i] * sigmoid_d(x);
+            if (q_out) q_out[o + i] = x;
+        }
+        v[h] = x;
+        f[i < nb ? F_FLUX + i : F_SHAPE + (i - nb)] = (float)x;
     }
-    build_source(L, q, n_bands, out + s);
+    if (lane >= nb && lane < FPHO_MAXBANDS) f[F_FLUX + lane] = 0.0f;
+    const int in = nb + 4, ir = nb + 5;
+    const double nser = __shfl_sync(0xffffffffu, in < 32 ? v[0] : v[1], in & 31);
+    const double rh = __shfl_sync(0xffffffffu, ir < 32 ? v[0] : v[1], ir & 31);
+    if (lane >= FPHO_MAXRADII) return;
+    const int k = lane;
+    float amp = 0.0f, dn = 0.0f, drh = 0.0f;
+    if (nser < L.sersic_min) {  // all weight on the radius nearest rh
+        int best = 0;
+        double bd = fabs(rh - L.radii[0]);
+        for (int j = 1; j < L.n_radii; ++j) {
+            const double d = fabs(rh - L.radii[j]);
+            if (d < bd) { bd = d; best = j; }
+        }
+        amp = (k == best) ? 1.0f : 0.0f;
+    } else if (rh < 0.0) {
+        amp = (k == 0) ? 1.0f : 0.0f;
+    } else if (k < L.n_radii) {
+        double w[3];
+        spline_eval(L, k, nser, rh, w);
+        amp = (float)w[0];
+        dn = (float)w[1];
+        drh = (float)w[2];
+    }
+    f[F_AMP + k] = amp;
+    f[F_DRH + k] = drh;
+    f[F_DN + k] = dn;
 }
 
 // lnp(z) = -chi2/2 + sum_i log jac_i and its gradient w.r.t. z, with
@@ -367,8 +365,8 @@ extern "C" int fpho_build_proposal(const fpho_spline *s, const double *theta, in
                          FPHO_MAX_ACTIVE_SOURCES);
     if (n_bands < 1 || n_bands > FPHO_MAXBANDS)
         return set_error(FPHO_ERR_LIMIT, "n_bands=%d outside [1, %d]", n_bands, FPHO_MAXBANDS);
-    build_proposal_kernel<<<(n_sources + 63) / 64, 64, 0, (cudaStream_t)stream>>>(
-        s->view, theta, n_sources, n_bands, nullptr, nullptr, out);
+    proposal_kernel<false><<<(n_sources + 3) / 4, PROP_THREADS, 0, (cudaStream_t)stream>>>(
+        s->view, theta, nullptr, nullptr, n_sources, n_bands, nullptr, nullptr, nullptr, out);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return set_error(FPHO_ERR_CUDA, "launch: %s", cudaGetErrorString(e));
     return FPHO_OK;
@@ -399,7 +397,7 @@ extern "C" int fpho_build_proposal_bounded(const fpho_spline *s, const double *z
         return set_error(FPHO_ERR_INVALID, "src_bands and src_offset go together");
     if (!src_bands && (n_bands < 1 || n_bands > FPHO_MAXBANDS))
         return set_error(FPHO_ERR_LIMIT, "n_bands=%d outside [1, %d]", n_bands, FPHO_MAXBANDS);
-    build_proposal_bounded_kernel<<<(n_sources + 63) / 64, 64, 0, (cudaStream_t)stream>>>(
+    proposal_kernel<true><<<(n_sources + 3) / 4, PROP_THREADS, 0, (cudaStream_t)stream>>>(
         s->view, z, lower, range, n_sources, n_bands, src_bands, src_offset, q_out, out);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return set_error(FPHO_ERR_CUDA, "launch: %s", cudaGetErrorString(e));
@@ -435,8 +433,8 @@ extern "C" int fpho_build_proposal_batch(const fpho_spline *s, const double *the
     if (!s || !theta || !src_bands || !src_offset || !out)
         return set_error(FPHO_ERR_INVALID, "NULL argument");
     if (n_sources < 1) return set_error(FPHO_ERR_INVALID, "n_sources=%d < 1", n_sources);
-    build_proposal_kernel<<<(n_sources + 63) / 64, 64, 0, (cudaStream_t)stream>>>(
-        s->view, theta, n_sources, 0, src_bands, src_offset, out);
+    proposal_kernel<false><<<(n_sources + 3) / 4, PROP_THREADS, 0, (cudaStream_t)stream>>>(
+        s->view, theta, nullptr, nullptr, n_sources, 0, src_bands, src_offset, nullptr, out);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return set_error(FPHO_ERR_CUDA, "launch: %s", cudaGetErrorString(e));
     return FPHO_OK;
