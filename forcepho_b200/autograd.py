@@ -161,6 +161,16 @@ def _param_maps(n_params, dst, src):
     return off, src[order]
 
 
+def _device_z(z, n):
+    """z as the contiguous float64 CUDA vector of n entries that the fused
+    launches read; anything else is refused before a kernel sees it."""
+    if not isinstance(z, torch.Tensor) or z.dtype != torch.float64 or not z.is_cuda:
+        raise TypeError("z must be a float64 CUDA tensor")
+    if z.numel() != n:
+        raise ValueError(f"z has {z.numel()} entries, the posterior has {n} parameters")
+    return z.contiguous().view(-1)
+
+
 class _LnpGrad:
     """lnp(z) and d lnp / dz in one launch (fpho_bounded_lnp_grad) from an
     evaluation's chi2 and dchi2, for a bounded transform `tr` and the
@@ -256,7 +266,7 @@ class DevicePosterior:
         """(lnp, d lnp / dz) at z: the transform and the proposal build in one
         launch, the evaluation, and lnp with its gradient in one launch
         (written into ``out`` = (lnp, grad) tensors when given)."""
-        z = z.contiguous()
+        z = _device_z(z, self.ndim)
         ev = self.ev
         _lib.call("fpho_build_proposal_bounded", ev.table.handle, z.data_ptr(),
                   self.tr.lower.data_ptr(), self.tr.range.data_ptr(), ev.n_sources, ev.n_bands,
@@ -356,7 +366,7 @@ class BatchPosterior:
         """(lnp, d lnp / dz) at z in five launches: transform and proposals,
         image Gaussians + tiles + reductions of the batch, lnp and gradient
         (written into ``out`` = (lnp, grad) tensors when given)."""
-        z = z.contiguous()
+        z = _device_z(z, self.ndim)
         _lib.call("fpho_build_proposal_bounded", self.table.handle, z.data_ptr(),
                   self.tr.lower.data_ptr(), self.tr.range.data_ptr(), self.src_bands.numel(), 0,
                   self.src_bands.data_ptr(), self.src_off.data_ptr(), None, self.prop.data_ptr(),

@@ -126,3 +126,13 @@ def test_param_maps_group_in_order():
     off, idx = _param_maps(4, dst, src)
     assert off.tolist() == [0, 2, 3, 6, 6]
     assert idx.tolist() == [11, 15, 13, 10, 12, 14]
+
+
+def test_fused_posterior_refuses_bad_z():
+    """The fused launches read z as ndim float64 values on the GPU: a z of
+    another type, device or length is refused before any launch."""
+    import torch
+    from forcepho_b200.autograd import _device_z
+    for bad in (np.zeros(3), torch.zeros(3), torch.zeros(3, dtype=torch.float32)):
+        with pytest.raises(TypeError):
+            _device_z(bad, 3)
